@@ -1,0 +1,237 @@
+"""Generate the golden fixtures in this folder by running the reference.
+
+Run once, where the reference's Python package is importable:
+
+    PYTHONPATH=<reference checkout> python tests/golden/make_golden.py [reference checkout]
+
+It writes small .npz files holding inputs and the reference's own outputs
+(grid arrays, transmissibilities, oil-water residuals and Jacobians, Newton
+histories, incompressible pressure solves) plus the reference's MATLAB golden
+arrays (examples/validation/ref_p2_*.mat, ref_p5_ow.mat) copied as data.  The
+tests read only the .npz files, so they run without the reference.
+"""
+
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).parent
+REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(os.environ.get("PYMRST_REFERENCE", "/root/reference"))
+sys.path.insert(0, str(REF))
+
+import scipy.io  # noqa: E402
+from scipy.ndimage import uniform_filter  # noqa: E402
+
+from pymrst.gridprocessing import cart_grid, compute_geometry  # noqa: E402
+from pymrst.modules.ad_blackoil import TwoPhaseOilWaterModelAD  # noqa: E402
+from pymrst.modules.ad_core import simulate_schedule_ad  # noqa: E402
+from pymrst.modules.ad_props import init_simple_adi_fluid  # noqa: E402
+from pymrst.params import add_well, make_rock  # noqa: E402
+from pymrst.solvers import compute_trans  # noqa: E402
+from pymrst.solvers.get_face_transmissibility import get_face_transmissibility  # noqa: E402
+from pymrst.utils.adi import combine_equations, init_variables_adi  # noqa: E402
+from pymrst.utils.units import BARSA, CENTI, DARCY, DAY, MILLI, POISE  # noqa: E402
+
+
+def lognormal_perm(dims, seed, sigma=1.0, mean_md=100.0):
+    rng = np.random.default_rng(seed)
+    logk = rng.normal(np.log(mean_md), sigma, size=tuple(dims))
+    logk = uniform_filter(logk, size=3, mode="nearest")
+    return np.exp(logk).ravel(order="F") * MILLI * DARCY
+
+
+def save(name, **arrays):
+    np.savez_compressed(HERE / name, **arrays)
+    print("wrote", name, sum(np.asarray(v).nbytes for v in arrays.values()), "bytes raw")
+
+
+def wells_arrays(prefix, wells):
+    out = {}
+    out[prefix + "count"] = np.array(len(wells))
+    for k, w in enumerate(wells):
+        out[f"{prefix}{k}_cells"] = np.asarray(w.cells)
+        out[f"{prefix}{k}_WI"] = np.asarray(w.WI)
+        out[f"{prefix}{k}_dZ"] = np.asarray(w.dZ)
+        out[f"{prefix}{k}_compi"] = np.asarray(w.compi)
+        out[f"{prefix}{k}_type"] = np.array(w.type)
+        out[f"{prefix}{k}_val"] = np.array(w.val)
+        out[f"{prefix}{k}_refDepth"] = np.array(w.refDepth)
+    return out
+
+
+def grid_fixture():
+    g = compute_geometry(cart_grid([4, 3, 2], [40.0, 30.0, 4.0]))
+    perm = lognormal_perm([4, 3, 2], 11)
+    rock1 = make_rock(g, perm[:, None], 0.2)
+    perm3 = np.column_stack([perm, 2 * perm, 0.1 * perm])
+    rock3 = make_rock(g, perm3, 0.2)
+    t1 = compute_trans(g, rock1)
+    t3 = compute_trans(g, rock3)
+    save("grid_trans.npz",
+         neighbors=g.faces.neighbors, cell_faces=g.cells.faces, facePos=g.cells.facePos,
+         cell_centroids=g.cells.centroids, face_centroids=g.faces.centroids,
+         normals=g.faces.normals, areas=g.faces.areas, volumes=g.cells.volumes,
+         perm=perm, perm3=perm3, hT1=t1, hT3=t3,
+         T1=get_face_transmissibility(g, rock1), T3=get_face_transmissibility(g, rock3))
+
+
+def ow_fluid(kind):
+    if kind == "cfg":
+        return init_simple_adi_fluid(mu=np.array([1.0, 5.0]) * CENTI * POISE,
+                                     rho=[1000.0, 800.0], n=[2, 2],
+                                     c=[1e-5 / BARSA, 1e-5 / BARSA], p_ref=200 * BARSA,
+                                     smin=[0.1, 0.1])
+    return init_simple_adi_fluid(mu=np.array([1.0, 5.0]) * CENTI * POISE,
+                                 rho=[1000.0, 800.0], n=[2, 2],
+                                 c=[1e-6 / BARSA, 1e-4 / BARSA], p_ref=200 * BARSA)
+
+
+def assemble_fixture(name, dims, phys, seed, fluid_kind, gravity, crossflow):
+    rng = np.random.default_rng(seed)
+    g = compute_geometry(cart_grid(dims, phys))
+    nc = g.cells.num
+    perm = lognormal_perm(dims, seed)
+    rock = make_rock(g, perm[:, None], 0.2)
+    fluid = ow_fluid(fluid_kind)
+    nx, ny, nz = dims
+    col = lambda i, j: i + nx * (j + ny * np.arange(nz))
+    gvec = np.array([0, 0, gravity]) if gravity else None
+    w = add_well(None, g, rock, col(0, 0), well_type="rate", val=2e-3,
+                 compi=np.array([1.0, 0.0]), sign=1, gravity=gvec)
+    w = add_well(w, g, rock, col(nx - 1, 0), well_type="rate", val=1e-3,
+                 compi=np.array([1.0, 0.0]), sign=1, gravity=gvec)
+    w = add_well(w, g, rock, col(nx - 1, ny - 1), well_type="bhp", val=150 * BARSA,
+                 compi=np.array([0.0, 1.0]), sign=-1, gravity=gvec)
+    if crossflow:
+        w = add_well(w, g, rock, col(nx // 2, ny // 2), well_type="bhp", val=200 * BARSA,
+                     compi=np.array([0.0, 1.0]), sign=-1, gravity=gvec)
+    model = TwoPhaseOilWaterModelAD(g, rock, fluid, w, gravity=gravity)
+    st0 = model.initial_state(200 * BARSA, 0.2)
+    st0.pressure = 200 * BARSA + rng.normal(0, 2 * BARSA, nc)
+    st0.sW = rng.uniform(0.1, 0.8, nc)
+    st0.sW[::7] = 0.1
+    st0.qWs = np.array([2e-3, 1e-3, 0.0] + ([0.0] if crossflow else []))
+    st0.qOs = np.array([0.0, 0.0, -1.5e-3] + ([-1e-4] if crossflow else []))
+    st = st0.copy()
+    st.pressure = st0.pressure + rng.normal(0, 1 * BARSA, nc)
+    st.sW = np.clip(st0.sW + rng.normal(0, 0.05, nc), 0.0, 1.0)
+    st.sW[::5] = 0.1
+    st.sW[3::11] = 0.9
+    st.bhp = np.array([230 * BARSA, 225 * BARSA, 150 * BARSA] + ([200 * BARSA] if crossflow else []))
+    st.qWs = np.array([1.9e-3, 1.1e-3, -2e-4] + ([1e-5] if crossflow else []))
+    st.qOs = np.array([1e-6, 0.0, -1.2e-3] + ([-2e-4] if crossflow else []))
+    if crossflow:
+        c4 = w[3].cells
+        st.pressure[c4] = 200 * BARSA + np.linspace(-3, 3, c4.size) * BARSA
+    dt = 10 * DAY
+    cdp = model._compute_cdp_per_well(st0)
+    v = init_variables_adi(st.pressure, st.sW, st.qWs, st.qOs, st.bhp)
+    eqs = model.assemble(st0, *v, dt, cdp)
+    eq = combine_equations(*eqs)
+    J = eq.jac[0].tocsr()
+    conv = model._converged(eqs, dt, st)
+    save(name, dims=np.array(dims), phys=np.array(phys, float), perm=perm, poro=np.array(0.2),
+         gravity=np.array(float(gravity)), fluid_kind=np.array(fluid_kind),
+         p0=st0.pressure, sw0=st0.sW, qws0=st0.qWs, qos0=st0.qOs, bhp0=st0.bhp,
+         p=st.pressure, sw=st.sW, qws=st.qWs, qos=st.qOs, bhp=st.bhp, dt=np.array(dt),
+         cdp=np.concatenate(cdp) if cdp else np.zeros(0),
+         res=eq.val, J_data=J.data, J_indices=J.indices, J_indptr=J.indptr,
+         J_shape=np.array(J.shape), converged=np.array(conv),
+         T=model.ops.T, pv=model.pv, **wells_arrays("w", w))
+
+
+def newton_fixture(name, dims, phys, seed, fluid_kind, gravity, nsteps, dt_days):
+    g = compute_geometry(cart_grid(dims, phys))
+    perm = lognormal_perm(dims, seed)
+    rock = make_rock(g, perm[:, None], 0.2)
+    fluid = ow_fluid(fluid_kind)
+    nx, ny, nz = dims
+    col = lambda i, j: i + nx * (j + ny * np.arange(nz))
+    gvec = np.array([0, 0, gravity]) if gravity else None
+    pvtot = float(np.sum(0.2 * g.cells.volumes))
+    rate = 0.25 * pvtot / (nsteps * dt_days * DAY) / 2
+    w = add_well(None, g, rock, col(0, 0), well_type="rate", val=rate,
+                 compi=np.array([1.0, 0.0]), sign=1, gravity=gvec)
+    w = add_well(w, g, rock, col(nx - 1, 0), well_type="rate", val=rate,
+                 compi=np.array([1.0, 0.0]), sign=1, gravity=gvec)
+    w = add_well(w, g, rock, col(nx // 2, ny - 1), well_type="bhp", val=150 * BARSA,
+                 compi=np.array([0.0, 1.0]), sign=-1, gravity=gvec)
+    model = TwoPhaseOilWaterModelAD(g, rock, fluid, w, gravity=gravity)
+    st0 = model.initial_state(200 * BARSA, 0.1 if fluid_kind == "cfg" else 0.2)
+    states, its = simulate_schedule_ad(st0, model, np.full(nsteps, dt_days * DAY), verbose=False)
+    save(name, dims=np.array(dims), phys=np.array(phys, float), perm=perm, poro=np.array(0.2),
+         gravity=np.array(float(gravity)), fluid_kind=np.array(fluid_kind),
+         p0=st0.pressure, sw0=st0.sW, dt_days=np.array(float(dt_days)), nsteps=np.array(nsteps),
+         its=its, p_hist=np.vstack([s.pressure for s in states]),
+         sw_hist=np.vstack([s.sW for s in states]),
+         qws_hist=np.vstack([s.qWs for s in states]), qos_hist=np.vstack([s.qOs for s in states]),
+         bhp_hist=np.vstack([s.bhp for s in states]), **wells_arrays("w", w))
+
+
+def phase5_fixture():
+    """validate_phase5.py's case, run by the reference, with the MATLAB arrays."""
+    g = compute_geometry(cart_grid([15, 15, 1], [300.0, 300.0, 10.0]))
+    kvals = (50 + (11 * np.arange(g.cells.num)) % 200) * MILLI * DARCY
+    rock = make_rock(g, kvals[:, None], 0.25)
+    fluid = ow_fluid("p5")
+    w = add_well(None, g, rock, np.array([0]), well_type="rate", val=2e-3,
+                 compi=np.array([1.0, 0.0]), sign=1)
+    w = add_well(w, g, rock, np.array([g.cells.num - 1]), well_type="bhp",
+                 val=150 * BARSA, compi=np.array([0.0, 1.0]), sign=-1)
+    model = TwoPhaseOilWaterModelAD(g, rock, fluid, w)
+    st0 = model.initial_state(200 * BARSA, 0.2)
+    states, its = simulate_schedule_ad(st0, model, np.full(8, 30.0) * DAY, verbose=False)
+    m = scipy.io.loadmat(REF / "examples/validation/ref_p5_ow.mat", squeeze_me=True)
+    save("ow_phase5.npz", perm=kvals, its=its,
+         p_hist=np.vstack([s.pressure for s in states]), sw_hist=np.vstack([s.sW for s in states]),
+         qws_hist=np.vstack([s.qWs for s in states]), qos_hist=np.vstack([s.qOs for s in states]),
+         bhp_hist=np.vstack([s.bhp for s in states]),
+         mat_p_hist=np.asarray(m["p_hist"], float), mat_sw_hist=np.asarray(m["sw_hist"], float),
+         mat_qWs=np.asarray(m["qWs"], float), mat_qOs=np.asarray(m["qOs"], float),
+         mat_bhp=np.asarray(m["bhp"], float),
+         mat_WI=np.concatenate([np.atleast_1d(m["WI1"]), np.atleast_1d(m["WI2"])]).astype(float),
+         **wells_arrays("w", w))
+
+
+def incomp_fixtures():
+    """The MATLAB incompTPFA goldens (validate_phase2.py cases) as data, plus
+    the reference's own incomp_tpfa on a five-spot-like case with wells."""
+    out = {}
+    for case in ("qfs", "bc", "wells", "gravity"):
+        m = scipy.io.loadmat(REF / f"examples/validation/ref_p2_{case}.mat", squeeze_me=True)
+        for k, v in m.items():
+            if k.startswith("__"):
+                continue
+            out[f"{case}__{k}"] = np.atleast_1d(np.asarray(v, dtype=float))
+    save("incomp_matlab.npz", **out)
+
+    from pymrst.modules.incomp import incomp_tpfa, init_single_fluid
+    from pymrst.solvers import init_state
+    dims = [16, 16, 4]
+    g = compute_geometry(cart_grid(dims, [160.0, 160.0, 8.0]))
+    perm = lognormal_perm(dims, 0)
+    rock = make_rock(g, perm[:, None], 0.2)
+    ht = compute_trans(g, rock)
+    fl = init_single_fluid(1 * CENTI * POISE, 1000.0)
+    nx, ny, nz = dims
+    w = add_well(None, g, rock, 0 + nx * (0 + ny * np.arange(nz)), well_type="rate", val=1e-3,
+                 radius=0.1, compi=np.array([1.0]))
+    w = add_well(w, g, rock, (nx - 1) + nx * ((ny - 1) + ny * np.arange(nz)), well_type="bhp",
+                 val=100 * BARSA, radius=0.1, compi=np.array([1.0]))
+    st = incomp_tpfa(init_state(g, w, 0.0), g, ht, fl, wells=w)
+    save("incomp_wells.npz", dims=np.array(dims), perm=perm, hT=ht, p=st.pressure, flux=st.flux,
+         facePressure=st.facePressure, bhp=np.array([ws.pressure for ws in st.wellSol]),
+         wflux0=st.wellSol[0].flux, wflux1=st.wellSol[1].flux, **wells_arrays("w", w))
+
+
+if __name__ == "__main__":
+    grid_fixture()
+    assemble_fixture("ow_assemble_nograv.npz", [6, 5, 3], [60.0, 50.0, 6.0], 3, "p5", 0.0, False)
+    assemble_fixture("ow_assemble_grav.npz", [6, 5, 4], [60.0, 50.0, 8.0], 4, "cfg", 9.80665, False)
+    assemble_fixture("ow_assemble_xflow.npz", [5, 5, 6], [50.0, 50.0, 30.0], 5, "cfg", 9.80665, True)
+    newton_fixture("ow_newton_grav.npz", [8, 6, 4], [80.0, 60.0, 8.0], 6, "cfg", 9.80665, 4, 10.0)
+    newton_fixture("ow_newton_nograv.npz", [10, 8, 3], [100.0, 80.0, 6.0], 7, "p5", 0.0, 4, 20.0)
+    phase5_fixture()
+    incomp_fixtures()
