@@ -1,0 +1,180 @@
+/*
+ * pymrst_b200 — C-ABI of the B200 (sm_100a) TPFA flow hot path.
+ *
+ * Plain pointers and sizes only.  Pointers named d_* are device pointers
+ * (e.g. torch.Tensor.data_ptr() of CUDA tensors); h_* are host pointers.
+ * `stream` is a cudaStream_t passed as void* (0 = legacy default stream).
+ * Every entry point returns an int status (PMB_OK == 0) and never throws;
+ * pmb_last_error() gives the message of the last failure on the calling
+ * thread.  A handle is bound to the stream it was created with and is not
+ * thread-safe; distinct handles are independent.  The caller owns every
+ * d_* / h_* buffer it passes; handles own their internal workspaces and
+ * release them in the matching *_destroy.
+ *
+ * Vector layout of the oil-water system ("cell-major"): for cell c,
+ * x[2c] = pressure, x[2c+1] = water saturation; then for well k,
+ * x[2nc+3k+0] = qWs, +1 = qOs, +2 = bhp.  Residual rows use the same
+ * layout: water, oil per cell, then eq_w, eq_o, ctrl per well.  The
+ * reference assembles the same system in variable-blocked order
+ * (pymrst/utils/adi/operators.py:204-211); the Python layer permutes.
+ */
+#ifndef PYMRST_B200_H
+#define PYMRST_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PMB_OK = 0,
+  PMB_ERR_CUDA = 1,      /* CUDA runtime error */
+  PMB_ERR_ARG = 2,       /* invalid argument / unsupported input */
+  PMB_ERR_NONFINITE = 3, /* NaN or Inf in a residual, update or Krylov scalar */
+  PMB_ERR_PIVOT = 4,     /* zero pivot in a block inverse or coarse solve */
+  PMB_ERR_NOCONV = 5,    /* Krylov solver did not reach its tolerance */
+  PMB_ERR_ALLOC = 6,     /* device or host allocation failed */
+  PMB_ERR_INTERNAL = 7
+};
+
+const char* pmb_last_error(void);
+int pmb_version(void);
+
+/* ------------------------------------------------------------------------
+ * Transmissibilities.
+ * pmb_compute_trans replaces compute_trans (pymrst/solvers/compute_trans.py:11-53):
+ * one-sided T = (c . K n) / (c . c) per half-face, c = face centroid - cell
+ * centroid, n the face normal oriented out of the cell, K the full 3x3
+ * tensor given row-major per cell (perm9, nc x 9), then |T| where
+ * fix_negative != 0, then the net-to-gross multiplier (ntg and half_tag may
+ * be NULL; half-faces with tag // 2 == 2 keep 1).
+ * pmb_face_trans replaces get_face_transmissibility
+ * (pymrst/solvers/get_face_transmissibility.py:12-31): T_f = 1 / sum 1/T_hf
+ * over the half-faces of face f, listed CSR-style by hf_ptr/hf_idx.
+ */
+int pmb_compute_trans(int64_t n_half, const int32_t* d_cell_no, const int32_t* d_half_face,
+                      const int32_t* d_face_first_cell, const double* d_cell_centroid,
+                      const double* d_face_centroid, const double* d_face_normal,
+                      const double* d_perm9, const double* d_ntg, const int32_t* d_half_tag,
+                      int32_t fix_negative, double* d_t_half, void* stream);
+int pmb_face_trans(int64_t nf, const int32_t* d_hf_ptr, const int32_t* d_hf_idx,
+                   const double* d_t_half, double* d_t_face, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Oil-water fully-implicit model (TwoPhaseOilWaterModelAD,
+ * pymrst/modules/ad_blackoil/models/two_phase_oil_water_model.py:77-657).
+ */
+typedef struct pmb_ow pmb_ow;
+
+typedef struct pmb_ow_desc {
+  int32_t nc, nf, nw;
+  const int32_t* h_N;     /* nf x 2 internal neighbour pairs (N[:,0], N[:,1]) */
+  const double* h_T;      /* nf harmonic face transmissibilities */
+  const double* h_gdz;    /* nf gravity * (z[N1] - z[N0]) */
+  const double* h_pv;     /* nc pore volumes */
+  /* fluid (init_simple_adi_fluid.py:217-239), water then oil */
+  double mu[2], rhoS[2], n_exp[2], c[2], b0[2], sl[2], su[2], p_ref;
+  /* wells: perforations of well k are perf_ptr[k] .. perf_ptr[k+1]-1,
+   * in the well's top-to-bottom order */
+  const int32_t* h_perf_ptr; /* nw+1 */
+  const int32_t* h_perf_cell;
+  const double* h_perf_WI;
+  const double* h_perf_dZ;
+  const double* h_compi;     /* nw x 2 */
+  const int32_t* h_well_type; /* 0 = bhp, 1 = rate */
+  const double* h_well_val;
+  double gravity;
+  double tol_cnv, tol_mb, tol_well, ds_max, dp_max_rel;
+} pmb_ow_desc;
+
+int pmb_ow_create(const pmb_ow_desc* desc, void* stream, pmb_ow** out);
+int pmb_ow_destroy(pmb_ow* h);
+/* h_out8 = [nc, nf, nw, nperf, nnzb, nvec, well_part_len, ncolors] */
+int pmb_ow_sizes(const pmb_ow* h, int64_t* h_out8);
+/* Block-CSR pattern of the cell part: row_ptr (nc+1), col (nnzb), host. */
+int pmb_ow_pattern(const pmb_ow* h, int32_t* h_row_ptr, int32_t* h_col);
+
+/* Per-perforation wellbore pressure drop for a timestep starting at d_x0
+ * (_compute_cdp_per_well, two_phase_oil_water_model.py:205-284).  Uses and
+ * updates the handle's previous-step cdp, as the reference model does. */
+int pmb_ow_compute_cdp(pmb_ow* h, const double* d_x0, double* d_cdp);
+/* Forget the previous-step cdp (a fresh model). */
+int pmb_ow_reset_cdp(pmb_ow* h);
+
+/* Residual and Jacobian at d_x for the step from d_x0 over dt
+ * (assemble, two_phase_oil_water_model.py:493-546).  d_jac: nnzb 2x2
+ * blocks, row-major within a block; d_well: the well part
+ * (well_part_len doubles).  want_jac = 0 computes the residual only. */
+int pmb_ow_assemble(pmb_ow* h, const double* d_x, const double* d_x0, double dt,
+                    const double* d_cdp, double* d_res, double* d_jac, double* d_well,
+                    int32_t want_jac);
+/* y = J x with the full operator (cells, wells, mixture coupling). */
+int pmb_ow_spmv(pmb_ow* h, const double* d_jac, const double* d_well, const double* d_x,
+                double* d_y);
+/* Convergence values (_converged, two_phase_oil_water_model.py:549-567):
+ * h_out8 = [cnv, mb, max|eq_w|/q_ref, max|eq_o|/q_ref, ctrl_ok, converged,
+ *           nonfinite, 0]. */
+int pmb_ow_convergence(pmb_ow* h, const double* d_res, const double* d_x, double dt,
+                       double* h_out8);
+/* Newton update with the reference's limits (step, :641-651): dp clipped to
+ * dp_max_rel*|p|, ds to ds_max, sW to [0,1]; well unknowns unclipped.
+ * The increment applied is sign * d_dx. */
+int pmb_ow_update(pmb_ow* h, double* d_x, const double* d_dx, double sign);
+
+/* ------------------------------------------------------------------------
+ * CPR-preconditioned GMRES on the oil-water operator (replaces CPRSolver.solve,
+ * pymrst/modules/ad_core/solvers/linear_solvers.py:426-545).
+ */
+typedef struct pmb_cpr pmb_cpr;
+
+typedef struct pmb_cpr_opts {
+  double rtol;              /* relative residual target, ||b - A x|| <= rtol ||b|| */
+  int32_t maxiter;          /* total Krylov iterations */
+  int32_t restart;          /* GMRES restart length */
+  int32_t precision;        /* 0: FP64 throughout; 1: FP32 Krylov + preconditioner
+                               inside FP64 iterative refinement */
+  int32_t use_pressure_stage;
+  int32_t local_sweeps;     /* red-black block Gauss-Seidel sweeps of the second stage */
+  int32_t amg_smoother_degree; /* Chebyshev degree on each level */
+  int32_t amg_cycle;        /* 0: V-cycle, 1: K-cycle (Krylov-accelerated) */
+  double amg_theta;         /* strength threshold of pairwise aggregation */
+  int32_t amg_coarse_size;  /* stop coarsening at this many unknowns */
+  int32_t amg_rebuild_interval; /* re-aggregate after this many setups */
+  double inner_rtol;        /* mixed precision: FP32 inner solve target */
+} pmb_cpr_opts;
+
+int pmb_cpr_default_opts(pmb_cpr_opts* out);
+int pmb_cpr_create(pmb_ow* model, const pmb_cpr_opts* opts, pmb_cpr** out);
+int pmb_cpr_destroy(pmb_cpr* s);
+/* Build / refresh the preconditioner for the Jacobian (d_jac, d_well) at
+ * state d_x (quasi-IMPES weights 1/b at the mean pressure). */
+int pmb_cpr_setup(pmb_cpr* s, const double* d_jac, const double* d_well, const double* d_x);
+/* Solve J x = b from x = 0.  h_info4 = [iterations, relres, ok, setups].
+ * Returns PMB_ERR_NOCONV when the tolerance was not reached. */
+int pmb_cpr_solve(pmb_cpr* s, const double* d_b, double* d_x, double* h_info4);
+/* Unknowns per level of the current pressure hierarchy. */
+int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
+
+/* ------------------------------------------------------------------------
+ * One backward-Euler step solved by Newton on the device (step,
+ * two_phase_oil_water_model.py:605-657): d_x holds the state at the start
+ * of the step and receives the new state.  h_stats8 = [iterations,
+ * converged, krylov_iterations, setups, cnv, mb, nonfinite, 0].  Returns
+ * PMB_OK also when Newton did not converge (converged = 0); a linear-solver
+ * failure returns PMB_ERR_NOCONV with d_x restored to the start state. */
+int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_iterations,
+                double* h_stats8);
+
+/* Host-side aggregation of the AMG hierarchy for a CSR matrix (no device
+ * needed): unknowns per level into h_sizes (up to max_levels), count in
+ * *n_levels.  Exposed for testing the set-up logic. */
+int pmb_amg_hierarchy_host(int32_t n, const int32_t* h_row_ptr, const int32_t* h_col,
+                           const double* h_val, double theta, int32_t coarse_size,
+                           int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYMRST_B200_H */

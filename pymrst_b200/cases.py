@@ -1,0 +1,123 @@
+"""Seeded synthetic oil-water workloads of the benchmark shapes.
+
+The reference measures on its own examples and on SPE10; neither dataset is
+available here, so these generators stand in with the stated shapes, sizes and
+value distributions (all seeded with numpy's default_rng):
+
+* `five_spot(dims, cell_size, seed)`: lognormal permeability, log k ~
+  N(ln(100 mD), sigma) smoothed by a 3x3x3 box filter; porosity 0.2; four rate
+  water injectors at the corner columns (compi [1, 0]) and one BHP producer
+  (100 bar) at the centre column; initial p = 200 bar, sW = 0.1.
+* `channelised(dims=(60, 220, 85), cell_size=(6.1, 3.05, 0.61), seed)`: the
+  upper 35 layers smooth lognormal (sigma 1.5), the lower layers binary
+  sinusoidal channels (2000 mD in 1 mD) with amplitude, wavelength and width
+  drawn per layer; porosity 0.05 + 0.30 * normalised log-permeability; same
+  well pattern.
+* `ow_fluid()`: Corey n = 2 with Swc = Sor = 0.1, mu_w = 1 cP, mu_o = 5 cP,
+  rho 1000 / 800 kg/m^3, compressibility 1e-5 / bar for both phases,
+  p_ref = 200 bar.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import List
+
+import numpy as np
+
+from .grid import Grid, cartesian_grid, cell_index
+from .params import (BARSA, CENTI, DARCY, DAY, MILLI, POISE, Rock, SimpleFluid, Well,
+                     add_well, init_simple_adi_fluid, make_rock)
+
+MD = MILLI * DARCY
+
+
+@dataclass
+class OWCase:
+    name: str
+    grid: Grid
+    rock: Rock
+    fluid: SimpleFluid
+    wells: List[Well]
+    p0: float
+    sw0: float
+    dt: float
+    nsteps: int
+    gravity: float
+
+
+def ow_fluid() -> SimpleFluid:
+    return init_simple_adi_fluid(mu=np.array([1.0, 5.0]) * CENTI * POISE, rho=[1000.0, 800.0],
+                                 n=[2, 2], c=[1e-5 / BARSA, 1e-5 / BARSA], p_ref=200 * BARSA,
+                                 smin=[0.1, 0.1])
+
+
+def _box_smooth(a: np.ndarray) -> np.ndarray:
+    """3x3x3 box filter with 'nearest' edges."""
+    from scipy.ndimage import uniform_filter
+    return uniform_filter(a, size=3, mode="nearest")
+
+
+def lognormal_logperm(dims, rng, sigma=1.0, mean_md=100.0) -> np.ndarray:
+    return _box_smooth(rng.normal(np.log(mean_md), sigma, size=tuple(dims)))
+
+
+def _five_spot_wells(g: Grid, rock: Rock, rate: float, bhp: float, gravity: float):
+    nx, ny, nz = g.cartDims
+    k = np.arange(nz)
+    gvec = np.array([0.0, 0.0, gravity]) if gravity else None
+    wells = None
+    for (i, j) in ((0, 0), (nx - 1, 0), (0, ny - 1), (nx - 1, ny - 1)):
+        wells = add_well(wells, g, rock, cell_index(g, i, j, k), well_type="rate", val=rate,
+                         compi=np.array([1.0, 0.0]), sign=1, gravity=gvec)
+    wells = add_well(wells, g, rock, cell_index(g, nx // 2, ny // 2, k), well_type="bhp",
+                     val=bhp, compi=np.array([0.0, 1.0]), sign=-1, gravity=gvec)
+    return wells
+
+
+def five_spot(dims=(100, 100, 10), cell_size=(10.0, 10.0, 2.0), seed=1, sigma=1.0,
+              nsteps=20, dt_days=10.0, gravity=9.80665, pv_fraction=0.25) -> OWCase:
+    rng = np.random.default_rng(seed)
+    dims = tuple(int(v) for v in dims)
+    g = cartesian_grid(dims, [d * s for d, s in zip(dims, cell_size)])
+    logk = lognormal_logperm(dims, rng, sigma)
+    perm = np.exp(logk).ravel(order="F") * MD
+    rock = make_rock(g, perm[:, None], 0.2)
+    pvtot = float(np.sum(rock.poro * g.cells.volumes))
+    rate = pv_fraction * pvtot / (nsteps * dt_days * DAY) / 4.0
+    wells = _five_spot_wells(g, rock, rate, 100 * BARSA, gravity)
+    return OWCase(f"five_spot_{dims[0]}x{dims[1]}x{dims[2]}", g, rock, ow_fluid(), wells,
+                  200 * BARSA, 0.1, dt_days * DAY, nsteps, gravity)
+
+
+def channelised(dims=(60, 220, 85), cell_size=(6.1, 3.05, 0.61), seed=2, n_smooth=35,
+                nsteps=20, dt_days=10.0, gravity=9.80665, pv_fraction=0.25) -> OWCase:
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = (int(v) for v in dims)
+    g = cartesian_grid((nx, ny, nz), [nx * cell_size[0], ny * cell_size[1], nz * cell_size[2]])
+    logk = np.empty((nx, ny, nz))
+    top = min(n_smooth, nz)
+    if top:
+        logk[:, :, :top] = lognormal_logperm((nx, ny, top), rng, sigma=1.5)
+    xs = np.arange(nx)[:, None]
+    ys = np.arange(ny)[None, :]
+    for k in range(top, nz):
+        mask = np.zeros((nx, ny), dtype=bool)
+        for _ in range(int(rng.integers(2, 5))):
+            amp = rng.uniform(2.0, 0.2 * nx)
+            wav = rng.uniform(0.3 * ny, 1.5 * ny)
+            wid = rng.uniform(2.0, 0.12 * nx)
+            x0 = rng.uniform(0, nx)
+            ph = rng.uniform(0, 2 * np.pi)
+            centre = x0 + amp * np.sin(2 * np.pi * ys / wav + ph)
+            mask |= np.abs(xs - centre) <= 0.5 * wid
+        logk[:, :, k] = np.where(mask, np.log(2000.0), np.log(1.0))
+    perm = np.exp(logk).ravel(order="F") * MD
+    lk = logk.ravel(order="F")
+    poro = 0.05 + 0.30 * (lk - lk.min()) / max(lk.max() - lk.min(), 1e-300)
+    rock = make_rock(g, perm[:, None], poro)
+    pvtot = float(np.sum(rock.poro * g.cells.volumes))
+    rate = pv_fraction * pvtot / (nsteps * dt_days * DAY) / 4.0
+    wells = _five_spot_wells(g, rock, rate, 100 * BARSA, gravity)
+    return OWCase(f"channelised_{nx}x{ny}x{nz}", g, rock, ow_fluid(), wells,
+                  200 * BARSA, 0.1, dt_days * DAY, nsteps, gravity)

@@ -1,0 +1,121 @@
+// Oil-water model: device data layout and the host class owning it.
+#pragma once
+
+#include "pmb_common.cuh"
+
+namespace pmb {
+
+struct FluidDev {
+  double mu_inv[2], rhoS[2], n[2], c[2], b0[2], sl[2], inv_range[2], p_ref;
+  int plain[2];  // kr = s^n without end-point scaling
+};
+
+// Well part of the Jacobian, one contiguous buffer of doubles:
+//   Bp[nperf][2][3]  d(cell rows water, oil of the perforated cell) / d(qWs, qOs, bhp)
+//   Cp[nperf][2][2]  d(eq_w, eq_o) / d(p, sW of the perforated cell)
+//   Up[nperf][2][2]  cell rows of perf i  <-  mixture (mix_w, mix_o) of its well
+//   Vp[nperf][2][2]  d(mix_w, mix_o) / d(p, sW of perf cell j)
+//   D [nw][3][3]     well rows / well unknowns
+//   M [nw]           1.0 where the mixture coupling is active (not a dead well)
+// The cell-cell coupling through the mixture, d cell_i / d cell_j = Up_i Vp_j
+// for perforations i, j of one well, is kept in this rank-2 form.
+struct WellLayout {
+  int64_t B, C, U, V, D, M, total;
+  static WellLayout make(int nperf, int nw) {
+    WellLayout l;
+    l.B = 0;
+    l.C = l.B + 6LL * nperf;
+    l.U = l.C + 4LL * nperf;
+    l.V = l.U + 4LL * nperf;
+    l.D = l.V + 4LL * nperf;
+    l.M = l.D + 9LL * nw;
+    l.total = l.M + nw;
+    return l;
+  }
+};
+
+// Read-only view passed to kernels by value.
+struct OWView {
+  int nc, nf, nw, nperf;
+  const int* row_ptr;    // nc+1
+  const int* col;        // nnzb
+  const int* nz_face;    // nnzb: f if the row cell is N[f,0], -(f+1) if N[f,1]; diagonal: INT_MIN
+  const int* diag_pos;   // nc
+  const double* T;       // nf
+  const double* gdz;     // nf
+  const double* pv;      // nc
+  FluidDev fl;
+  // wells
+  const int* perf_ptr;   // nw+1
+  const int* perf_cell;  // nperf
+  const double* perf_WI;
+  const int* well_type;  // 0 bhp, 1 rate
+  const double* well_val;
+  const double* compi;   // nw*2
+  const double* perf_dZ;
+  const int* perf_well;  // nperf
+  // perforated cells: unique cells pcell[0..npc), perfs of pcell q are
+  // pc_perf[pc_ptr[q] .. pc_ptr[q+1])
+  int npc;
+  const int* pcell;
+  const int* pc_ptr;
+  const int* pc_perf;
+  const int* cell_pc;    // nc: index into pcell, or -1
+  WellLayout wl;
+  double gravity;
+  double q_ref;
+  double tol_cnv, tol_mb, tol_well, ds_max, dp_max_rel;
+};
+
+class OWModel {
+ public:
+  OWModel(const pmb_ow_desc& d, cudaStream_t s);
+  OWView view() const { return v_; }
+  cudaStream_t stream() const { return stream_; }
+  int nc() const { return v_.nc; }
+  int nw() const { return v_.nw; }
+  int nperf() const { return v_.nperf; }
+  int64_t nnzb() const { return nnzb_; }
+  int64_t nvec() const { return 2LL * v_.nc + 3LL * v_.nw; }
+  int ncolors() const { return ncolors_; }
+  const std::vector<int>& h_row_ptr() const { return h_row_ptr_; }
+  const std::vector<int>& h_col() const { return h_col_; }
+  const std::vector<int>& h_color_ptr() const { return h_color_ptr_; }
+  const int* color_cells() const { return color_cells_.get(); }
+
+  void compute_cdp(const double* x0, double* cdp);
+  void reset_cdp() { have_last_cdp_ = false; }
+  void assemble(const double* x, const double* x0, double dt, const double* cdp, double* res,
+                double* jac, double* well, bool want_jac);
+  void spmv(const double* jac, const double* well, const double* x, double* y);
+  // Device-side convergence values into d_out (8 doubles); no sync.
+  void convergence_async(const double* res, const double* x, double dt, double* d_out);
+  // x += sgn * dx with the reference update limits
+  void update(double* x, const double* dx, double sgn = 1.0);
+
+  // internal buffers
+  double* jac() { return jac_.get(); }
+  double* well() { return well_.get(); }
+  double* res() { return res_.get(); }
+  double* cdp() { return cdp_.get(); }
+  double* x0() { return x0_.get(); }
+  double* dx() { return dx_.get(); }
+  double* conv_out() { return conv_out_.get(); }
+
+ private:
+  cudaStream_t stream_;
+  OWView v_{};
+  int64_t nnzb_ = 0;
+  int ncolors_ = 0;
+  std::vector<int> h_row_ptr_, h_col_, h_color_ptr_;
+  DArray<int> row_ptr_, col_, nz_face_, diag_pos_, perf_ptr_, perf_cell_, well_type_, perf_well_;
+  DArray<int> pcell_, pc_ptr_, pc_perf_, color_cells_, cell_pc_;
+  DArray<double> T_, gdz_, pv_, perf_WI_, perf_dZ_, well_val_, compi_;
+  // scratch / state
+  DArray<double> pf_cq_, pf_dloc_, last_cdp_, conv_part_, conv_out_;
+  DArray<double> jac_, well_, res_, cdp_, x0_, dx_;
+  bool have_last_cdp_ = false;
+  double pv_tot_ = 0.0;
+};
+
+}  // namespace pmb
