@@ -1,0 +1,467 @@
+// Aggregation AMG: host aggregation, device Galerkin refresh, Chebyshev
+// smoothing, V-cycle, dense coarsest solve.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "pmb_amg.cuh"
+
+namespace pmb {
+
+// ---------------------------------------------------------------------------
+// host: pairwise aggregation and Galerkin structure
+// ---------------------------------------------------------------------------
+
+// Greedy pairwise matching: each unmatched unknown i (in order) is paired
+// with its strongest unmatched neighbour j, strength s_ij = -a_ij, among
+// those with s_ij >= theta * max_k s_ik; otherwise it stays alone.
+static int pairwise_match(int n, const int* rp, const int* ci, const double* v, double theta,
+                          std::vector<int>& agg) {
+  agg.assign(n, -1);
+  int na = 0;
+  for (int i = 0; i < n; ++i) {
+    if (agg[i] >= 0) continue;
+    double mx = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k)
+      if (ci[k] != i) mx = std::max(mx, -v[k]);
+    int best = -1;
+    double bv = -1.0;
+    if (mx > 0.0) {
+      for (int k = rp[i]; k < rp[i + 1]; ++k) {
+        const int j = ci[k];
+        if (j == i || agg[j] >= 0) continue;
+        const double s = -v[k];
+        if (s >= theta * mx && s > bv) { bv = s; best = j; }
+      }
+    }
+    agg[i] = na;
+    if (best >= 0) agg[best] = na;
+    ++na;
+  }
+  return na;
+}
+
+struct HostCSR {
+  int n = 0;
+  std::vector<int> rp, ci;
+  std::vector<double> v;
+};
+
+// Coarse pattern of P^T A P for aggregation `agg` (n -> nc) and, for every
+// coarse entry, the fine entries that sum into it (in increasing order).
+static void galerkin_structure(int n, const int* rp, const int* ci, const std::vector<int>& agg, int nc,
+                               std::vector<int>& crp, std::vector<int>& cci, std::vector<int>& gptr,
+                               std::vector<int>& gidx, std::vector<int>& cptr, std::vector<int>& cmem) {
+  cptr.assign(nc + 1, 0);
+  for (int i = 0; i < n; ++i) ++cptr[agg[i] + 1];
+  for (int I = 0; I < nc; ++I) cptr[I + 1] += cptr[I];
+  cmem.assign(n, 0);
+  {
+    std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+    for (int i = 0; i < n; ++i) cmem[fill[agg[i]]++] = i;
+  }
+  crp.assign(nc + 1, 0);
+  cci.clear();
+  std::vector<std::pair<int, int>> ent;      // (coarse col, fine nnz)
+  std::vector<std::pair<int, int>> all_map;  // (coarse nnz, fine nnz)
+  all_map.reserve(rp[n]);
+  for (int I = 0; I < nc; ++I) {
+    ent.clear();
+    for (int m = cptr[I]; m < cptr[I + 1]; ++m) {
+      const int i = cmem[m];
+      for (int k = rp[i]; k < rp[i + 1]; ++k) ent.emplace_back(agg[ci[k]], k);
+    }
+    std::sort(ent.begin(), ent.end());
+    for (size_t e = 0; e < ent.size(); ++e) {
+      if (e == 0 || ent[e].first != ent[e - 1].first) cci.push_back(ent[e].first);
+      all_map.emplace_back((int)cci.size() - 1, ent[e].second);
+    }
+    crp[I + 1] = (int)cci.size();
+  }
+  const int nnzc = (int)cci.size();
+  gptr.assign(nnzc + 1, 0);
+  for (auto& p : all_map) ++gptr[p.first + 1];
+  for (int K = 0; K < nnzc; ++K) gptr[K + 1] += gptr[K];
+  gidx.assign(all_map.size(), 0);
+  std::vector<int> fill(gptr.begin(), gptr.end() - 1);
+  for (auto& p : all_map) gidx[fill[p.first]++] = p.second;
+}
+
+static void galerkin_values(const std::vector<int>& gptr, const std::vector<int>& gidx,
+                            const std::vector<double>& fv, std::vector<double>& cv) {
+  const int nnzc = (int)gptr.size() - 1;
+  cv.assign(nnzc, 0.0);
+  for (int K = 0; K < nnzc; ++K) {
+    double s = 0.0;
+    for (int g = gptr[K]; g < gptr[K + 1]; ++g) s += fv[gidx[g]];
+    cv[K] = s;
+  }
+}
+
+std::vector<AMGHostLevel> amg_build_hierarchy(int n, const int* row_ptr, const int* col,
+                                              const double* val, double theta, int passes,
+                                              int coarse_size, int max_levels) {
+  std::vector<AMGHostLevel> out;
+  HostCSR cur;
+  cur.n = n;
+  cur.rp.assign(row_ptr, row_ptr + n + 1);
+  cur.ci.assign(col, col + row_ptr[n]);
+  cur.v.assign(val, val + row_ptr[n]);
+  while (cur.n > coarse_size && (int)out.size() < max_levels) {
+    std::vector<int> agg(cur.n);
+    std::iota(agg.begin(), agg.end(), 0);
+    int na = cur.n;
+    HostCSR work = cur;
+    for (int p = 0; p < passes; ++p) {
+      std::vector<int> a2;
+      int na2 = pairwise_match(work.n, work.rp.data(), work.ci.data(), work.v.data(), theta, a2);
+      if (na2 > 0.7 * work.n)
+        na2 = pairwise_match(work.n, work.rp.data(), work.ci.data(), work.v.data(), 0.0, a2);
+      for (int i = 0; i < cur.n; ++i) agg[i] = a2[agg[i]];
+      na = na2;
+      if (p + 1 < passes) {
+        HostCSR next;
+        std::vector<int> gp, gi, cp, cm;
+        galerkin_structure(work.n, work.rp.data(), work.ci.data(), a2, na2, next.rp, next.ci, gp, gi, cp, cm);
+        next.n = na2;
+        galerkin_values(gp, gi, work.v, next.v);
+        work = std::move(next);
+      }
+    }
+    if (na >= 0.95 * cur.n) break;  // coarsening stalled
+    AMGHostLevel L;
+    L.n = cur.n;
+    L.row_ptr = cur.rp;
+    L.col = cur.ci;
+    L.agg = agg;
+    HostCSR next;
+    galerkin_structure(cur.n, cur.rp.data(), cur.ci.data(), agg, na, next.rp, next.ci, L.gptr, L.gidx,
+                       L.cptr, L.cmem);
+    next.n = na;
+    galerkin_values(L.gptr, L.gidx, cur.v, next.v);
+    out.push_back(std::move(L));
+    cur = std::move(next);
+  }
+  AMGHostLevel last;
+  last.n = cur.n;
+  last.row_ptr = cur.rp;
+  last.col = cur.ci;
+  out.push_back(std::move(last));
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// device kernels
+// ---------------------------------------------------------------------------
+
+// Inverse diagonal and the Gershgorin bound max_i sum_j |a_ij| / |a_ii| of
+// D^{-1} A (positive doubles order like their bit patterns, so the maximum
+// is an integer atomicMax and independent of the order of arrival).
+template <class T>
+__global__ void diag_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                            const T* __restrict__ a, T* __restrict__ dinv,
+                            unsigned long long* __restrict__ lmax_bits, int* status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double d = 0.0, s = 0.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) {
+    const double v = (double)a[k];
+    s += fabs(v);
+    if (ci[k] == i) d = v;
+  }
+  if (d == 0.0 || !isfinite(d)) {
+    atomicExch(status, PMB_ERR_PIVOT);
+    d = 1.0;
+  }
+  dinv[i] = (T)(1.0 / d);
+  const double g = s / fabs(d);
+  atomicMax(lmax_bits, (unsigned long long)__double_as_longlong(g));
+}
+
+__global__ void lmax_from_bits(const unsigned long long* bits, double* lmax) {
+  lmax[0] = __longlong_as_double((long long)bits[0]);
+}
+
+template <class T>
+__global__ void galerkin_kernel(int nnzc, const int* __restrict__ gptr, const int* __restrict__ gidx,
+                                const T* __restrict__ fv, T* __restrict__ cv) {
+  const int K = blockIdx.x * blockDim.x + threadIdx.x;
+  if (K >= nnzc) return;
+  double s = 0.0;
+  for (int g = gptr[K]; g < gptr[K + 1]; ++g) s += (double)fv[gidx[g]];
+  cv[K] = (T)s;
+}
+
+// Chebyshev on D^{-1} A over [lmax/10, lmax]: step `step` of the
+// three-term recurrence; x_out = x_in + d, d = c1 d + c2 D^{-1}(b - A x_in).
+template <class T, bool ZERO>
+__global__ void cheb_step_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                 const T* __restrict__ a, const T* __restrict__ dinv,
+                                 const T* __restrict__ b, const T* __restrict__ xin,
+                                 T* __restrict__ xout, T* __restrict__ d, const double* lmax, int step) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double lm = lmax[0];
+  const double lo = lm / 10.0;
+  const double theta = 0.5 * (lm + lo), delta = 0.5 * (lm - lo), sigma = theta / delta;
+  double rho = 1.0 / sigma, c1 = 0.0, c2 = 1.0 / theta;
+  for (int k = 1; k <= step; ++k) {
+    const double rho1 = 1.0 / (2.0 * sigma - rho);
+    c1 = rho1 * rho;
+    c2 = 2.0 * rho1 / delta;
+    rho = rho1;
+  }
+  double r = (double)b[i];
+  if (!ZERO) {
+    for (int k = rp[i]; k < rp[i + 1]; ++k) r -= (double)a[k] * (double)xin[ci[k]];
+  }
+  r *= (double)dinv[i];
+  const double dn = (step == 0 ? 0.0 : c1 * (double)d[i]) + c2 * r;
+  d[i] = (T)dn;
+  xout[i] = (T)((ZERO ? 0.0 : (double)xin[i]) + dn);
+}
+
+// b_c[I] = sum over members i of (b_i - (A x)_i)
+template <class T>
+__global__ void restrict_residual_kernel(int nc, const int* __restrict__ cptr, const int* __restrict__ cmem,
+                                         const int* __restrict__ rp, const int* __restrict__ ci,
+                                         const T* __restrict__ a, const T* __restrict__ b,
+                                         const T* __restrict__ x, T* __restrict__ bc) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nc) return;
+  double s = 0.0;
+  for (int m = cptr[I]; m < cptr[I + 1]; ++m) {
+    const int i = cmem[m];
+    double r = (double)b[i];
+    for (int k = rp[i]; k < rp[i + 1]; ++k) r -= (double)a[k] * (double)x[ci[k]];
+    s += r;
+  }
+  bc[I] = (T)s;
+}
+
+template <class T>
+__global__ void prolong_add_kernel(int n, const int* __restrict__ agg, const T* __restrict__ xc,
+                                   T* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = (T)((double)x[i] + (double)xc[agg[i]]);
+}
+
+template <class T>
+__global__ void copy_kernel(int n, const T* __restrict__ a, T* __restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = a[i];
+}
+
+// Dense coarsest level (FP64): assemble, invert by Gauss-Jordan with
+// partial pivoting in one CTA, apply as a dense product.
+template <class T>
+__global__ void dense_assemble_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                      const T* __restrict__ a, double* __restrict__ M) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int j = 0; j < n; ++j) M[(size_t)i * n + j] = 0.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) M[(size_t)i * n + ci[k]] = (double)a[k];
+}
+
+__global__ void gauss_jordan_kernel(int n, double* __restrict__ M, double* __restrict__ Inv,
+                                    int* __restrict__ status) {
+  __shared__ int piv;
+  __shared__ double pval;
+  const int t = threadIdx.x, nt = blockDim.x;
+  for (int idx = t; idx < n * n; idx += nt) Inv[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int c = 0; c < n; ++c) {
+    if (t == 0) {
+      int p = c;
+      double best = fabs(M[(size_t)c * n + c]);
+      for (int r = c + 1; r < n; ++r) {
+        const double v = fabs(M[(size_t)r * n + c]);
+        if (v > best) { best = v; p = r; }
+      }
+      piv = p;
+      pval = M[(size_t)p * n + c];
+      if (!(best > 0.0) || !isfinite(best)) atomicExch(status, PMB_ERR_PIVOT);
+    }
+    __syncthreads();
+    const int p = piv;
+    const double pv = (pval == 0.0 || !isfinite(pval)) ? 1.0 : pval;
+    if (p != c) {
+      for (int j = t; j < n; j += nt) {
+        const double a = M[(size_t)c * n + j];
+        M[(size_t)c * n + j] = M[(size_t)p * n + j];
+        M[(size_t)p * n + j] = a;
+        const double b = Inv[(size_t)c * n + j];
+        Inv[(size_t)c * n + j] = Inv[(size_t)p * n + j];
+        Inv[(size_t)p * n + j] = b;
+      }
+    }
+    __syncthreads();
+    for (int j = t; j < n; j += nt) {
+      M[(size_t)c * n + j] /= pv;
+      Inv[(size_t)c * n + j] /= pv;
+    }
+    __syncthreads();
+    // eliminate column c from every other row; M[r][c] is read, not written,
+    // in this pass, and updated with the Inv column afterwards
+    for (int idx = t; idx < n * n; idx += nt) {
+      const int r = idx / n, j = idx % n;
+      if (r == c || j == c) continue;
+      const double f = M[(size_t)r * n + c];
+      M[(size_t)r * n + j] -= f * M[(size_t)c * n + j];
+      Inv[(size_t)r * n + j] -= f * Inv[(size_t)c * n + j];
+    }
+    __syncthreads();
+    for (int r = t; r < n; r += nt) {
+      if (r == c) continue;
+      const double f = M[(size_t)r * n + c];
+      Inv[(size_t)r * n + c] -= f * Inv[(size_t)c * n + c];
+      M[(size_t)r * n + c] = 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+template <class T>
+__global__ void dense_apply_kernel(int n, const double* __restrict__ Inv, const T* __restrict__ b,
+                                   T* __restrict__ x) {
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int j = lane; j < n; j += 32) s += Inv[(size_t)row * n + j] * (double)b[j];
+  s = warp_sum(s);
+  if (lane == 0) x[row] = (T)s;
+}
+
+// ---------------------------------------------------------------------------
+// host class
+// ---------------------------------------------------------------------------
+
+template <class T>
+void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<int>& h_col,
+                   const int* d_row_ptr, const int* d_col, const std::vector<double>& h_val,
+                   double theta, int coarse_size, cudaStream_t s) {
+  auto H = amg_build_hierarchy(n, h_row_ptr.data(), h_col.data(), h_val.data(), theta, 2, coarse_size, 40);
+  levels_.clear();
+  levels_.resize(H.size() - 1);
+  for (size_t l = 0; l + 1 < H.size(); ++l) {
+    AMGLevel<T>& L = levels_[l];
+    const AMGHostLevel& h = H[l];
+    L.n = h.n;
+    L.nnz = (int)h.col.size();
+    if (l == 0) {
+      L.row_ptr = d_row_ptr;
+      L.col = d_col;
+    } else {
+      L.own_row_ptr.upload(h.row_ptr, s);
+      L.own_col.upload(h.col, s);
+      L.row_ptr = L.own_row_ptr.get();
+      L.col = L.own_col.get();
+    }
+    L.val.resize(L.nnz);
+    L.dinv.resize(L.n);
+    L.x.resize(L.n);
+    L.b.resize(L.n);
+    L.r.resize(L.n);
+    L.t.resize(L.n);
+    L.agg.upload(h.agg, s);
+    L.cptr.upload(h.cptr, s);
+    L.cmem.upload(h.cmem, s);
+    L.gptr.upload(h.gptr, s);
+    L.gidx.upload(h.gidx, s);
+    L.lmax.resize(1);
+  }
+  const AMGHostLevel& c = H.back();
+  nco_ = c.n;
+  PMB_REQUIRE(nco_ <= 4096, "coarsest AMG level too large for the dense solve");
+  if (levels_.empty()) {
+    // the whole matrix is the coarsest level: its pattern is the operator's
+    co_row_ptr_.upload(c.row_ptr, s);
+    co_col_.upload(c.col, s);
+  } else {
+    co_row_ptr_.upload(c.row_ptr, s);
+    co_col_.upload(c.col, s);
+  }
+  co_nnz_ = (int)c.col.size();
+  co_val_.resize(std::max(co_nnz_, 1));
+  co_dense_.resize((size_t)nco_ * nco_);
+  co_inv_.resize((size_t)nco_ * nco_);
+  co_x_.resize(nco_);
+  co_b_.resize(nco_);
+  bits_.resize(std::max<size_t>(levels_.size(), 1));
+  PMB_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class T>
+void AMG<T>::refresh(cudaStream_t s, int* d_status) {
+  for (size_t l = 0; l < levels_.size(); ++l) {
+    AMGLevel<T>& L = levels_[l];
+    PMB_CUDA(cudaMemsetAsync(bits_.get() + l, 0, sizeof(unsigned long long), s));
+    diag_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(),
+                                                       bits_.get() + l, d_status);
+    lmax_from_bits<<<1, 1, 0, s>>>(bits_.get() + l, L.lmax.get());
+    const bool last = (l + 1 == levels_.size());
+    T* cval = last ? co_val_.get() : levels_[l + 1].val.get();
+    const int nnzc = last ? co_nnz_ : levels_[l + 1].nnz;
+    galerkin_kernel<T><<<grid_for(nnzc, 256), 256, 0, s>>>(nnzc, L.gptr.get(), L.gidx.get(), L.val.get(), cval);
+    PMB_CHECK_LAUNCH();
+  }
+  dense_assemble_kernel<T><<<grid_for(nco_, 128), 128, 0, s>>>(nco_, co_row_ptr_.get(), co_col_.get(),
+                                                                co_val_.get(), co_dense_.get());
+  gauss_jordan_kernel<<<1, 1024, 0, s>>>(nco_, co_dense_.get(), co_inv_.get(), d_status);
+  PMB_CHECK_LAUNCH();
+}
+
+template <class T>
+void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start) {
+  // ping-pong between x and L.t; the result ends in x
+  const int g = grid_for(L.n, 256);
+  T* cur = x;
+  T* nxt = L.t.get();
+  int step = 0;
+  if (zero_start) {
+    cheb_step_kernel<T, true><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, nullptr,
+                                                cur, L.r.get(), L.lmax.get(), 0);
+    step = 1;
+  }
+  for (; step < degree; ++step) {
+    cheb_step_kernel<T, false><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, cur,
+                                                 nxt, L.r.get(), L.lmax.get(), step);
+    std::swap(cur, nxt);
+  }
+  if (cur != x) copy_kernel<T><<<g, 256, 0, s>>>(L.n, cur, x);
+  PMB_CHECK_LAUNCH();
+}
+
+template <class T>
+void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
+  if (l == (int)levels_.size()) {
+    dense_apply_kernel<T><<<grid_for(32LL * nco_, 256), 256, 0, s>>>(nco_, co_inv_.get(), b, x);
+    PMB_CHECK_LAUNCH();
+    return;
+  }
+  AMGLevel<T>& L = levels_[l];
+  const bool next_is_coarsest = (l + 1 == (int)levels_.size());
+  const int nc = next_is_coarsest ? nco_ : levels_[l + 1].n;
+  T* bc = next_is_coarsest ? co_b_.get() : levels_[l + 1].b.get();
+  T* xc = next_is_coarsest ? co_x_.get() : levels_[l + 1].x.get();
+  smooth(L, b, x, s, true);
+  restrict_residual_kernel<T><<<grid_for(nc, 256), 256, 0, s>>>(nc, L.cptr.get(), L.cmem.get(), L.row_ptr,
+                                                                 L.col, L.val.get(), b, x, bc);
+  PMB_CHECK_LAUNCH();
+  cycle(l + 1, bc, xc, s);
+  prolong_add_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.agg.get(), xc, x);
+  PMB_CHECK_LAUNCH();
+  smooth(L, b, x, s, false);
+}
+
+template <class T>
+void AMG<T>::apply(const T* b, T* x, cudaStream_t s) {
+  cycle(0, b, x, s);
+}
+
+template class AMG<double>;
+template class AMG<float>;
+
+}  // namespace pmb

@@ -1,0 +1,318 @@
+// extern "C" entry points (include/pymrst_b200.h) and the device Newton step.
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "pmb_cpr.cuh"
+
+namespace pmb {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+void compute_trans(long long nh, const int* cell_no, const int* hface, const int* first_cell, const double* cc,
+                   const double* fc, const double* fn, const double* K9, const double* ntg, const int* tag,
+                   int fix_negative, double* out, cudaStream_t s);
+void face_trans(long long nf, const int* ptr, const int* idx, const double* th, double* tf, cudaStream_t s);
+
+static void require_aligned(const void* p, size_t a, const char* what) {
+  PMB_REQUIRE(p != nullptr, std::string(what) + " is NULL");
+  PMB_REQUIRE(reinterpret_cast<uintptr_t>(p) % a == 0,
+              std::string(what) + " must be " + std::to_string(a) + "-byte aligned");
+}
+
+}  // namespace pmb
+
+using namespace pmb;
+
+struct pmb_ow {
+  std::unique_ptr<OWModel> m;
+  PinnedArray<double> conv;
+};
+
+struct pmb_cpr {
+  pmb_ow* owner = nullptr;
+  std::unique_ptr<CPRSolver> s;
+};
+
+extern "C" {
+
+const char* pmb_last_error(void) { return g_last_error.c_str(); }
+
+int pmb_version(void) { return 1; }
+
+int pmb_compute_trans(int64_t n_half, const int32_t* d_cell_no, const int32_t* d_half_face,
+                      const int32_t* d_face_first_cell, const double* d_cell_centroid,
+                      const double* d_face_centroid, const double* d_face_normal, const double* d_perm9,
+                      const double* d_ntg, const int32_t* d_half_tag, int32_t fix_negative, double* d_t_half,
+                      void* stream) {
+  return guarded([&] {
+    PMB_REQUIRE(n_half >= 0, "negative half-face count");
+    if (n_half == 0) return;
+    PMB_REQUIRE(d_cell_no && d_half_face && d_face_first_cell && d_cell_centroid && d_face_centroid &&
+                    d_face_normal && d_perm9 && d_t_half,
+                "NULL argument");
+    compute_trans(n_half, d_cell_no, d_half_face, d_face_first_cell, d_cell_centroid, d_face_centroid,
+                  d_face_normal, d_perm9, d_ntg, d_half_tag, fix_negative, d_t_half, (cudaStream_t)stream);
+  });
+}
+
+int pmb_face_trans(int64_t nf, const int32_t* d_hf_ptr, const int32_t* d_hf_idx, const double* d_t_half,
+                   double* d_t_face, void* stream) {
+  return guarded([&] {
+    PMB_REQUIRE(nf >= 0, "negative face count");
+    if (nf == 0) return;
+    PMB_REQUIRE(d_hf_ptr && d_hf_idx && d_t_half && d_t_face, "NULL argument");
+    face_trans(nf, d_hf_ptr, d_hf_idx, d_t_half, d_t_face, (cudaStream_t)stream);
+  });
+}
+
+int pmb_ow_create(const pmb_ow_desc* desc, void* stream, pmb_ow** out) {
+  return guarded([&] {
+    PMB_REQUIRE(desc && out, "NULL argument");
+    *out = nullptr;
+    auto h = std::make_unique<pmb_ow>();
+    h->m = std::make_unique<OWModel>(*desc, (cudaStream_t)stream);
+    h->conv.resize(8);
+    *out = h.release();
+  });
+}
+
+int pmb_ow_destroy(pmb_ow* h) {
+  return guarded([&] { delete h; });
+}
+
+int pmb_ow_sizes(const pmb_ow* h, int64_t* out) {
+  return guarded([&] {
+    PMB_REQUIRE(h && out, "NULL argument");
+    const OWModel& m = *h->m;
+    const OWView v = m.view();
+    out[0] = v.nc; out[1] = v.nf; out[2] = v.nw; out[3] = v.nperf;
+    out[4] = m.nnzb(); out[5] = m.nvec(); out[6] = v.wl.total; out[7] = m.ncolors();
+  });
+}
+
+int pmb_ow_pattern(const pmb_ow* h, int32_t* row_ptr, int32_t* col) {
+  return guarded([&] {
+    PMB_REQUIRE(h && row_ptr && col, "NULL argument");
+    const auto& rp = h->m->h_row_ptr();
+    const auto& cc = h->m->h_col();
+    std::memcpy(row_ptr, rp.data(), rp.size() * sizeof(int32_t));
+    std::memcpy(col, cc.data(), cc.size() * sizeof(int32_t));
+  });
+}
+
+int pmb_ow_compute_cdp(pmb_ow* h, const double* d_x0, double* d_cdp) {
+  return guarded([&] {
+    PMB_REQUIRE(h, "NULL handle");
+    require_aligned(d_x0, 16, "x0");
+    if (h->m->nperf() == 0) return;
+    PMB_REQUIRE(d_cdp, "cdp is NULL");
+    h->m->compute_cdp(d_x0, d_cdp);
+  });
+}
+
+int pmb_ow_reset_cdp(pmb_ow* h) {
+  return guarded([&] {
+    PMB_REQUIRE(h, "NULL handle");
+    h->m->reset_cdp();
+  });
+}
+
+int pmb_ow_assemble(pmb_ow* h, const double* d_x, const double* d_x0, double dt, const double* d_cdp,
+                    double* d_res, double* d_jac, double* d_well, int32_t want_jac) {
+  return guarded([&] {
+    PMB_REQUIRE(h, "NULL handle");
+    PMB_REQUIRE(dt > 0.0, "dt must be positive");
+    require_aligned(d_x, 16, "x");
+    require_aligned(d_x0, 16, "x0");
+    require_aligned(d_res, 16, "res");
+    if (want_jac) {
+      require_aligned(d_jac, 32, "jac");
+      PMB_REQUIRE(d_well, "well part is NULL");
+    }
+    PMB_REQUIRE(h->m->nperf() == 0 || d_cdp, "cdp is NULL");
+    h->m->assemble(d_x, d_x0, dt, d_cdp, d_res, d_jac, d_well, want_jac != 0);
+  });
+}
+
+int pmb_ow_spmv(pmb_ow* h, const double* d_jac, const double* d_well, const double* d_x, double* d_y) {
+  return guarded([&] {
+    PMB_REQUIRE(h, "NULL handle");
+    require_aligned(d_jac, 32, "jac");
+    require_aligned(d_x, 16, "x");
+    require_aligned(d_y, 16, "y");
+    PMB_REQUIRE(d_well, "well part is NULL");
+    PMB_REQUIRE(d_x != d_y, "x and y must not alias");
+    h->m->spmv(d_jac, d_well, d_x, d_y);
+  });
+}
+
+int pmb_ow_convergence(pmb_ow* h, const double* d_res, const double* d_x, double dt, double* out8) {
+  return guarded([&] {
+    PMB_REQUIRE(h && out8, "NULL argument");
+    require_aligned(d_res, 16, "res");
+    require_aligned(d_x, 16, "x");
+    OWModel& m = *h->m;
+    m.convergence_async(d_res, d_x, dt, m.conv_out());
+    PMB_CUDA(cudaMemcpyAsync(h->conv.get(), m.conv_out(), 8 * sizeof(double), cudaMemcpyDeviceToHost, m.stream()));
+    PMB_CUDA(cudaStreamSynchronize(m.stream()));
+    for (int i = 0; i < 8; ++i) out8[i] = h->conv[i];
+  });
+}
+
+int pmb_ow_update(pmb_ow* h, double* d_x, const double* d_dx, double sign) {
+  return guarded([&] {
+    PMB_REQUIRE(h, "NULL handle");
+    require_aligned(d_x, 16, "x");
+    require_aligned(d_dx, 16, "dx");
+    h->m->update(d_x, d_dx, sign);
+  });
+}
+
+int pmb_cpr_default_opts(pmb_cpr_opts* o) {
+  return guarded([&] {
+    PMB_REQUIRE(o, "NULL argument");
+    o->rtol = 1e-8;
+    o->maxiter = 200;
+    o->restart = 50;
+    o->precision = 0;
+    o->use_pressure_stage = 1;
+    o->local_sweeps = 2;
+    o->amg_smoother_degree = 2;
+    o->amg_cycle = 0;
+    o->amg_theta = 0.25;
+    o->amg_coarse_size = 200;
+    o->amg_rebuild_interval = 8;
+    o->inner_rtol = 1e-4;
+  });
+}
+
+int pmb_cpr_create(pmb_ow* model, const pmb_cpr_opts* opts, pmb_cpr** out) {
+  return guarded([&] {
+    PMB_REQUIRE(model && opts && out, "NULL argument");
+    *out = nullptr;
+    auto s = std::make_unique<pmb_cpr>();
+    s->owner = model;
+    s->s = std::make_unique<CPRSolver>(*model->m, *opts);
+    *out = s.release();
+  });
+}
+
+int pmb_cpr_destroy(pmb_cpr* s) {
+  return guarded([&] { delete s; });
+}
+
+int pmb_cpr_setup(pmb_cpr* s, const double* d_jac, const double* d_well, const double* d_x) {
+  return guarded([&] {
+    PMB_REQUIRE(s, "NULL handle");
+    require_aligned(d_jac, 32, "jac");
+    require_aligned(d_x, 16, "x");
+    PMB_REQUIRE(d_well, "well part is NULL");
+    s->s->setup(d_jac, d_well, d_x);
+  });
+}
+
+int pmb_cpr_solve(pmb_cpr* s, const double* d_b, double* d_x, double* info4) {
+  int rc = guarded([&] {
+    PMB_REQUIRE(s && info4, "NULL argument");
+    require_aligned(d_b, 16, "b");
+    require_aligned(d_x, 16, "x");
+    PMB_REQUIRE(d_b != d_x, "b and x must not alias");
+    if (!s->s->solve(d_b, d_x, info4))
+      throw Error(PMB_ERR_NOCONV, "CPR-GMRES did not reach its tolerance (relres " +
+                                      std::to_string(info4[1]) + " after " +
+                                      std::to_string((long long)info4[0]) + " iterations)");
+  });
+  return rc;
+}
+
+int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* sizes, int32_t* n_levels) {
+  return guarded([&] {
+    PMB_REQUIRE(s && sizes && n_levels, "NULL argument");
+    const int nl = s->s->num_levels();
+    *n_levels = nl;
+    for (int l = 0; l < nl && l < max_levels; ++l) sizes[l] = s->s->level_size(l);
+  });
+}
+
+int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_iterations, double* stats) {
+  return guarded([&] {
+    PMB_REQUIRE(h && s && stats, "NULL argument");
+    PMB_REQUIRE(s->owner == h, "solver belongs to another model");
+    PMB_REQUIRE(dt > 0.0, "dt must be positive");
+    PMB_REQUIRE(max_iterations >= 0, "negative iteration limit");
+    require_aligned(d_x, 16, "x");
+    OWModel& m = *h->m;
+    CPRSolver& cpr = *s->s;
+    cudaStream_t st = m.stream();
+    const long long n = m.nvec();
+    for (int i = 0; i < 8; ++i) stats[i] = 0.0;
+    PMB_CUDA(cudaMemcpyAsync(m.x0(), d_x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    m.compute_cdp(m.x0(), m.cdp());
+    double krylov = 0.0;
+    auto evaluate = [&](bool want_jac) {
+      m.assemble(d_x, m.x0(), dt, m.cdp(), m.res(), m.jac(), m.well(), want_jac);
+      m.convergence_async(m.res(), d_x, dt, m.conv_out());
+      PMB_CUDA(cudaMemcpyAsync(h->conv.get(), m.conv_out(), 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      PMB_CUDA(cudaStreamSynchronize(st));
+    };
+    for (int it = 0; it < max_iterations; ++it) {
+      evaluate(true);
+      stats[4] = h->conv[0];
+      stats[5] = h->conv[1];
+      stats[6] = h->conv[6];
+      if (h->conv[5] != 0.0) {
+        stats[0] = it;
+        stats[1] = 1.0;
+        stats[2] = krylov;
+        stats[3] = (double)cpr.setups();
+        return;
+      }
+      if (h->conv[6] != 0.0) break;  // non-finite residual: the step fails
+      cpr.setup(m.jac(), m.well(), d_x);
+      double info[4];
+      const bool ok = cpr.solve(m.res(), m.dx(), info);
+      krylov += info[0];
+      if (!ok) {
+        PMB_CUDA(cudaMemcpyAsync(d_x, m.x0(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        PMB_CUDA(cudaStreamSynchronize(st));
+        stats[0] = it;
+        stats[2] = krylov;
+        stats[3] = (double)cpr.setups();
+        throw Error(PMB_ERR_NOCONV, "CPR-GMRES did not converge in Newton iteration " + std::to_string(it) +
+                                        " (relres " + std::to_string(info[1]) + ")");
+      }
+      m.update(d_x, m.dx(), -1.0);
+    }
+    if (h->conv[6] == 0.0) evaluate(false);
+    stats[0] = max_iterations;
+    stats[1] = h->conv[5] != 0.0 ? 1.0 : 0.0;
+    stats[2] = krylov;
+    stats[3] = (double)cpr.setups();
+    stats[4] = h->conv[0];
+    stats[5] = h->conv[1];
+    stats[6] = h->conv[6];
+  });
+}
+
+int pmb_amg_hierarchy_host(int32_t n, const int32_t* row_ptr, const int32_t* col, const double* val,
+                           double theta, int32_t coarse_size, int32_t max_levels, int64_t* sizes,
+                           int32_t* n_levels) {
+  return guarded([&] {
+    PMB_REQUIRE(n > 0 && row_ptr && col && val && sizes && n_levels, "invalid argument");
+    auto H = amg_build_hierarchy(n, row_ptr, col, val, theta, 2, coarse_size, 40);
+    *n_levels = (int)H.size();
+    for (int l = 0; l < (int)H.size() && l < max_levels; ++l) sizes[l] = H[l].n;
+    // consistency of every level's aggregation and Galerkin map
+    for (size_t l = 0; l + 1 < H.size(); ++l) {
+      const AMGHostLevel& L = H[l];
+      const int nc = H[l + 1].n;
+      for (int a : L.agg) PMB_REQUIRE(a >= 0 && a < nc, "aggregate index out of range");
+      PMB_REQUIRE((int)L.cmem.size() == L.n, "aggregates do not partition the unknowns");
+      PMB_REQUIRE((int)L.gidx.size() == (int)L.col.size(), "Galerkin map does not cover every entry");
+    }
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+// Aggregation AMG for the CPR pressure system.
+//
+// Set-up splits in two.  Aggregation (which fine unknowns form a coarse
+// unknown) runs in C++ on the host from the current matrix values and is
+// kept for several Newton iterations.  Every refresh then recomputes all
+// coarse operators on the device from the new fine values: plain
+// (unsmoothed) aggregation makes the Galerkin product P^T A P a pure sum of
+// fine entries, done as a gather over precomputed index lists, so the whole
+// hierarchy is exact for the current matrix without a sparse triple product.
+#pragma once
+
+#include "pmb_common.cuh"
+
+namespace pmb {
+
+struct AMGHostLevel {
+  int n = 0;
+  std::vector<int> row_ptr, col;      // pattern of this level's matrix
+  std::vector<int> agg;               // fine unknown -> coarse unknown (next level)
+  std::vector<int> cptr, cmem;        // members of each coarse unknown
+  std::vector<int> gptr, gidx;        // coarse nnz <- fine nnz indices
+};
+
+// Pairwise aggregation hierarchy from a CSR matrix (host).  `passes`
+// successive pairwise matchings form one level (aggregates of up to
+// 2^passes); a matching whose coarsening ratio is poor at threshold `theta`
+// is redone with theta = 0.  The last entry is the coarsest level (no agg).
+std::vector<AMGHostLevel> amg_build_hierarchy(int n, const int* row_ptr, const int* col,
+                                              const double* val, double theta, int passes,
+                                              int coarse_size, int max_levels);
+
+template <class T>
+struct AMGLevel {
+  int n = 0, nnz = 0;
+  const int* row_ptr = nullptr;  // device (level 0 borrows the operator pattern)
+  const int* col = nullptr;
+  DArray<int> own_row_ptr, own_col;
+  DArray<T> val, dinv, x, b, r, t;
+  DArray<int> agg, cptr, cmem, gptr, gidx;
+  DArray<double> lmax;  // Chebyshev upper bound (device scalar)
+};
+
+template <class T>
+class AMG {
+ public:
+  // Build aggregation from host values of the level-0 matrix (pattern given
+  // both on host and device).
+  void build(int n, const std::vector<int>& h_row_ptr, const std::vector<int>& h_col,
+             const int* d_row_ptr, const int* d_col, const std::vector<double>& h_val, double theta,
+             int coarse_size, cudaStream_t s);
+  // Refresh all levels from level-0 values already written to level0_val().
+  void refresh(cudaStream_t s, int* d_status);
+  // x = M^{-1} b with one V-cycle.
+  void apply(const T* b, T* x, cudaStream_t s);
+  T* level0_val() { return levels_.empty() ? co_val_.get() : levels_[0].val.get(); }
+  bool built() const { return nco_ > 0; }
+  int num_levels() const { return (int)levels_.size() + (nco_ > 0 ? 1 : 0); }
+  int level_size(int l) const { return l < (int)levels_.size() ? levels_[l].n : nco_; }
+  int degree = 2;
+
+ private:
+  void cycle(int l, const T* b, T* x, cudaStream_t s);
+  void smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start);
+  std::vector<AMGLevel<T>> levels_;
+  // coarsest level: dense inverse in FP64
+  int nco_ = 0, co_nnz_ = 0;
+  DArray<int> co_row_ptr_, co_col_;
+  DArray<T> co_val_;
+  DArray<double> co_dense_, co_inv_;
+  DArray<T> co_x_, co_b_;
+  DArray<unsigned long long> bits_;
+};
+
+}  // namespace pmb

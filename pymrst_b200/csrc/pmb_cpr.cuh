@@ -1,0 +1,45 @@
+// CPR-preconditioned flexible GMRES on the oil-water operator.
+#pragma once
+
+#include "pmb_amg.cuh"
+#include "pmb_ow.cuh"
+
+namespace pmb {
+
+class CPRSolver {
+ public:
+  CPRSolver(OWModel& m, const pmb_cpr_opts& o);
+  void setup(const double* jac, const double* well, const double* x);
+  // Returns true when converged; info = [iterations, relres, ok, setups].
+  bool solve(const double* b, double* x, double* info);
+  const pmb_cpr_opts& opts() const { return o_; }
+  int num_levels() const { return amg_.num_levels(); }
+  int level_size(int l) const { return amg_.level_size(l); }
+  long long setups() const { return setups_; }
+  long long total_iterations() const { return total_its_; }
+
+ private:
+  void precond(const double* r, double* z);
+  void local_stage(const double* r, double* z);
+  void check_status();
+  double norm(const double* v);
+
+  OWModel& m_;
+  pmb_cpr_opts o_;
+  cudaStream_t s_;
+  const double* jac_ = nullptr;
+  const double* well_ = nullptr;
+  AMG<double> amg_;
+  int since_build_ = 0;
+  long long setups_ = 0, total_its_ = 0;
+  DArray<double> w_;        // quasi-IMPES weights (2)
+  DArray<double> part_;     // reduction partials
+  DArray<int> status_;
+  DArray<double> bp_, xp_, ap_;  // pressure system rhs / solution / values for aggregation
+  DArray<double> V_, Z_, wv_, r_, hcol_, htmp_, y_;
+  PinnedArray<double> h_pin_;
+  PinnedArray<int> st_pin_;
+  std::vector<double> h_ap_;
+};
+
+}  // namespace pmb
