@@ -40,6 +40,8 @@ enum {
 
 const char* pmb_last_error(void);
 int pmb_version(void);
+/* Number of kernels this library has launched in the process so far. */
+int pmb_launch_count(int64_t* h_out);
 
 /* ------------------------------------------------------------------------
  * Transmissibilities.

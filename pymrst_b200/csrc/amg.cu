@@ -400,7 +400,9 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
     PMB_CUDA(cudaMemsetAsync(bits_.get() + l, 0, sizeof(unsigned long long), s));
     diag_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(),
                                                        bits_.get() + l, d_status);
+    PMB_CHECK_LAUNCH();
     lmax_from_bits<<<1, 1, 0, s>>>(bits_.get() + l, L.lmax.get());
+    PMB_CHECK_LAUNCH();
     const bool last = (l + 1 == levels_.size());
     T* cval = last ? co_val_.get() : levels_[l + 1].val.get();
     const int nnzc = last ? co_nnz_ : levels_[l + 1].nnz;
@@ -409,6 +411,7 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
   }
   dense_assemble_kernel<T><<<grid_for(nco_, 128), 128, 0, s>>>(nco_, co_row_ptr_.get(), co_col_.get(),
                                                                 co_val_.get(), co_dense_.get());
+  PMB_CHECK_LAUNCH();
   gauss_jordan_kernel<<<1, 1024, 0, s>>>(nco_, co_dense_.get(), co_inv_.get(), d_status);
   PMB_CHECK_LAUNCH();
 }
@@ -423,15 +426,19 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
   if (zero_start) {
     cheb_step_kernel<T, true><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, nullptr,
                                                 cur, L.r.get(), L.lmax.get(), 0);
+    PMB_CHECK_LAUNCH();
     step = 1;
   }
   for (; step < degree; ++step) {
     cheb_step_kernel<T, false><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, cur,
                                                  nxt, L.r.get(), L.lmax.get(), step);
+    PMB_CHECK_LAUNCH();
     std::swap(cur, nxt);
   }
-  if (cur != x) copy_kernel<T><<<g, 256, 0, s>>>(L.n, cur, x);
-  PMB_CHECK_LAUNCH();
+  if (cur != x) {
+    copy_kernel<T><<<g, 256, 0, s>>>(L.n, cur, x);
+    PMB_CHECK_LAUNCH();
+  }
 }
 
 template <class T>

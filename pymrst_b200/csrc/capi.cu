@@ -1,4 +1,5 @@
 // extern "C" entry points (include/pymrst_b200.h) and the device Newton step.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -9,6 +10,9 @@ namespace pmb {
 
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void compute_trans(long long nh, const int* cell_no, const int* hface, const int* first_cell, const double* cc,
                    const double* fc, const double* fn, const double* K9, const double* ntg, const int* tag,
@@ -40,6 +44,13 @@ extern "C" {
 const char* pmb_last_error(void) { return g_last_error.c_str(); }
 
 int pmb_version(void) { return 1; }
+
+int pmb_launch_count(int64_t* out) {
+  return guarded([&] {
+    PMB_REQUIRE(out, "NULL argument");
+    *out = g_launches.load();
+  });
+}
 
 int pmb_compute_trans(int64_t n_half, const int32_t* d_cell_no, const int32_t* d_half_face,
                       const int32_t* d_face_first_cell, const double* d_cell_centroid,

@@ -232,6 +232,9 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   PMB_REQUIRE(o_.precision == 0, "precision must be 0 (FP64)");
   const long long n = m.nvec();
   const int mm = o_.restart;
+  // Krylov vectors are stored with a stride padded to 32 doubles so that every
+  // slice V_j / Z_j stays 256-byte aligned for the double2 / double4 kernels.
+  ld_ = (n + 31) / 32 * 32;
   w_.resize(2);
   part_.resize((size_t)kRedBlocks * (mm + 2));
   status_.resize(1);
@@ -239,8 +242,8 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   bp_.resize(m.nc());
   xp_.resize(m.nc());
   ap_.resize(m.nnzb());
-  V_.resize((size_t)(mm + 1) * n);
-  Z_.resize((size_t)mm * n);
+  V_.resize((size_t)(mm + 1) * ld_);
+  Z_.resize((size_t)mm * ld_);
   wv_.resize(n);
   r_.resize(n);
   hcol_.resize(mm + 2);
@@ -272,6 +275,7 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
   ++setups_;
   if (!o_.use_pressure_stage) return;
   psum_kernel<<<kRedBlocks, 256, 0, s_>>>(v.nc, reinterpret_cast<const double2*>(x), part_.get());
+  PMB_CHECK_LAUNCH();
   weights_kernel<<<1, 32, 0, s_>>>(v, kRedBlocks, part_.get(), w_.get());
   PMB_CHECK_LAUNCH();
   const long long nnzb = m_.nnzb();
@@ -304,9 +308,12 @@ void CPRSolver::local_stage(const double* r, double* z) {
       if (cnt <= 0) continue;
       gs_color_kernel<<<grid_for(cnt, 256), 256, 0, s_>>>(v, cp[q], cp[q + 1], m_.color_cells(), A, well_, r, z,
                                                           status_.get());
+      PMB_CHECK_LAUNCH();
     }
-    if (v.nw) gs_well_kernel<<<1, 128, 0, s_>>>(v, well_, r, z);
-    PMB_CHECK_LAUNCH();
+    if (v.nw) {
+      gs_well_kernel<<<1, 128, 0, s_>>>(v, well_, r, z);
+      PMB_CHECK_LAUNCH();
+    }
   }
 }
 
@@ -316,18 +323,21 @@ void CPRSolver::precond(const double* r, double* z) {
   if (o_.use_pressure_stage) {
     restrict_p_kernel<<<grid_for(v.nc, 256), 256, 0, s_>>>(v.nc, reinterpret_cast<const double2*>(r), w_.get(),
                                                            bp_.get());
+    PMB_CHECK_LAUNCH();
     amg_.apply(bp_.get(), xp_.get(), s_);
     prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, xp_.get(), z);
+    PMB_CHECK_LAUNCH();
   } else {
     prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, nullptr, z);
+    PMB_CHECK_LAUNCH();
   }
-  PMB_CHECK_LAUNCH();
   local_stage(r, z);
 }
 
 double CPRSolver::norm(const double* a) {
   const long long n = m_.nvec();
   mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, a, n, 1, a, part_.get());
+  PMB_CHECK_LAUNCH();
   mdot_final_kernel<<<1, 32, 0, s_>>>(1, kRedBlocks, part_.get(), htmp_.get(), nullptr, 1);
   PMB_CHECK_LAUNCH();
   PMB_CUDA(cudaMemcpyAsync(h_pin_.get(), htmp_.get(), sizeof(double), cudaMemcpyDeviceToHost, s_));
@@ -361,21 +371,29 @@ bool CPRSolver::solve(const double* b, double* x, double* info) {
     int j = 0;
     bool stop = false;
     for (; j < mm && !stop; ++j) {
-      double* vj = V_.get() + (size_t)j * n;
-      double* zj = Z_.get() + (size_t)j * n;
+      double* vj = V_.get() + (size_t)j * ld_;
+      double* zj = Z_.get() + (size_t)j * ld_;
       precond(vj, zj);
       m_.spmv(jac_, well_, zj, wv_.get());
       // classical Gram-Schmidt, twice
       const int nv = j + 1;
-      mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, V_.get(), n, nv, wv_.get(), part_.get());
+      mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, V_.get(), ld_, nv, wv_.get(), part_.get());
+      PMB_CHECK_LAUNCH();
       mdot_final_kernel<<<1, 64, 0, s_>>>(nv, kRedBlocks, part_.get(), hcol_.get(), nullptr, 0);
-      vupdate_kernel<<<gv, 256, 0, s_>>>(n, V_.get(), n, nv, hcol_.get(), wv_.get());
-      mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, V_.get(), n, nv, wv_.get(), part_.get());
+      PMB_CHECK_LAUNCH();
+      vupdate_kernel<<<gv, 256, 0, s_>>>(n, V_.get(), ld_, nv, hcol_.get(), wv_.get());
+      PMB_CHECK_LAUNCH();
+      mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, V_.get(), ld_, nv, wv_.get(), part_.get());
+      PMB_CHECK_LAUNCH();
       mdot_final_kernel<<<1, 64, 0, s_>>>(nv, kRedBlocks, part_.get(), htmp_.get(), hcol_.get(), 0);
-      vupdate_kernel<<<gv, 256, 0, s_>>>(n, V_.get(), n, nv, htmp_.get(), wv_.get());
+      PMB_CHECK_LAUNCH();
+      vupdate_kernel<<<gv, 256, 0, s_>>>(n, V_.get(), ld_, nv, htmp_.get(), wv_.get());
+      PMB_CHECK_LAUNCH();
       mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, wv_.get(), n, 1, wv_.get(), part_.get());
+      PMB_CHECK_LAUNCH();
       mdot_final_kernel<<<1, 32, 0, s_>>>(1, kRedBlocks, part_.get(), hcol_.get() + nv, nullptr, 1);
-      scale_kernel<<<gv, 256, 0, s_>>>(n, wv_.get(), hcol_.get() + nv, V_.get() + (size_t)(j + 1) * n);
+      PMB_CHECK_LAUNCH();
+      scale_kernel<<<gv, 256, 0, s_>>>(n, wv_.get(), hcol_.get() + nv, V_.get() + (size_t)(j + 1) * ld_);
       PMB_CHECK_LAUNCH();
       PMB_CUDA(cudaMemcpyAsync(h_pin_.get(), hcol_.get(), sizeof(double) * (nv + 1), cudaMemcpyDeviceToHost, s_));
       PMB_CUDA(cudaMemcpyAsync(st_pin_.get(), status_.get(), sizeof(int), cudaMemcpyDeviceToHost, s_));
@@ -410,7 +428,8 @@ bool CPRSolver::solve(const double* b, double* x, double* info) {
     }
     for (int i = 0; i < j; ++i) h_pin_[i] = y[i];
     PMB_CUDA(cudaMemcpyAsync(y_.get(), h_pin_.get(), sizeof(double) * j, cudaMemcpyHostToDevice, s_));
-    xupdate_kernel<<<gv, 256, 0, s_>>>(n, Z_.get(), n, j, y_.get(), x);
+    xupdate_kernel<<<gv, 256, 0, s_>>>(n, Z_.get(), ld_, j, y_.get(), x);
+    PMB_CHECK_LAUNCH();
     // true residual
     m_.spmv(jac_, well_, x, wv_.get());
     sub_kernel<<<gv, 256, 0, s_>>>(n, b, wv_.get(), r_.get());

@@ -30,7 +30,14 @@ struct Error : std::runtime_error {
                                            " (" + __FILE__ + ":" + std::to_string(__LINE__) + ")"); \
   } while (0)
 
-#define PMB_CHECK_LAUNCH() PMB_CUDA(cudaGetLastError())
+// Every kernel launch in this library is followed by exactly one
+// PMB_CHECK_LAUNCH(), which also counts it (pmb_launch_count).
+void count_launch();
+#define PMB_CHECK_LAUNCH()          \
+  do {                              \
+    ::pmb::count_launch();          \
+    PMB_CUDA(cudaGetLastError());   \
+  } while (0)
 
 #define PMB_REQUIRE(cond, msg)                                        \
   do {                                                                \

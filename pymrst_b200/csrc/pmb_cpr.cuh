@@ -31,6 +31,7 @@ class CPRSolver {
   const double* well_ = nullptr;
   AMG<double> amg_;
   int since_build_ = 0;
+  long long ld_ = 0;       // padded stride of the Krylov bases
   long long setups_ = 0, total_its_ = 0;
   DArray<double> w_;        // quasi-IMPES weights (2)
   DArray<double> part_;     // reduction partials
