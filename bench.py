@@ -1,0 +1,400 @@
+"""Benchmark: fully-implicit oil-water timesteps on the 1.12M-cell
+channelised model (60 x 220 x 85 cells of 6.1 x 3.05 x 0.61 m), metric
+cell-Newton-iterations/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One "step" is one backward-Euler timestep (10 days) solved by Newton with the
+device CPR-GMRES; consecutive steps continue the same schedule.  `value`
+counts cells x Newton iterations over the timed steps divided by the device
+time (CUDA events, max over ranks); `e2e` repeats the timed steps through the
+public `GpuOilWaterModel.step(state, dt)` with the state in pinned host memory
+copied in and out every step.  Under torchrun every rank runs its own replica
+(the single-model path does not shard), so N ranks do N times the work.
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+numpy/SuperLU oracle restatement) on the host cores, one bounded Newton-
+iteration sample per step, in one process per core.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-Newton-its/s FI oil-water 1.1M cells: mixed-prec CPR vs FP64 GPU vs CPU"
+UNIT = "cell*Newton-iterations/s"
+WORKLOAD = dict(name="channelised oil-water 60x220x85 (1,122,000 cells), 10-day steps",
+                dims=(60, 220, 85), cell_size=(6.1, 3.05, 0.61))
+# Bounded CPU sample of the same model family: the channelised generator at
+# 18 x 66 x 25 cells (29,700 cells, the full model's aspect ratios), first
+# Newton iterations of the first timestep, SuperLU direct solve as the
+# reference's default linear solver.  A smaller sample favours the CPU
+# (direct-solve cost grows faster than linearly).
+CPU_SAMPLE = dict(dims=(18, 66, 25), cell_size=(6.1 * 60 / 18, 3.05 * 220 / 66, 0.61 * 85 / 25))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--dims", default=None, help="override grid dims, e.g. 30,110,40")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle samples
+# ---------------------------------------------------------------------------
+
+def cpu_sample_worker(budget: float, seed: int = 2):
+    """Newton iterations of the reference algorithm (oracle) on the CPU
+    sample, until `budget` seconds are used; returns (cells, its, seconds)."""
+    import scipy.sparse.linalg as spla
+    from oracle import ow as oow
+    from pymrst_b200 import cases
+    case = cases.channelised(dims=CPU_SAMPLE["dims"], cell_size=CPU_SAMPLE["cell_size"], seed=seed,
+                             n_smooth=int(round(CPU_SAMPLE["dims"][2] * 35 / 85)))
+    prob = oow.build_problem(case.grid, case.rock, case.fluid.params, case.wells, gravity=case.gravity)
+    st0 = oow.initial_state(prob, case.p0, case.sw0)
+    st = st0.copy()
+    cdp = oow.compute_cdp(prob, st0)
+    its = 0
+    t0 = time.perf_counter()
+    while True:
+        res, J = oow.assemble(prob, st0, st, case.dt, cdp)
+        oow.converged(prob, res, case.dt, st)
+        upd = spla.spsolve(J.tocsc(), -res)
+        oow.apply_update(prob, st, upd)
+        its += 1
+        el = time.perf_counter() - t0
+        if el >= budget or its >= 25:
+            return prob.nc, its, el
+
+
+def _pool_worker(args):
+    budget, seed = args
+    return cpu_sample_worker(budget, seed)
+
+
+def run_reference(args):
+    """The reference arm: the CPU algorithm on all host cores (one process
+    per core, each a bounded sample), rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    budget = max(2.0, args.cpu_budget / 2)
+    ctx = mp.get_context("spawn")
+    values = []
+    with ctx.Pool(cores) as pool:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            out = pool.map(_pool_worker, [(budget, 2 + j) for j in range(cores)])
+            wall = time.perf_counter() - t0
+            v = sum(nc * its for nc, its, _ in out) / wall
+            if i >= args.warmup:
+                values.append((v, wall))
+    v = float(np.mean([a for a, _ in values]))
+    ms = float(np.mean([b for _, b in values])) * 1e3
+    sample = (f"reference algorithm (numpy/SuperLU restatement) on the channelised generator at "
+              f"{'x'.join(map(str, CPU_SAMPLE['dims']))} cells, Newton iterations of the first "
+              f"10-day step for ~{budget:.0f} s per process, {cores} processes")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD["name"] + " (CPU runs a bounded sample)",
+                       "sample_cells": int(np.prod(CPU_SAMPLE["dims"]))},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True,
+                                         text=True, timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([s.strip() for s in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def kernel_roofline(model, x, x0, dt, torch, N, reps=20):
+    """Live per-launch timing of the assembly and operator kernels on the
+    current state, with their algorithmic bytes."""
+    nc, nw = model.nc, model.nw
+    nnzb = model.sizes["nnzb"]
+    nf = model.N.shape[0]
+    nvec = model.sizes["nvec"]
+    cdp = torch.as_tensor(np.concatenate([np.zeros(np.asarray(w.cells).size) for w in model.wells]),
+                          device="cuda")
+    res, jac, well = model.assemble_device(x, x0, dt, cdp, True)
+    y = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+    out = {}
+
+    def time_it(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e-3
+
+    # assembly: state (16 B) + previous state (16 B) + pv (8) + residual (16)
+    # per cell; T, gdz (16 B) per interface; row_ptr/col/face code/diag_pos
+    # indices (4 B each); the Jacobian blocks written (32 B each).
+    asm_bytes = nc * (16 + 16 + 8 + 16 + 4 + 4) + nf * 16 + nnzb * (32 + 4 + 4)
+    t = time_it(lambda: N.check(N.lib().pmb_ow_assemble(model._handle, N.ptr(x), N.ptr(x0), float(dt),
+                                                         N.ptr(cdp), N.ptr(res), N.ptr(jac), N.ptr(well), 1)))
+    out["assemble"] = dict(seconds=t, bytes=asm_bytes)
+    # operator application: blocks (32 B) + column index (4 B) per block,
+    # row_ptr, x read once, y written once
+    spmv_bytes = nnzb * 36 + (nc + 1) * 4 + nvec * 16
+    t = time_it(lambda: N.check(N.lib().pmb_ow_spmv(model._handle, N.ptr(jac), N.ptr(well), N.ptr(x), N.ptr(y))))
+    out["spmv"] = dict(seconds=t, bytes=spmv_bytes)
+    return out
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from pymrst_b200 import _native as N
+    from pymrst_b200 import cases
+    from pymrst_b200.build import build
+    from pymrst_b200.ow_model import GpuOilWaterModel
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if rank == 0:
+        build()
+    if world > 1:
+        dist.barrier()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # bounded CPU sample before any heavy GPU work (single process)
+        nc_s, its_s, el = cpu_sample_worker(args.cpu_budget)
+        cpu = {"value": nc_s * its_s / el, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": (f"reference algorithm (numpy/SuperLU restatement) on the channelised generator at "
+                          f"{'x'.join(map(str, CPU_SAMPLE['dims']))} = {nc_s} cells: {its_s} Newton "
+                          f"iterations of the first 10-day step in {el:.1f} s, one core")}
+
+    dims = tuple(int(v) for v in args.dims.split(",")) if args.dims else WORKLOAD["dims"]
+    n_smooth = int(round(dims[2] * 35 / 85))
+    case = cases.channelised(dims=dims, cell_size=WORKLOAD["cell_size"], n_smooth=n_smooth)
+    copts = dict(rtol=1e-8, maxiter=400, restart=50, amg_rebuild_interval=1_000_000,
+                 precision=1 if args.precision == "mixed" else 0)
+    model = GpuOilWaterModel(case.grid, case.rock, case.fluid, case.wells, gravity=case.gravity,
+                             cpr_options=copts)
+    stream = torch.cuda.current_stream()
+    x = model.to_device(model.initial_state(case.p0, case.sw0))
+    backup = x.clone()
+    dt = case.dt
+
+    def one_step(xv):
+        """One report step with the reference's halving cuts; returns
+        (Newton iterations, Krylov iterations, cuts)."""
+        t_local, its, kry, cuts, h = 0.0, 0, 0, 0, dt
+        while t_local < dt - 1e-12 * dt:
+            h = min(h, dt - t_local)
+            backup.copy_(xv)
+            ok, nit, st = model.step_device(xv, h)
+            its += nit
+            kry += int(st[2])
+            if ok:
+                t_local += h
+                h = min(2 * h, dt - t_local) if cuts else h
+            else:
+                xv.copy_(backup)
+                cuts += 1
+                if cuts > 6:
+                    raise RuntimeError("timestep failed after 6 cuts")
+                h /= 2
+        return its, kry, cuts
+
+    for _ in range(args.warmup):
+        one_step(x)
+    torch.cuda.synchronize()
+    x_e2e_start = x.clone()
+    l0 = N.launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    its_total = kry_total = cuts_total = 0
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            i, k, c = one_step(x)
+            its_total += i
+            kry_total += k
+            cuts_total += c
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = N.launch_count() - l0
+    sec = e0.elapsed_time(e1) * 1e-3
+    t = torch.tensor([sec, float(its_total) * model.nc], dtype=torch.float64, device="cuda")
+    if world > 1:
+        tmax = t[:1].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        work = t[1:].clone()
+        dist.all_reduce(work, op=dist.ReduceOp.SUM)
+        sec, cell_its = float(tmax.item()), float(work.item())
+    else:
+        cell_its = float(t[1].item())
+    value = cell_its / sec
+
+    # e2e: the same steps through the public host-state API (pinned copies in
+    # and out each step)
+    st_host = model.from_device(x_e2e_start)
+    model.step(st_host, dt)  # warm the staging buffers
+    st_host = model.from_device(x_e2e_start)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    its_e2e = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        # a report step through the public API (cuts handled like the driver)
+        t_local, h, cuts = 0.0, dt, 0
+        while t_local < dt - 1e-12 * dt:
+            h = min(h, dt - t_local)
+            new, ok, nit = model.step(st_host, h)
+            its_e2e += nit
+            if ok:
+                st_host = new
+                t_local += h
+                h = min(2 * h, dt - t_local) if cuts else h
+            else:
+                cuts += 1
+                h /= 2
+    torch.cuda.synchronize()
+    sec_e2e = time.perf_counter() - t0
+    te = torch.tensor([sec_e2e, float(its_e2e) * model.nc], dtype=torch.float64, device="cuda")
+    if world > 1:
+        a = te[:1].clone(); dist.all_reduce(a, op=dist.ReduceOp.MAX)
+        b = te[1:].clone(); dist.all_reduce(b, op=dist.ReduceOp.SUM)
+        sec_e2e, cell_its_e2e = float(a.item()), float(b.item())
+    else:
+        cell_its_e2e = float(te[1].item())
+    nvec_bytes = model.sizes["nvec"] * 8
+
+    kr = kernel_roofline(model, x, x_e2e_start, dt, torch, N)
+    peak, peak_kind = peaks()
+    ach = kr["spmv"]["bytes"] / kr["spmv"]["seconds"] / 1e9
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded channelised permeability, five-spot wells)",
+            "config": {"workload": WORKLOAD["name"], "cells": model.nc, "wells": model.nw,
+                       "dt_days": dt / 86400.0, "precision": args.precision,
+                       "newton_iterations": its_total, "krylov_iterations": kry_total, "cuts": cuts_total,
+                       "cpr": {k: copts[k] for k in copts}, "amg_levels": model.cpr_levels(),
+                       "l2": "inputs larger than L2 (Jacobian %.0f MB)" % (model.sizes['nnzb'] * 32 / 1e6),
+                       "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
+            "e2e": {"value": cell_its_e2e / sec_e2e, "unit": UNIT, "h2d_bytes_per_step": nvec_bytes,
+                    "d2h_bytes_per_step": nvec_bytes},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "bsr2_spmv_kernel + ow_well_spmv_kernel (pmb_ow_spmv)",
+                         "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "kernels": {k: {"ms": v["seconds"] * 1e3, "bytes": v["bytes"],
+                                         "GBps": v["bytes"] / v["seconds"] / 1e9} for k, v in kr.items()}},
+            "clocks": clocks.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

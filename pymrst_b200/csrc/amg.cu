@@ -264,7 +264,7 @@ __global__ void dense_assemble_kernel(int n, const int* __restrict__ rp, const i
   for (int k = rp[i]; k < rp[i + 1]; ++k) M[(size_t)i * n + ci[k]] = (double)a[k];
 }
 
-__global__ void gauss_jordan_kernel(int n, double* __restrict__ M, double* __restrict__ Inv,
+__global__ void __launch_bounds__(512) gauss_jordan_kernel(int n, double* __restrict__ M, double* __restrict__ Inv,
                                     int* __restrict__ status) {
   __shared__ int piv;
   __shared__ double pval;
@@ -412,7 +412,7 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
   dense_assemble_kernel<T><<<grid_for(nco_, 128), 128, 0, s>>>(nco_, co_row_ptr_.get(), co_col_.get(),
                                                                 co_val_.get(), co_dense_.get());
   PMB_CHECK_LAUNCH();
-  gauss_jordan_kernel<<<1, 1024, 0, s>>>(nco_, co_dense_.get(), co_inv_.get(), d_status);
+  gauss_jordan_kernel<<<1, 512, 0, s>>>(nco_, co_dense_.get(), co_inv_.get(), d_status);
   PMB_CHECK_LAUNCH();
 }
 

@@ -303,12 +303,27 @@ class GpuOilWaterModel:
         N.check(rc)
         return bool(stats[1]), int(stats[0]), list(stats)
 
+    def _staging(self):
+        """Pinned host buffer and device state buffer reused by `step`."""
+        if getattr(self, "_pin", None) is None:
+            torch = _torch()
+            n = self.sizes["nvec"]
+            self._pin = torch.empty(n, dtype=torch.float64, pin_memory=True)
+            self._xdev = torch.empty(n, dtype=torch.float64, device="cuda")
+        return self._pin, self._xdev
+
     def step(self, state: OWState, dt: float):
-        """One backward-Euler step (two_phase_oil_water_model.py:605-657)."""
-        x = self.to_device(state)
+        """One backward-Euler step (two_phase_oil_water_model.py:605-657):
+        the state goes to the device through a pinned buffer, the Newton loop
+        runs there, and the new state comes back the same way."""
+        pin, x = self._staging()
+        pin.numpy()[:] = self.pack(state)
+        x.copy_(pin, non_blocking=True)
         ok, its, stats = self.step_device(x, dt)
+        pin.copy_(x, non_blocking=True)
+        _torch().cuda.current_stream().synchronize()
         self.last_stats = stats
-        return self.from_device(x), ok, its
+        return self.unpack(pin.numpy().copy()), ok, its
 
     # -- assembly export (parity / protocol) ---------------------------------
     def compute_cdp(self, st0: OWState):
