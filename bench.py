@@ -230,6 +230,7 @@ def run_ours(args):
     from pymrst_b200 import cases
     from pymrst_b200.build import build
     from pymrst_b200.ow_model import GpuOilWaterModel
+    from pymrst_b200.replicas import reduce_timing
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -307,16 +308,13 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     launches = N.launch_count() - l0
-    sec = e0.elapsed_time(e1) * 1e-3
-    t = torch.tensor([sec, float(its_total) * model.nc], dtype=torch.float64, device="cuda")
-    if world > 1:
-        tmax = t[:1].clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        work = t[1:].clone()
-        dist.all_reduce(work, op=dist.ReduceOp.SUM)
-        sec, cell_its = float(tmax.item()), float(work.item())
-    else:
-        cell_its = float(t[1].item())
+    if os.environ.get("PMB_PROFILE") == "1" and rank == 0:
+        prof = N.profile_report(reset=True)
+        total = e0.elapsed_time(e1)
+        print(f"# timed region {total:.1f} ms; phases (total ms, count, ms each):", file=sys.stderr)
+        for k, (ms, cnt) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
+            print(f"#   {k:28s} {ms:10.2f} {cnt:7d} {ms / max(cnt, 1):9.4f}", file=sys.stderr)
+    sec, cell_its = reduce_timing(e0.elapsed_time(e1) * 1e-3, float(its_total) * model.nc)
     value = cell_its / sec
 
     # e2e: the same steps through the public host-state API (pinned copies in
@@ -344,14 +342,7 @@ def run_ours(args):
                 cuts += 1
                 h /= 2
     torch.cuda.synchronize()
-    sec_e2e = time.perf_counter() - t0
-    te = torch.tensor([sec_e2e, float(its_e2e) * model.nc], dtype=torch.float64, device="cuda")
-    if world > 1:
-        a = te[:1].clone(); dist.all_reduce(a, op=dist.ReduceOp.MAX)
-        b = te[1:].clone(); dist.all_reduce(b, op=dist.ReduceOp.SUM)
-        sec_e2e, cell_its_e2e = float(a.item()), float(b.item())
-    else:
-        cell_its_e2e = float(te[1].item())
+    sec_e2e, cell_its_e2e = reduce_timing(time.perf_counter() - t0, float(its_e2e) * model.nc)
     nvec_bytes = model.sizes["nvec"] * 8
 
     kr = kernel_roofline(model, x, x_e2e_start, dt, torch, N)

@@ -42,6 +42,9 @@ const char* pmb_last_error(void);
 int pmb_version(void);
 /* Number of kernels this library has launched in the process so far. */
 int pmb_launch_count(int64_t* h_out);
+/* Phase timings collected when the environment has PMB_PROFILE=1, as text
+ * lines "name total_ms count" (synchronises the device). */
+int pmb_profile_report(char* h_buf, int32_t len, int32_t reset);
 
 /* ------------------------------------------------------------------------
  * Transmissibilities.

@@ -53,6 +53,7 @@ SIGNATURES = {
     "pmb_last_error": (C.c_char_p, []),
     "pmb_version": (c_int, []),
     "pmb_launch_count": (c_int, [P_i64]),
+    "pmb_profile_report": (c_int, [C.c_char_p, c_int, c_int]),
     "pmb_compute_trans": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_vp, c_vp]),
     "pmb_face_trans": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_ow_create": (c_int, [C.POINTER(OWDesc), c_vp, C.POINTER(c_vp)]),
@@ -109,6 +110,17 @@ def launch_count() -> int:
     v = C.c_int64()
     check(lib().pmb_launch_count(C.byref(v)))
     return int(v.value)
+
+
+def profile_report(reset: bool = True) -> dict:
+    """{phase: (total_ms, count)} collected under PMB_PROFILE=1."""
+    buf = C.create_string_buffer(1 << 16)
+    check(lib().pmb_profile_report(buf, len(buf), int(reset)))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, ms, cnt = line.split()
+        out[name] = (float(ms), int(cnt))
+    return out
 
 
 def ptr(t) -> int:

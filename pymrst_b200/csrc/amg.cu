@@ -15,30 +15,59 @@ namespace pmb {
 // Greedy pairwise matching: each unmatched unknown i (in order) is paired
 // with its strongest unmatched neighbour j, strength s_ij = -a_ij, among
 // those with s_ij >= theta * max_k s_ik; otherwise it stays alone.
+// Rows without any negative coupling (possible after upwinding with gravity,
+// and on Galerkin coarse levels) use |a_ij| as strength instead.  With
+// `attach`, an unknown left alone joins the aggregate of its strongest
+// neighbour, so every connected unknown is coarsened.
 static int pairwise_match(int n, const int* rp, const int* ci, const double* v, double theta,
-                          std::vector<int>& agg) {
+                          std::vector<int>& agg, bool attach) {
   agg.assign(n, -1);
+  std::vector<int> alone;
   int na = 0;
   for (int i = 0; i < n; ++i) {
     if (agg[i] >= 0) continue;
     double mx = 0.0;
     for (int k = rp[i]; k < rp[i + 1]; ++k)
       if (ci[k] != i) mx = std::max(mx, -v[k]);
+    const bool use_abs = !(mx > 0.0);
+    if (use_abs)
+      for (int k = rp[i]; k < rp[i + 1]; ++k)
+        if (ci[k] != i) mx = std::max(mx, std::fabs(v[k]));
     int best = -1;
     double bv = -1.0;
     if (mx > 0.0) {
       for (int k = rp[i]; k < rp[i + 1]; ++k) {
         const int j = ci[k];
         if (j == i || agg[j] >= 0) continue;
-        const double s = -v[k];
+        const double s = use_abs ? std::fabs(v[k]) : -v[k];
         if (s >= theta * mx && s > bv) { bv = s; best = j; }
       }
     }
     agg[i] = na;
     if (best >= 0) agg[best] = na;
+    else alone.push_back(i);
     ++na;
   }
-  return na;
+  if (!attach || alone.empty()) return na;
+  // move singletons into a neighbour's aggregate, then renumber densely
+  for (int i : alone) {
+    int best = -1;
+    double bv = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      const int j = ci[k];
+      if (j == i) continue;
+      const double s = std::fabs(v[k]);
+      if (s > bv) { bv = s; best = j; }
+    }
+    if (best >= 0) agg[i] = agg[best];
+  }
+  std::vector<int> ren(na, -1);
+  int m = 0;
+  for (int i = 0; i < n; ++i) {
+    if (ren[agg[i]] < 0) ren[agg[i]] = m++;
+    agg[i] = ren[agg[i]];
+  }
+  return m;
 }
 
 struct HostCSR {
@@ -114,9 +143,9 @@ std::vector<AMGHostLevel> amg_build_hierarchy(int n, const int* row_ptr, const i
     HostCSR work = cur;
     for (int p = 0; p < passes; ++p) {
       std::vector<int> a2;
-      int na2 = pairwise_match(work.n, work.rp.data(), work.ci.data(), work.v.data(), theta, a2);
+      int na2 = pairwise_match(work.n, work.rp.data(), work.ci.data(), work.v.data(), theta, a2, false);
       if (na2 > 0.7 * work.n)
-        na2 = pairwise_match(work.n, work.rp.data(), work.ci.data(), work.v.data(), 0.0, a2);
+        na2 = pairwise_match(work.n, work.rp.data(), work.ci.data(), work.v.data(), 0.0, a2, true);
       for (int i = 0; i < cur.n; ++i) agg[i] = a2[agg[i]];
       na = na2;
       if (p + 1 < passes) {

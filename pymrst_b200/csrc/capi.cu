@@ -1,5 +1,8 @@
 // extern "C" entry points (include/pymrst_b200.h) and the device Newton step.
 #include <atomic>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -13,6 +16,60 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// ---- phase timers -----------------------------------------------------------
+struct PendingPhase {
+  std::string name;
+  cudaEvent_t e0, e1;
+};
+static std::mutex g_prof_mu;
+static std::vector<PendingPhase> g_pending;
+static std::map<std::string, std::pair<double, long long>> g_phase;  // ms, count
+
+static void collect_phases() {
+  std::vector<PendingPhase> keep;
+  for (auto& p : g_pending) {
+    if (cudaEventQuery(p.e1) == cudaSuccess) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p.e0, p.e1);
+      auto& a = g_phase[p.name];
+      a.first += ms;
+      a.second += 1;
+      cudaEventDestroy(p.e0);
+      cudaEventDestroy(p.e1);
+    } else {
+      keep.push_back(p);
+    }
+  }
+  g_pending.swap(keep);
+}
+
+bool PhaseTimer::enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("PMB_PROFILE");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+PhaseTimer::PhaseTimer(const char* name, cudaStream_t s) : name_(name), s_(s) {
+  if (!enabled()) return;
+  cudaEventCreate(&e0_);
+  cudaEventRecord(e0_, s_);
+}
+
+PhaseTimer::~PhaseTimer() {
+  if (!e0_) return;
+  cudaEvent_t e1;
+  cudaEventCreate(&e1);
+  cudaEventRecord(e1, s_);
+  std::lock_guard<std::mutex> g(g_prof_mu);
+  g_pending.push_back({name_, e0_, e1});
+  if (g_pending.size() > 4096) {
+    cudaEventSynchronize(e1);
+    collect_phases();
+  }
+}
 
 void compute_trans(long long nh, const int* cell_no, const int* hface, const int* first_cell, const double* cc,
                    const double* fc, const double* fn, const double* K9, const double* ntg, const int* tag,
@@ -44,6 +101,21 @@ extern "C" {
 const char* pmb_last_error(void) { return g_last_error.c_str(); }
 
 int pmb_version(void) { return 1; }
+
+int pmb_profile_report(char* buf, int32_t len, int32_t reset) {
+  return guarded([&] {
+    PMB_REQUIRE(buf && len > 0, "invalid buffer");
+    cudaDeviceSynchronize();
+    std::lock_guard<std::mutex> g(g_prof_mu);
+    collect_phases();
+    std::string s;
+    for (auto& kv : g_phase)
+      s += kv.first + " " + std::to_string(kv.second.first) + " " + std::to_string(kv.second.second) + "\n";
+    std::strncpy(buf, s.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
+    if (reset) g_phase.clear();
+  });
+}
 
 int pmb_launch_count(int64_t* out) {
   return guarded([&] {
@@ -263,7 +335,11 @@ int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_itera
     m.compute_cdp(m.x0(), m.cdp());
     double krylov = 0.0;
     auto evaluate = [&](bool want_jac) {
-      m.assemble(d_x, m.x0(), dt, m.cdp(), m.res(), m.jac(), m.well(), want_jac);
+      {
+        PhaseTimer pt("newton.assemble", st);
+        m.assemble(d_x, m.x0(), dt, m.cdp(), m.res(), m.jac(), m.well(), want_jac);
+      }
+      PhaseTimer pt("newton.convergence", st);
       m.convergence_async(m.res(), d_x, dt, m.conv_out());
       PMB_CUDA(cudaMemcpyAsync(h->conv.get(), m.conv_out(), 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
       PMB_CUDA(cudaStreamSynchronize(st));
@@ -281,9 +357,16 @@ int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_itera
         return;
       }
       if (h->conv[6] != 0.0) break;  // non-finite residual: the step fails
-      cpr.setup(m.jac(), m.well(), d_x);
+      {
+        PhaseTimer pt("newton.cpr_setup", st);
+        cpr.setup(m.jac(), m.well(), d_x);
+      }
       double info[4];
-      const bool ok = cpr.solve(m.res(), m.dx(), info);
+      bool ok;
+      {
+        PhaseTimer pt("newton.cpr_solve", st);
+        ok = cpr.solve(m.res(), m.dx(), info);
+      }
       krylov += info[0];
       if (!ok) {
         PMB_CUDA(cudaMemcpyAsync(d_x, m.x0(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));

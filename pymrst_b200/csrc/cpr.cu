@@ -324,13 +324,17 @@ void CPRSolver::precond(const double* r, double* z) {
     restrict_p_kernel<<<grid_for(v.nc, 256), 256, 0, s_>>>(v.nc, reinterpret_cast<const double2*>(r), w_.get(),
                                                            bp_.get());
     PMB_CHECK_LAUNCH();
-    amg_.apply(bp_.get(), xp_.get(), s_);
+    {
+      PhaseTimer pt("cpr.amg_cycle", s_);
+      amg_.apply(bp_.get(), xp_.get(), s_);
+    }
     prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, xp_.get(), z);
     PMB_CHECK_LAUNCH();
   } else {
     prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, nullptr, z);
     PMB_CHECK_LAUNCH();
   }
+  PhaseTimer pt("cpr.local_stage", s_);
   local_stage(r, z);
 }
 
@@ -374,9 +378,13 @@ bool CPRSolver::solve(const double* b, double* x, double* info) {
       double* vj = V_.get() + (size_t)j * ld_;
       double* zj = Z_.get() + (size_t)j * ld_;
       precond(vj, zj);
-      m_.spmv(jac_, well_, zj, wv_.get());
+      {
+        PhaseTimer pt("gmres.spmv", s_);
+        m_.spmv(jac_, well_, zj, wv_.get());
+      }
       // classical Gram-Schmidt, twice
       const int nv = j + 1;
+      PhaseTimer pt_orth("gmres.orthogonalise", s_);
       mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, V_.get(), ld_, nv, wv_.get(), part_.get());
       PMB_CHECK_LAUNCH();
       mdot_final_kernel<<<1, 64, 0, s_>>>(nv, kRedBlocks, part_.get(), hcol_.get(), nullptr, 0);

@@ -33,6 +33,22 @@ struct Error : std::runtime_error {
 // Every kernel launch in this library is followed by exactly one
 // PMB_CHECK_LAUNCH(), which also counts it (pmb_launch_count).
 void count_launch();
+
+// Optional phase timing (environment PMB_PROFILE=1): CUDA events bracket a
+// named phase on a stream; elapsed times are collected when the host next
+// synchronises and reported by pmb_profile_report.
+class PhaseTimer {
+ public:
+  PhaseTimer(const char* name, cudaStream_t s);
+  ~PhaseTimer();
+  static bool enabled();
+
+ private:
+  const char* name_;
+  cudaStream_t s_;
+  cudaEvent_t e0_ = nullptr;
+};
+
 #define PMB_CHECK_LAUNCH()          \
   do {                              \
     ::pmb::count_launch();          \
