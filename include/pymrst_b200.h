@@ -122,6 +122,23 @@ int pmb_ow_spmv(pmb_ow* h, const double* d_jac, const double* d_well, const doub
  *           nonfinite, 0]. */
 int pmb_ow_convergence(pmb_ow* h, const double* d_res, const double* d_x, double dt,
                        double* h_out8);
+/* Allocation-free CNV / MB check over the cells; it has no counterpart in
+ * the reference.  For callers that cannot allocate device memory where they
+ * run the check (inside another framework's memory pool, or where
+ * cudaMalloc's implicit synchronisation is not allowed): no handle, no
+ * cudaMalloc / cudaFree; the per-block partial sums live in a static device
+ * array of 458,752 bytes, so nc may be at most 16,777,216 (larger sizes are
+ * rejected with PMB_ERR_ARG).  d_res and d_x hold the cell part of the
+ * cell-major layout (2*nc doubles each), d_pv the pore volumes;
+ * h_fluid5 = [c_w, c_o, b0_w, b0_o, p_ref]; d_out4 (device) receives
+ * [cnv, mb, non-finite cell count, 0], the cnv and mb of pmb_ow_convergence.
+ * The first call on a device looks up the array's device address, so make
+ * it before any stream capture.  Calls that overlap on the GPU share the
+ * array and race. */
+int pmb_ow_cnv_mb_noalloc(int32_t nc, const double* d_res, const double* d_x, const double* d_pv,
+                          double pv_total, const double* h_fluid5, double dt, double* d_out4,
+                          void* stream);
+
 /* Newton update with the reference's limits (step, :641-651): dp clipped to
  * dp_max_rel*|p|, ds to ds_max, sW to [0,1]; well unknowns unclipped.
  * The increment applied is sign * d_dx. */

@@ -66,6 +66,7 @@ SIGNATURES = {
     "pmb_ow_spmv": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_ow_convergence": (c_int, [c_vp, c_vp, c_vp, c_dbl, P_dbl]),
     "pmb_ow_update": (c_int, [c_vp, c_vp, c_vp, c_dbl]),
+    "pmb_ow_cnv_mb_noalloc": (c_int, [c_int, c_vp, c_vp, c_vp, c_dbl, P_dbl, c_dbl, c_vp, c_vp]),
     "pmb_cpr_default_opts": (c_int, [C.POINTER(CPROpts)]),
     "pmb_cpr_create": (c_int, [c_vp, C.POINTER(CPROpts), C.POINTER(c_vp)]),
     "pmb_cpr_destroy": (c_int, [c_vp]),
