@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--dims", default=None, help="override grid dims, e.g. 30,110,40")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpr", default="", help="CPR option overrides, e.g. amg_cycle=2,local_sweeps=1")
     return ap.parse_args()
 
 
@@ -257,7 +258,10 @@ def run_ours(args):
     n_smooth = int(round(dims[2] * 35 / 85))
     case = cases.channelised(dims=dims, cell_size=WORKLOAD["cell_size"], n_smooth=n_smooth)
     copts = dict(rtol=1e-8, maxiter=400, restart=50, amg_rebuild_interval=1_000_000,
-                 precision=1 if args.precision == "mixed" else 0)
+                 precision=1 if args.precision == "mixed" else 0, amg_cycle=2, local_sweeps=2)
+    for kv in filter(None, args.cpr.split(",")):
+        k, v = kv.split("=")
+        copts[k] = float(v) if k in ("rtol", "amg_theta", "inner_rtol") else int(v)
     model = GpuOilWaterModel(case.grid, case.rock, case.fluid, case.wells, gravity=case.gravity,
                              cpr_options=copts)
     stream = torch.cuda.current_stream()

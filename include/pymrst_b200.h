@@ -91,6 +91,10 @@ typedef struct pmb_ow_desc {
   const double* h_well_val;
   double gravity;
   double tol_cnv, tol_mb, tol_well, ds_max, dp_max_rel;
+  /* nf flags (may be NULL): nonzero where the interface is vertical, so that
+   * N[f,0] -> N[f,1] continues a vertical line of cells; the CPR second stage
+   * solves along these lines */
+  const int32_t* h_line_face;
 } pmb_ow_desc;
 
 int pmb_ow_create(const pmb_ow_desc* desc, void* stream, pmb_ow** out);
@@ -159,7 +163,8 @@ typedef struct pmb_cpr_opts {
   int32_t use_pressure_stage;
   int32_t local_sweeps;     /* red-black block Gauss-Seidel sweeps of the second stage */
   int32_t amg_smoother_degree; /* Chebyshev degree on each level */
-  int32_t amg_cycle;        /* 0: V-cycle, 1: K-cycle (Krylov-accelerated) */
+  int32_t amg_cycle;        /* 0: V-cycle; k > 0: K-cycle, the coarse corrections of the
+                               first k levels accelerated by two Krylov steps */
   double amg_theta;         /* strength threshold of pairwise aggregation */
   int32_t amg_coarse_size;  /* stop coarsening at this many unknowns */
   int32_t amg_rebuild_interval; /* re-aggregate after this many setups */

@@ -36,6 +36,7 @@ class OWDesc(C.Structure):
         ("gravity", c_dbl),
         ("tol_cnv", c_dbl), ("tol_mb", c_dbl), ("tol_well", c_dbl), ("ds_max", c_dbl),
         ("dp_max_rel", c_dbl),
+        ("h_line_face", P_i32),
     ]
 
 

@@ -363,6 +363,85 @@ __global__ void dense_apply_kernel(int n, const double* __restrict__ Inv, const 
   if (lane == 0) x[row] = (T)s;
 }
 
+// K-cycle pieces ------------------------------------------------------------
+
+template <class T>
+__global__ void __launch_bounds__(256) csr_spmv_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                                       const T* __restrict__ a, const T* __restrict__ x,
+                                                       T* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) s += (double)a[k] * (double)x[ci[k]];
+  y[i] = (T)s;
+}
+
+// NDOT = 2: [v1.v1, v1.rc]; NDOT = 5: [v1.v1, v1.v2, v2.v2, v1.rc, v2.rc]
+template <class T, int NDOT>
+__global__ void __launch_bounds__(256) kdots_kernel(int n, const T* __restrict__ v1, const T* __restrict__ v2,
+                                                    const T* __restrict__ rc, double* __restrict__ part) {
+  __shared__ double sh[32];
+  double d[NDOT];
+  for (int q = 0; q < NDOT; ++q) d[q] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double a = (double)v1[i], r = (double)rc[i];
+    if (NDOT == 2) {
+      d[0] += a * a;
+      d[1] += a * r;
+    } else {
+      const double b = (double)v2[i];
+      d[0] += a * a;
+      d[1] += a * b;
+      d[2] += b * b;
+      d[3] += a * r;
+      d[4] += b * r;
+    }
+  }
+  for (int q = 0; q < NDOT; ++q) {
+    const double s = block_sum(d[q], sh);
+    if (threadIdx.x == 0) part[q * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// mode 0: coef[0] = (v1.rc)/(v1.v1); mode 1: least-squares pair
+// [coef[1], coef[2]] minimising |rc - y0 v1 - y1 v2|.
+__global__ void kcoef_kernel(int G, int mode, const double* __restrict__ part, double* __restrict__ coef) {
+  if (threadIdx.x != 0) return;
+  const int nd = mode == 0 ? 2 : 5;
+  double d[5] = {0, 0, 0, 0, 0};
+  for (int q = 0; q < nd; ++q)
+    for (int b = 0; b < G; ++b) d[q] += part[q * G + b];
+  if (mode == 0) {
+    coef[0] = d[0] > 0.0 ? d[1] / d[0] : 0.0;
+  } else {
+    const double a11 = d[0], a12 = d[1], a22 = d[2], r1 = d[3], r2 = d[4];
+    const double det = a11 * a22 - a12 * a12;
+    if (det > 1e-14 * a11 * a22 && isfinite(det)) {
+      coef[1] = (a22 * r1 - a12 * r2) / det;
+      coef[2] = (a11 * r2 - a12 * r1) / det;
+    } else {
+      coef[1] = a11 > 0.0 ? r1 / a11 : 0.0;
+      coef[2] = 0.0;
+    }
+  }
+}
+
+// out = a - coef[0] * b
+template <class T>
+__global__ void kaxpy_kernel(int n, const T* __restrict__ a, const T* __restrict__ b, const double* __restrict__ coef,
+                             T* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (T)((double)a[i] - coef[0] * (double)b[i]);
+}
+
+// out = coef[1] c1 + coef[2] c2
+template <class T>
+__global__ void kcombine_kernel(int n, const T* __restrict__ c1, const T* __restrict__ c2,
+                                const double* __restrict__ coef, T* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (T)(coef[1] * (double)c1[i] + coef[2] * (double)c2[i]);
+}
+
 // ---------------------------------------------------------------------------
 // host class
 // ---------------------------------------------------------------------------
@@ -400,6 +479,15 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
     L.gptr.upload(h.gptr, s);
     L.gidx.upload(h.gidx, s);
     L.lmax.resize(1);
+    if (l >= 1) {  // K-cycle work vectors of a coarse level
+      L.kc1.resize(L.n);
+      L.kc2.resize(L.n);
+      L.kv1.resize(L.n);
+      L.kv2.resize(L.n);
+      L.kr2.resize(L.n);
+      L.kpart.resize(5 * 2 * kNumSM);
+      L.kcoef.resize(3);
+    }
   }
   const AMGHostLevel& c = H.back();
   nco_ = c.n;
@@ -486,10 +574,44 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
   restrict_residual_kernel<T><<<grid_for(nc, 256), 256, 0, s>>>(nc, L.cptr.get(), L.cmem.get(), L.row_ptr,
                                                                  L.col, L.val.get(), b, x, bc);
   PMB_CHECK_LAUNCH();
-  cycle(l + 1, bc, xc, s);
+  coarse_correction(l, bc, xc, s);
   prolong_add_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.agg.get(), xc, x);
   PMB_CHECK_LAUNCH();
   smooth(L, b, x, s, false);
+}
+
+// Coarse correction of level l: a plain recursive cycle, or on the first
+// k_levels levels two Krylov-accelerated cycles (K-cycle):
+//   c1 = B rc, v1 = A c1, r2 = rc - (v1.rc / v1.v1) v1,
+//   c2 = B r2, v2 = A c2, ec = y0 c1 + y1 c2 with y minimising |rc - y0 v1 - y1 v2|.
+template <class T>
+void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
+  const bool kc = l < k_levels && l + 1 < (int)levels_.size();
+  if (!kc) {
+    cycle(l + 1, rc, ec, s);
+    return;
+  }
+  AMGLevel<T>& C = levels_[l + 1];
+  const int n = C.n, g = grid_for(n, 256);
+  const int G = std::min(2 * kNumSM, g);
+  cycle(l + 1, rc, C.kc1.get(), s);
+  csr_spmv_kernel<T><<<g, 256, 0, s>>>(n, C.row_ptr, C.col, C.val.get(), C.kc1.get(), C.kv1.get());
+  PMB_CHECK_LAUNCH();
+  kdots_kernel<T, 2><<<G, 256, 0, s>>>(n, C.kv1.get(), nullptr, rc, C.kpart.get());
+  PMB_CHECK_LAUNCH();
+  kcoef_kernel<<<1, 32, 0, s>>>(G, 0, C.kpart.get(), C.kcoef.get());
+  PMB_CHECK_LAUNCH();
+  kaxpy_kernel<T><<<g, 256, 0, s>>>(n, rc, C.kv1.get(), C.kcoef.get(), C.kr2.get());
+  PMB_CHECK_LAUNCH();
+  cycle(l + 1, C.kr2.get(), C.kc2.get(), s);
+  csr_spmv_kernel<T><<<g, 256, 0, s>>>(n, C.row_ptr, C.col, C.val.get(), C.kc2.get(), C.kv2.get());
+  PMB_CHECK_LAUNCH();
+  kdots_kernel<T, 5><<<G, 256, 0, s>>>(n, C.kv1.get(), C.kv2.get(), rc, C.kpart.get());
+  PMB_CHECK_LAUNCH();
+  kcoef_kernel<<<1, 32, 0, s>>>(G, 1, C.kpart.get(), C.kcoef.get());
+  PMB_CHECK_LAUNCH();
+  kcombine_kernel<T><<<g, 256, 0, s>>>(n, C.kc1.get(), C.kc2.get(), C.kcoef.get(), ec);
+  PMB_CHECK_LAUNCH();
 }
 
 template <class T>

@@ -191,6 +191,110 @@ __global__ void __launch_bounds__(256) gs_color_kernel(OWView v, int cstart, int
   reinterpret_cast<double2*>(z)[c] = zc;
 }
 
+__device__ __forceinline__ double4 inv2(double4 D, bool& ok) {
+  const double det = D.x * D.w - D.y * D.z;
+  ok = det != 0.0 && isfinite(det);
+  const double id = ok ? 1.0 / det : 0.0;
+  return make_double4(id * D.w, -id * D.y, -id * D.z, id * D.x);
+}
+__device__ __forceinline__ double4 mul2(double4 a, double4 b) {
+  return make_double4(a.x * b.x + a.y * b.z, a.x * b.y + a.y * b.w, a.z * b.x + a.w * b.z, a.z * b.y + a.w * b.w);
+}
+__device__ __forceinline__ double2 mv2(double4 a, double2 v) {
+  return make_double2(a.x * v.x + a.y * v.y, a.z * v.x + a.w * v.y);
+}
+
+// Line Gauss-Seidel for one colour of vertical lines, one warp per line:
+// the lanes form the block residual r - J z of the line's cells, then lane 0
+// solves the line's block-tridiagonal system (its couplings to the previous
+// and next cell of the line) by block Thomas elimination and adds the
+// correction to z.  Lines of one colour never touch, so every warp writes
+// only its own cells.  `ys` / `gs` are per-line-position scratch (the
+// forward-eliminated right-hand side and the inverted pivots).
+__global__ void __launch_bounds__(128) line_gs_kernel(OWView v, int lstart, int lend,
+                                                      const int* __restrict__ clines,
+                                                      const int* __restrict__ lptr,
+                                                      const int* __restrict__ lcells,
+                                                      const int* __restrict__ llo,
+                                                      const int* __restrict__ lup,
+                                                      const double4* __restrict__ A,
+                                                      const double* __restrict__ wj,
+                                                      const double* __restrict__ r, double* __restrict__ z,
+                                                      double2* __restrict__ ys, double4* __restrict__ gs,
+                                                      int* status) {
+  const int lane = threadIdx.x & 31;
+  const int li = lstart + (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  if (li >= lend) return;  // uniform across the warp
+  const int L = clines[li];
+  const int t0 = lptr[L], t1 = lptr[L + 1];
+  const double2* z2 = reinterpret_cast<const double2*>(z);
+  for (int t = t0 + lane; t < t1; t += 32) {
+    const int c = lcells[t];
+    double2 rc = reinterpret_cast<const double2*>(r)[c];
+    for (int k = v.row_ptr[c]; k < v.row_ptr[c + 1]; ++k) {
+      const double2 q = mv2(A[k], z2[v.col[k]]);
+      rc.x -= q.x;
+      rc.y -= q.y;
+    }
+    const int q = v.cell_pc[c];
+    if (q >= 0) {
+      const double* zw = z + 2LL * v.nc;
+      for (int jj = v.pc_ptr[q]; jj < v.pc_ptr[q + 1]; ++jj) {
+        const int i = v.pc_perf[jj];
+        const int kw = v.perf_well[i];
+        const double* B = wj + v.wl.B + 6LL * i;
+        rc.x -= B[0] * zw[3 * kw] + B[1] * zw[3 * kw + 1] + B[2] * zw[3 * kw + 2];
+        rc.y -= B[3] * zw[3 * kw] + B[4] * zw[3 * kw + 1] + B[5] * zw[3 * kw + 2];
+      }
+    }
+    ys[t] = rc;
+  }
+  __syncwarp();
+  if (lane != 0) return;
+  // forward elimination
+  double4 Gp = make_double4(0, 0, 0, 0);
+  double2 yp = make_double2(0, 0);
+  for (int t = t0; t < t1; ++t) {
+    const int c = lcells[t];
+    double4 D = A[v.diag_pos[c]];
+    double2 y = ys[t];
+    if (t > t0 && llo[t] >= 0 && lup[t - 1] >= 0) {
+      const double4 LG = mul2(A[llo[t]], Gp);
+      const double4 LGU = mul2(LG, A[lup[t - 1]]);
+      D.x -= LGU.x; D.y -= LGU.y; D.z -= LGU.z; D.w -= LGU.w;
+      const double2 q = mv2(LG, yp);
+      y.x -= q.x;
+      y.y -= q.y;
+    }
+    bool ok;
+    const double4 G = inv2(D, ok);
+    if (!ok) {
+      atomicExch(status, PMB_ERR_PIVOT);
+      return;
+    }
+    gs[t] = G;
+    ys[t] = y;
+    Gp = G;
+    yp = y;
+  }
+  // back substitution
+  double2 dn = make_double2(0, 0);
+  for (int t = t1 - 1; t >= t0; --t) {
+    double2 y = ys[t];
+    if (t + 1 < t1 && lup[t] >= 0) {
+      const double2 q = mv2(A[lup[t]], dn);
+      y.x -= q.x;
+      y.y -= q.y;
+    }
+    dn = mv2(gs[t], y);
+    const int c = lcells[t];
+    double2 zc = z2[c];
+    zc.x += dn.x;
+    zc.y += dn.y;
+    reinterpret_cast<double2*>(z)[c] = zc;
+  }
+}
+
 // Well unknowns: z_w += inv(D_k) (r_w - C z_cells - D_k z_w).
 __global__ void gs_well_kernel(OWView v, const double* __restrict__ wj, const double* __restrict__ r,
                                double* __restrict__ z) {
@@ -241,6 +345,10 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   status_.zero(s_);
   bp_.resize(m.nc());
   xp_.resize(m.nc());
+  if (m.has_lines()) {
+    line_y_.resize(2LL * m.nc());
+    line_g_.resize(4LL * m.nc());
+  }
   ap_.resize(m.nnzb());
   V_.resize((size_t)(mm + 1) * ld_);
   Z_.resize((size_t)mm * ld_);
@@ -253,6 +361,7 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   st_pin_.resize(1);
   st_pin_[0] = 0;
   amg_.degree = std::max(1, o_.amg_smoother_degree);
+  amg_.k_levels = std::max(0, o_.amg_cycle);
   PMB_CUDA(cudaStreamSynchronize(s_));
 }
 
@@ -302,6 +411,25 @@ void CPRSolver::local_stage(const double* r, double* z) {
   const OWView v = m_.view();
   const auto& cp = m_.h_color_ptr();
   const double4* A = reinterpret_cast<const double4*>(jac_);
+  if (m_.has_lines()) {
+    const auto& Ls = m_.lines();
+    for (int sweep = 0; sweep < std::max(1, o_.local_sweeps); ++sweep) {
+      for (int q = 0; q + 1 < (int)Ls.h_color_ptr.size(); ++q) {
+        const int cnt = Ls.h_color_ptr[q + 1] - Ls.h_color_ptr[q];
+        if (cnt <= 0) continue;
+        line_gs_kernel<<<grid_for(32LL * cnt, 128), 128, 0, s_>>>(
+            v, Ls.h_color_ptr[q], Ls.h_color_ptr[q + 1], Ls.color_lines.get(), Ls.line_ptr.get(),
+            Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(), A, well_, r, z,
+            reinterpret_cast<double2*>(line_y_.get()), reinterpret_cast<double4*>(line_g_.get()), status_.get());
+        PMB_CHECK_LAUNCH();
+      }
+      if (v.nw) {
+        gs_well_kernel<<<1, 128, 0, s_>>>(v, well_, r, z);
+        PMB_CHECK_LAUNCH();
+      }
+    }
+    return;
+  }
   for (int sweep = 0; sweep < std::max(1, o_.local_sweeps); ++sweep) {
     for (int q = 0; q + 1 < (int)cp.size(); ++q) {
       const int cnt = cp[q + 1] - cp[q];

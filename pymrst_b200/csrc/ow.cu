@@ -810,6 +810,7 @@ OWModel::OWModel(const pmb_ow_desc& d, cudaStream_t s) : stream_(s) {
   v_.ds_max = d.ds_max; v_.dp_max_rel = d.dp_max_rel;
   pv_tot_ = pv_tot;
 
+  build_lines(d, code);
   jac_.resize(4 * nnzb_);
   well_.resize(std::max<int64_t>(v_.wl.total, 1));
   res_.resize(nvec());
@@ -879,6 +880,89 @@ void OWModel::convergence_async(const double* res, const double* x, double dt, d
   PMB_CHECK_LAUNCH();
   ow_conv_final_kernel<<<1, 256, 0, stream_>>>(v_, conv_part_.get(), kConvBlocks, res, dt, pv_tot_, d_out);
   PMB_CHECK_LAUNCH();
+}
+
+// Vertical lines from the flagged interfaces: each cell keeps at most one
+// successor (N[f,1] of a flagged face where it is N[f,0]) and one predecessor;
+// lines start at cells without a predecessor.  Cells caught in a cycle of
+// flagged faces become lines of their own.
+void OWModel::build_lines(const pmb_ow_desc& d, const std::vector<int>& code) {
+  (void)code;
+  const int nc = v_.nc, nf = v_.nf;
+  if (!d.h_line_face || nf == 0) return;
+  std::vector<int> next(nc, -1), prev(nc, -1);
+  for (int f = 0; f < nf; ++f) {
+    if (!d.h_line_face[f]) continue;
+    const int a = d.h_N[2 * f], b = d.h_N[2 * f + 1];
+    if (next[a] == -1 && prev[b] == -1) {
+      next[a] = b;
+      prev[b] = a;
+    }
+  }
+  std::vector<int> line_ptr(1, 0), cells;
+  cells.reserve(nc);
+  std::vector<char> seen(nc, 0);
+  for (int c = 0; c < nc; ++c) {
+    if (prev[c] != -1) continue;
+    for (int t = c; t != -1 && !seen[t]; t = next[t]) {
+      seen[t] = 1;
+      cells.push_back(t);
+    }
+    line_ptr.push_back((int)cells.size());
+  }
+  for (int c = 0; c < nc; ++c)
+    if (!seen[c]) {
+      seen[c] = 1;
+      cells.push_back(c);
+      line_ptr.push_back((int)cells.size());
+    }
+  const int nl = (int)line_ptr.size() - 1;
+  auto find = [&](int row, int colv) {
+    const int* b = h_col_.data() + h_row_ptr_[row];
+    const int* e = h_col_.data() + h_row_ptr_[row + 1];
+    const int* it = std::lower_bound(b, e, colv);
+    return (it != e && *it == colv) ? (int)(it - h_col_.data()) : -1;
+  };
+  std::vector<int> lo(nc, -1), up(nc, -1), line_of(nc, 0);
+  int max_len = 0;
+  for (int L = 0; L < nl; ++L) {
+    const int t0 = line_ptr[L], t1 = line_ptr[L + 1];
+    max_len = std::max(max_len, t1 - t0);
+    for (int t = t0; t < t1; ++t) {
+      line_of[cells[t]] = L;
+      if (t > t0) lo[t] = find(cells[t], cells[t - 1]);
+      if (t + 1 < t1) up[t] = find(cells[t], cells[t + 1]);
+    }
+  }
+  // greedy colouring of the line graph
+  std::vector<int> lcolor(nl, -1), mark;
+  int ncol = 0;
+  for (int L = 0; L < nl; ++L) {
+    mark.assign(ncol + 1, 0);
+    for (int t = line_ptr[L]; t < line_ptr[L + 1]; ++t) {
+      const int c = cells[t];
+      for (int k = h_row_ptr_[c]; k < h_row_ptr_[c + 1]; ++k) {
+        const int M = line_of[h_col_[k]];
+        if (M != L && lcolor[M] >= 0) mark[lcolor[M]] = 1;
+      }
+    }
+    int q = 0;
+    while (q < ncol && mark[q]) ++q;
+    lcolor[L] = q;
+    if (q == ncol) ++ncol;
+  }
+  lines_.h_color_ptr.assign(ncol + 1, 0);
+  for (int L = 0; L < nl; ++L) ++lines_.h_color_ptr[lcolor[L] + 1];
+  for (int q = 0; q < ncol; ++q) lines_.h_color_ptr[q + 1] += lines_.h_color_ptr[q];
+  std::vector<int> clines(nl), cf(lines_.h_color_ptr.begin(), lines_.h_color_ptr.end() - 1);
+  for (int L = 0; L < nl; ++L) clines[cf[lcolor[L]]++] = L;
+  lines_.nlines = nl;
+  lines_.max_len = max_len;
+  lines_.line_ptr.upload(line_ptr, stream_);
+  lines_.line_cells.upload(cells, stream_);
+  lines_.line_lo.upload(lo, stream_);
+  lines_.line_up.upload(up, stream_);
+  lines_.color_lines.upload(clines, stream_);
 }
 
 void OWModel::update(double* x, const double* dx, double sgn) {

@@ -36,6 +36,8 @@ struct AMGLevel {
   const int* col = nullptr;
   DArray<int> own_row_ptr, own_col;
   DArray<T> val, dinv, x, b, r, t;
+  DArray<T> kc1, kc2, kv1, kv2, kr2;  // K-cycle vectors of this level (as a coarse level)
+  DArray<double> kpart, kcoef;        // K-cycle reduction partials and coefficients
   DArray<int> agg, cptr, cmem, gptr, gidx;
   DArray<double> lmax;  // Chebyshev upper bound (device scalar)
 };
@@ -50,8 +52,11 @@ class AMG {
              int coarse_size, cudaStream_t s);
   // Refresh all levels from level-0 values already written to level0_val().
   void refresh(cudaStream_t s, int* d_status);
-  // x = M^{-1} b with one V-cycle.
+  // x = M^{-1} b with one cycle: V-cycle, or (k_levels > 0) a K-cycle whose
+  // coarse corrections on the first k_levels levels are accelerated by two
+  // minimal-residual Krylov steps.
   void apply(const T* b, T* x, cudaStream_t s);
+  int k_levels = 0;
   T* level0_val() { return levels_.empty() ? co_val_.get() : levels_[0].val.get(); }
   bool built() const { return nco_ > 0; }
   int num_levels() const { return (int)levels_.size() + (nco_ > 0 ? 1 : 0); }
@@ -60,6 +65,7 @@ class AMG {
 
  private:
   void cycle(int l, const T* b, T* x, cudaStream_t s);
+  void coarse_correction(int l, const T* rc, T* ec, cudaStream_t s);
   void smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start);
   std::vector<AMGLevel<T>> levels_;
   // coarsest level: dense inverse in FP64

@@ -38,6 +38,7 @@ class CPRSolver {
   DArray<int> status_;
   DArray<double> bp_, xp_, ap_;  // pressure system rhs / solution / values for aggregation
   DArray<double> V_, Z_, wv_, r_, hcol_, htmp_, y_;
+  DArray<double> line_y_, line_g_;  // line Gauss-Seidel scratch (per line position)
   PinnedArray<double> h_pin_;
   PinnedArray<int> st_pin_;
   std::vector<double> h_ap_;

@@ -82,6 +82,17 @@ class OWModel {
   const std::vector<int>& h_col() const { return h_col_; }
   const std::vector<int>& h_color_ptr() const { return h_color_ptr_; }
   const int* color_cells() const { return color_cells_.get(); }
+  // Vertical lines: cells of line L are line_cells[line_ptr[L] .. line_ptr[L+1])
+  // top to bottom; line_lo / line_up give, per line position, the block-CSR
+  // index of the coupling to the previous / next cell of the line (-1 at the
+  // ends).  Lines are coloured so that lines of one colour never touch.
+  struct Lines {
+    int nlines = 0, max_len = 0;
+    std::vector<int> h_color_ptr;  // per colour: range in color_lines
+    DArray<int> line_ptr, line_cells, line_lo, line_up, color_lines;
+  };
+  const Lines& lines() const { return lines_; }
+  bool has_lines() const { return lines_.nlines > 0 && lines_.max_len > 1; }
 
   void compute_cdp(const double* x0, double* cdp);
   void reset_cdp() { have_last_cdp_ = false; }
@@ -116,6 +127,8 @@ class OWModel {
   DArray<double> jac_, well_, res_, cdp_, x0_, dx_;
   bool have_last_cdp_ = false;
   double pv_tot_ = 0.0;
+  Lines lines_;
+  void build_lines(const pmb_ow_desc& d, const std::vector<int>& code);
 };
 
 }  // namespace pmb

@@ -147,6 +147,7 @@ class GpuOilWaterModel:
         self.fluid_params = prm
         Nall = np.asarray(g.faces.neighbors, dtype=np.int64)
         internal = np.all(Nall >= 0, axis=1)
+        self._internal = internal
         self.N = Nall[internal]
         if T is None:
             tf, _ = face_transmissibility_device(g, rock)
@@ -196,6 +197,13 @@ class GpuOilWaterModel:
             well_type=np.array([self._well_type(w) for w in self.wells] or [0], dtype=np.int32),
             well_val=np.array([float(np.ravel(w.val)[0]) for w in self.wells] or [0.0], dtype=np.float64),
         )
+        # vertical interfaces (|n_z| dominant) chain cells into the lines the
+        # CPR second stage solves along
+        normals = getattr(self.g.faces, "normals", None)
+        if normals is not None and np.asarray(normals).shape[1] == 3 and self.N.shape[0]:
+            nrm = np.abs(np.asarray(normals)[self._internal])
+            line = (nrm[:, 2] > nrm[:, 0]) & (nrm[:, 2] > nrm[:, 1])
+            self._h["line_face"] = np.ascontiguousarray(line, dtype=np.int32)
         h = self._h
         d = N.OWDesc()
         d.nc, d.nf, d.nw = self.nc, self.N.shape[0], nw
@@ -218,6 +226,8 @@ class GpuOilWaterModel:
         d.gravity = self.gravity
         d.tol_cnv, d.tol_mb, d.tol_well = self.tol_cnv, self.tol_mb, self.tol_well
         d.ds_max, d.dp_max_rel = self.ds_max, self.dp_max_rel
+        if "line_face" in h:
+            d.h_line_face = N.as_p(h["line_face"], N.C.c_int32)
         hd = N.c_vp()
         stream = torch.cuda.current_stream().cuda_stream
         N.check(N.lib().pmb_ow_create(N.C.byref(d), stream, N.C.byref(hd)))
