@@ -279,6 +279,10 @@ def run_ours(args):
             ok, nit, st = model.step_device(xv, h)
             its += nit
             kry += int(st[2])
+            if os.environ.get("PMB_VERBOSE") == "1":
+                print(f"# step dt={h / 86400:.3g} d ok={ok} newton={nit} krylov={int(st[2])} "
+                      f"cnv={st[4]:.2e} mb={st[5]:.2e} {getattr(model, 'last_failure', '') if not ok else ''}",
+                      file=sys.stderr, flush=True)
             if ok:
                 t_local += h
                 h = min(2 * h, dt - t_local) if cuts else h
