@@ -138,6 +138,94 @@ __global__ void restrict_p_kernel(int nc, const double2* __restrict__ r, const d
   bp[c] = w[0] * rr.x + w[1] * rr.y;
 }
 
+// ---- pressure system with well bhp unknowns --------------------------------
+//
+// Pressure unknowns [p_cells, bhp_wells].  For well k, with D its 3x3 block
+// (rows eq_w, eq_o, ctrl; columns qWs, qOs, bhp) and D2 = D[0:2, 0:2], the
+// rate unknowns are eliminated exactly from the control row and from the
+// weighted cell rows:
+//   well row:  a = D[2,0:2] D2^{-1};  diagonal D[2,2] - a D[0:2,2];
+//              cell columns -a C_i[:, p]
+//   cell rows: g_i = (w B_i[:, 0:2]) D2^{-1};  bhp column w B_i[:, 2] - g_i D[0:2,2]
+// (the coupling between perforated cells that the elimination would add is
+// left out of the preconditioner).
+
+__global__ void ext_cells_kernel(long long nnzb, const double4* __restrict__ A, const double* __restrict__ w,
+                                 const int* __restrict__ bsr2ext, double* __restrict__ ext) {
+  const double ww = w[0], wo = w[1];
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnzb;
+       k += (long long)gridDim.x * blockDim.x) {
+    const double4 a = A[k];
+    ext[bsr2ext[k]] = ww * a.x + wo * a.z;
+  }
+}
+
+__global__ void ext_wells_kernel(OWView v, const double* __restrict__ wj, const double* __restrict__ w,
+                                 const int* __restrict__ perf_cw, const int* __restrict__ perf_wc,
+                                 const int* __restrict__ well_diag, double* __restrict__ ext,
+                                 double* __restrict__ g_perf, double* __restrict__ a_well) {
+  const double ww = w[0], wo = w[1];
+  for (int k = threadIdx.x; k < v.nw; k += blockDim.x) {
+    const double* D = wj + v.wl.D + 9LL * k;
+    const double det = D[0] * D[4] - D[1] * D[3];
+    const bool ok = det != 0.0 && isfinite(det);
+    const double id = ok ? 1.0 / det : 0.0;
+    const double i00 = id * D[4], i01 = -id * D[1], i10 = -id * D[3], i11 = id * D[0];
+    const double a0 = D[6] * i00 + D[7] * i10, a1 = D[6] * i01 + D[7] * i11;
+    a_well[2 * k] = a0;
+    a_well[2 * k + 1] = a1;
+    const int i0 = v.perf_ptr[k], i1 = v.perf_ptr[k + 1];
+    for (int i = i0; i < i1; ++i) {
+      ext[perf_cw[i]] = 0.0;
+      ext[perf_wc[i]] = 0.0;
+    }
+    ext[well_diag[k]] = D[8] - (a0 * D[2] + a1 * D[5]);
+    for (int i = i0; i < i1; ++i) {
+      const double* C = wj + v.wl.C + 4LL * i;
+      ext[perf_wc[i]] += -(a0 * C[0] + a1 * C[2]);
+      const double* B = wj + v.wl.B + 6LL * i;
+      const double wb0 = ww * B[0] + wo * B[3], wb1 = ww * B[1] + wo * B[4], wb2 = ww * B[2] + wo * B[5];
+      const double g0 = wb0 * i00 + wb1 * i10, g1 = wb0 * i01 + wb1 * i11;
+      g_perf[2 * i] = g0;
+      g_perf[2 * i + 1] = g1;
+      ext[perf_cw[i]] += wb2 - (g0 * D[2] + g1 * D[5]);
+    }
+  }
+}
+
+// Right-hand side of the well-augmented pressure system: perforated cells
+// lose g_i r_w[0:2]; well rows get r_ctrl - a r_w[0:2].  Cell rows were
+// written by restrict_p_kernel.
+__global__ void restrict_wells_kernel(OWView v, const double* __restrict__ r, const double* __restrict__ g_perf,
+                                      const double* __restrict__ a_well, double* __restrict__ bp) {
+  const double* rwb = r + 2LL * v.nc;
+  for (int q = threadIdx.x; q < v.npc; q += blockDim.x) {
+    const int c = v.pcell[q];
+    double s = bp[c];
+    for (int j = v.pc_ptr[q]; j < v.pc_ptr[q + 1]; ++j) {
+      const int i = v.pc_perf[j];
+      const double* rw = rwb + 3LL * v.perf_well[i];
+      s -= g_perf[2 * i] * rw[0] + g_perf[2 * i + 1] * rw[1];
+    }
+    bp[c] = s;
+  }
+  for (int k = threadIdx.x; k < v.nw; k += blockDim.x) {
+    const double* rw = rwb + 3LL * k;
+    bp[v.nc + k] = rw[2] - (a_well[2 * k] * rw[0] + a_well[2 * k + 1] * rw[1]);
+  }
+}
+
+// z = P xp with well bhp: cells (xp, 0); wells (0, 0, xp[nc + k]).
+__global__ void prolong_pw_kernel(int nc, int nw, const double* __restrict__ xp, double* __restrict__ z) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nc) reinterpret_cast<double2*>(z)[t] = make_double2(xp[t], 0.0);
+  if (t < nw) {
+    z[2LL * nc + 3LL * t] = 0.0;
+    z[2LL * nc + 3LL * t + 1] = 0.0;
+    z[2LL * nc + 3LL * t + 2] = xp[nc + t];
+  }
+}
+
 // z = P xp (cells: (xp, 0); wells: 0)
 __global__ void prolong_p_kernel(int nc, int nwv, const double* __restrict__ xp, double* __restrict__ z) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -343,13 +431,15 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   part_.resize((size_t)kRedBlocks * (mm + 2));
   status_.resize(1);
   status_.zero(s_);
-  bp_.resize(m.nc());
-  xp_.resize(m.nc());
+  np_ = m.nc();
+  if (m.nw() > 0) build_pressure_pattern();
+  bp_.resize(np_);
+  xp_.resize(np_);
   if (m.has_lines()) {
     line_y_.resize(2LL * m.nc());
     line_g_.resize(4LL * m.nc());
   }
-  ap_.resize(m.nnzb());
+  ap_.resize(np_ > m.nc() ? h_ecol_.size() : (size_t)m.nnzb());
   V_.resize((size_t)(mm + 1) * ld_);
   Z_.resize((size_t)mm * ld_);
   wv_.resize(n);
@@ -363,6 +453,77 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   amg_.degree = std::max(1, o_.amg_smoother_degree);
   amg_.k_levels = std::max(0, o_.amg_cycle);
   PMB_CUDA(cudaStreamSynchronize(s_));
+}
+
+// CSR pattern of the well-augmented pressure system: cell rows keep their
+// block-CSR columns (in order) followed by the bhp columns of the wells that
+// perforate them; well rows list their perforated cells, then themselves.
+void CPRSolver::build_pressure_pattern() {
+  const OWView v = m_.view();
+  const int nc = v.nc, nw = v.nw;
+  const auto& rp = m_.h_row_ptr();
+  const auto& col = m_.h_col();
+  std::vector<int> perf_ptr(nw + 1), perf_cell(v.nperf);
+  PMB_CUDA(cudaMemcpy(perf_ptr.data(), v.perf_ptr, sizeof(int) * (nw + 1), cudaMemcpyDeviceToHost));
+  if (v.nperf)
+    PMB_CUDA(cudaMemcpy(perf_cell.data(), v.perf_cell, sizeof(int) * v.nperf, cudaMemcpyDeviceToHost));
+  std::vector<std::vector<int>> cell_wells(nc);
+  std::vector<std::vector<int>> well_cells(nw);
+  for (int k = 0; k < nw; ++k)
+    for (int i = perf_ptr[k]; i < perf_ptr[k + 1]; ++i) {
+      cell_wells[perf_cell[i]].push_back(k);
+      well_cells[k].push_back(perf_cell[i]);
+    }
+  for (auto& s : cell_wells) { std::sort(s.begin(), s.end()); s.erase(std::unique(s.begin(), s.end()), s.end()); }
+  for (auto& s : well_cells) { std::sort(s.begin(), s.end()); s.erase(std::unique(s.begin(), s.end()), s.end()); }
+  np_ = nc + nw;
+  h_erp_.assign(np_ + 1, 0);
+  h_ecol_.clear();
+  std::vector<int> bsr2ext(rp[nc]);
+  for (int c = 0; c < nc; ++c) {
+    for (int k = rp[c]; k < rp[c + 1]; ++k) {
+      bsr2ext[k] = (int)h_ecol_.size();
+      h_ecol_.push_back(col[k]);
+    }
+    for (int k : cell_wells[c]) h_ecol_.push_back(nc + k);
+    h_erp_[c + 1] = (int)h_ecol_.size();
+  }
+  std::vector<int> well_diag(nw);
+  for (int k = 0; k < nw; ++k) {
+    for (int c : well_cells[k]) h_ecol_.push_back(c);
+    well_diag[k] = (int)h_ecol_.size();
+    h_ecol_.push_back(nc + k);
+    h_erp_[nc + k + 1] = (int)h_ecol_.size();
+  }
+  std::vector<int> perf_cw(v.nperf), perf_wc(v.nperf);
+  for (int k = 0; k < nw; ++k)
+    for (int i = perf_ptr[k]; i < perf_ptr[k + 1]; ++i) {
+      const int c = perf_cell[i];
+      const int ncell_cols = rp[c + 1] - rp[c];
+      const auto& cw = cell_wells[c];
+      perf_cw[i] = h_erp_[c] + ncell_cols + (int)(std::lower_bound(cw.begin(), cw.end(), k) - cw.begin());
+      const auto& wc = well_cells[k];
+      perf_wc[i] = h_erp_[nc + k] + (int)(std::lower_bound(wc.begin(), wc.end(), c) - wc.begin());
+    }
+  erp_.upload(h_erp_, s_);
+  ecol_.upload(h_ecol_, s_);
+  bsr2ext_.upload(bsr2ext, s_);
+  perf_cw_.upload(perf_cw, s_);
+  perf_wc_.upload(perf_wc, s_);
+  well_diag_.upload(well_diag, s_);
+  g_perf_.resize(2LL * std::max(v.nperf, 1));
+  a_well_.resize(2LL * nw);
+}
+
+void CPRSolver::pressure_values(double* ext) {
+  const OWView v = m_.view();
+  const long long nnzb = m_.nnzb();
+  ext_cells_kernel<<<grid_for(nnzb, 256), 256, 0, s_>>>(nnzb, reinterpret_cast<const double4*>(jac_), w_.get(),
+                                                         bsr2ext_.get(), ext);
+  PMB_CHECK_LAUNCH();
+  ext_wells_kernel<<<1, 128, 0, s_>>>(v, well_, w_.get(), perf_cw_.get(), perf_wc_.get(), well_diag_.get(), ext,
+                                      g_perf_.get(), a_well_.get());
+  PMB_CHECK_LAUNCH();
 }
 
 void CPRSolver::check_status() {
@@ -388,21 +549,31 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
   weights_kernel<<<1, 32, 0, s_>>>(v, kRedBlocks, part_.get(), w_.get());
   PMB_CHECK_LAUNCH();
   const long long nnzb = m_.nnzb();
+  const bool with_wells = np_ > v.nc;
+  auto values = [&](double* dst) {
+    if (with_wells) {
+      pressure_values(dst);
+    } else {
+      ap_kernel<<<grid_for(nnzb, 256), 256, 0, s_>>>(nnzb, reinterpret_cast<const double4*>(jac), w_.get(), dst);
+      PMB_CHECK_LAUNCH();
+    }
+  };
   const bool rebuild = !amg_.built() || since_build_ >= std::max(1, o_.amg_rebuild_interval);
   if (rebuild) {
-    ap_kernel<<<grid_for(nnzb, 256), 256, 0, s_>>>(nnzb, reinterpret_cast<const double4*>(jac), w_.get(),
-                                                   ap_.get());
-    PMB_CHECK_LAUNCH();
-    h_ap_.resize(nnzb);
-    PMB_CUDA(cudaMemcpyAsync(h_ap_.data(), ap_.get(), sizeof(double) * nnzb, cudaMemcpyDeviceToHost, s_));
+    values(ap_.get());
+    const size_t nnz = ap_.size();
+    h_ap_.resize(nnz);
+    PMB_CUDA(cudaMemcpyAsync(h_ap_.data(), ap_.get(), sizeof(double) * nnz, cudaMemcpyDeviceToHost, s_));
     PMB_CUDA(cudaStreamSynchronize(s_));
-    amg_.build(v.nc, m_.h_row_ptr(), m_.h_col(), v.row_ptr, v.col, h_ap_, o_.amg_theta,
-               std::max(16, o_.amg_coarse_size), s_);
+    if (with_wells)
+      amg_.build(np_, h_erp_, h_ecol_, erp_.get(), ecol_.get(), h_ap_, o_.amg_theta,
+                 std::max(16, o_.amg_coarse_size), s_);
+    else
+      amg_.build(v.nc, m_.h_row_ptr(), m_.h_col(), v.row_ptr, v.col, h_ap_, o_.amg_theta,
+                 std::max(16, o_.amg_coarse_size), s_);
     since_build_ = 0;
   }
-  ap_kernel<<<grid_for(nnzb, 256), 256, 0, s_>>>(nnzb, reinterpret_cast<const double4*>(jac), w_.get(),
-                                                 amg_.level0_val());
-  PMB_CHECK_LAUNCH();
+  values(amg_.level0_val());
   amg_.refresh(s_, status_.get());
   ++since_build_;
 }
@@ -452,11 +623,19 @@ void CPRSolver::precond(const double* r, double* z) {
     restrict_p_kernel<<<grid_for(v.nc, 256), 256, 0, s_>>>(v.nc, reinterpret_cast<const double2*>(r), w_.get(),
                                                            bp_.get());
     PMB_CHECK_LAUNCH();
+    if (np_ > v.nc) {
+      restrict_wells_kernel<<<1, 256, 0, s_>>>(v, r, g_perf_.get(), a_well_.get(), bp_.get());
+      PMB_CHECK_LAUNCH();
+    }
     {
       PhaseTimer pt("cpr.amg_cycle", s_);
       amg_.apply(bp_.get(), xp_.get(), s_);
     }
-    prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, xp_.get(), z);
+    if (np_ > v.nc) {
+      prolong_pw_kernel<<<gpro, 256, 0, s_>>>(v.nc, v.nw, xp_.get(), z);
+    } else {
+      prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, xp_.get(), z);
+    }
     PMB_CHECK_LAUNCH();
   } else {
     prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, nullptr, z);

@@ -39,6 +39,16 @@ class CPRSolver {
   DArray<double> bp_, xp_, ap_;  // pressure system rhs / solution / values for aggregation
   DArray<double> V_, Z_, wv_, r_, hcol_, htmp_, y_;
   DArray<double> line_y_, line_g_;  // line Gauss-Seidel scratch (per line position)
+  // Pressure system with one bhp unknown per well (np_ = nc + nw): CSR
+  // pattern, the position of every cell block in it (bsr2ext), of each
+  // perforation's (cell, well) and (well, cell) entries, and of each well's
+  // diagonal; per-perforation and per-well elimination coefficients.
+  int np_ = 0;
+  std::vector<int> h_erp_, h_ecol_;
+  DArray<int> erp_, ecol_, bsr2ext_, perf_cw_, perf_wc_, well_diag_;
+  DArray<double> g_perf_, a_well_;
+  void build_pressure_pattern();
+  void pressure_values(double* ext);
   PinnedArray<double> h_pin_;
   PinnedArray<int> st_pin_;
   std::vector<double> h_ap_;
