@@ -15,7 +15,8 @@ static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 
 static std::atomic<long long> g_launches{0};
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(); }
 
 // ---- phase timers -----------------------------------------------------------
 struct PendingPhase {
@@ -367,6 +368,13 @@ int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_itera
         PhaseTimer pt("newton.cpr_solve", st);
         ok = cpr.solve(m.res(), m.dx(), info);
       }
+      static const bool trace = [] {
+        const char* e = std::getenv("PMB_NEWTON_TRACE");
+        return e && e[0] == '1';
+      }();
+      if (trace)
+        std::fprintf(stderr, "# newton it=%d cnv=%.3e mb=%.3e well_w=%.3e well_o=%.3e ctrl_ok=%g krylov=%g relres=%.2e\n",
+                     it, h->conv[0], h->conv[1], h->conv[2], h->conv[3], h->conv[4], info[0], info[1]);
       krylov += info[0];
       if (!ok) {
         PMB_CUDA(cudaMemcpyAsync(d_x, m.x0(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));

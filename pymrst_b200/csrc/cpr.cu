@@ -9,6 +9,7 @@
 // pressure correction (so it contains the "r - A x" of the second stage), in
 // place of one block-Jacobi application.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 
 #include "pmb_cpr.cuh"
@@ -572,6 +573,7 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
       amg_.build(v.nc, m_.h_row_ptr(), m_.h_col(), v.row_ptr, v.col, h_ap_, o_.amg_theta,
                  std::max(16, o_.amg_coarse_size), s_);
     since_build_ = 0;
+    drop_graph();  // the hierarchy's buffers are new
   }
   values(amg_.level0_val());
   amg_.refresh(s_, status_.get());
@@ -616,7 +618,69 @@ void CPRSolver::local_stage(const double* r, double* z) {
   }
 }
 
+CPRSolver::~CPRSolver() {
+  drop_graph();
+  if (cap_s_) cudaStreamDestroy(cap_s_);
+}
+
+void CPRSolver::drop_graph() {
+  if (pg_exec_) cudaGraphExecDestroy(pg_exec_);
+  pg_exec_ = nullptr;
+  pg_valid_ = false;
+}
+
 void CPRSolver::precond(const double* r, double* z) {
+  static const bool use_graph = [] {
+    const char* e = std::getenv("PMB_NO_GRAPH");
+    return !(e && e[0] == '1');
+  }();
+  if (!use_graph || PhaseTimer::enabled()) {
+    precond_body(r, z);
+    return;
+  }
+  const long long n = m_.nvec();
+  if (!pin_.size()) {
+    pin_.resize(n);
+    pout_.resize(n);
+  }
+  if (!pg_valid_ || pg_jac_ != jac_ || pg_well_ != well_) {
+    drop_graph();
+    // capture on a private stream (the legacy default stream cannot be
+    // captured); the graph is then launched on the solver's stream
+    if (!cap_s_) PMB_CUDA(cudaStreamCreateWithFlags(&cap_s_, cudaStreamNonBlocking));
+    PMB_CUDA(cudaStreamSynchronize(s_));
+    const long long before = launch_count();
+    const cudaStream_t saved = s_;
+    s_ = cap_s_;
+    PMB_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t g = nullptr;
+    try {
+      precond_body(pin_.get(), pout_.get());
+    } catch (...) {
+      cudaStreamEndCapture(s_, &g);
+      if (g) cudaGraphDestroy(g);
+      s_ = saved;
+      throw;
+    }
+    const cudaError_t ce = cudaStreamEndCapture(s_, &g);
+    s_ = saved;
+    PMB_CUDA(ce);
+    pg_nodes_ = launch_count() - before;
+    count_launch(-pg_nodes_);  // captured, not launched
+    const cudaError_t e = cudaGraphInstantiate(&pg_exec_, g, 0);
+    cudaGraphDestroy(g);
+    PMB_CUDA(e);
+    pg_valid_ = true;
+    pg_jac_ = jac_;
+    pg_well_ = well_;
+  }
+  PMB_CUDA(cudaMemcpyAsync(pin_.get(), r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s_));
+  PMB_CUDA(cudaGraphLaunch(pg_exec_, s_));
+  count_launch(pg_nodes_);
+  PMB_CUDA(cudaMemcpyAsync(z, pout_.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, s_));
+}
+
+void CPRSolver::precond_body(const double* r, double* z) {
   const OWView v = m_.view();
   const int gpro = grid_for(std::max<long long>(v.nc, 3LL * v.nw), 256);
   if (o_.use_pressure_stage) {

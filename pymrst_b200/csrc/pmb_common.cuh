@@ -32,7 +32,8 @@ struct Error : std::runtime_error {
 
 // Every kernel launch in this library is followed by exactly one
 // PMB_CHECK_LAUNCH(), which also counts it (pmb_launch_count).
-void count_launch();
+void count_launch(long long n = 1);
+long long launch_count();
 
 // Optional phase timing (environment PMB_PROFILE=1): CUDA events bracket a
 // named phase on a stream; elapsed times are collected when the host next

@@ -20,6 +20,22 @@ class CPRSolver {
 
  private:
   void precond(const double* r, double* z);
+  void precond_body(const double* r, double* z);
+  // The preconditioner replayed as one CUDA graph on fixed input/output
+  // vectors; re-captured when the hierarchy or the operator buffers change.
+  cudaGraphExec_t pg_exec_ = nullptr;
+  bool pg_valid_ = false;
+  long long pg_nodes_ = 0;
+  const double* pg_jac_ = nullptr;
+  const double* pg_well_ = nullptr;
+  DArray<double> pin_, pout_;
+  cudaStream_t cap_s_ = nullptr;
+  void drop_graph();
+
+ public:
+  ~CPRSolver();
+
+ private:
   void local_stage(const double* r, double* z);
   void check_status();
   double norm(const double* v);
