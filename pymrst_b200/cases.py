@@ -46,6 +46,26 @@ class OWCase:
     gravity: float
 
 
+def hydrostatic_pressure(case: "OWCase", p_top: float = None) -> np.ndarray:
+    """Cell pressures in oil-hydrostatic equilibrium below `p_top` (at the
+    shallowest cell centre), integrating dp/dz = rho_o b_o(p) g cell by cell
+    down each column."""
+    p_top = case.p0 if p_top is None else float(p_top)
+    z = np.asarray(case.grid.cells.centroids)[:, 2]
+    if not case.gravity:
+        return np.full(z.size, p_top)
+    prm = case.fluid.params
+    rho = prm.rhoS[1]
+    p = np.empty_like(z)
+    zmin = z.min()
+    # fixed-point on the compressible density (converges in a few sweeps)
+    p[:] = p_top + rho * case.gravity * (z - zmin)
+    for _ in range(5):
+        b = prm.b0[1] * np.exp(prm.c[1] * (0.5 * (p + p_top) - prm.p_ref))
+        p = p_top + rho * b * case.gravity * (z - zmin)
+    return p
+
+
 def ow_fluid() -> SimpleFluid:
     return init_simple_adi_fluid(mu=np.array([1.0, 5.0]) * CENTI * POISE, rho=[1000.0, 800.0],
                                  n=[2, 2], c=[1e-5 / BARSA, 1e-5 / BARSA], p_ref=200 * BARSA,
@@ -106,7 +126,7 @@ def channelised(dims=(60, 220, 85), cell_size=(6.1, 3.05, 0.61), seed=2, n_smoot
         for _ in range(int(rng.integers(2, 5))):
             amp = rng.uniform(2.0, 0.2 * nx)
             wav = rng.uniform(0.3 * ny, 1.5 * ny)
-            wid = rng.uniform(2.0, 0.12 * nx)
+            wid = rng.uniform(2.0, max(2.0, 0.12 * nx))
             x0 = rng.uniform(0, nx)
             ph = rng.uniform(0, 2 * np.pi)
             centre = x0 + amp * np.sin(2 * np.pi * ys / wav + ph)
