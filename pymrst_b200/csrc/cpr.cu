@@ -131,8 +131,14 @@ __global__ void ap_kernel(long long nnzb, const double4* __restrict__ A, const d
   }
 }
 
+__global__ void to_f32_kernel(long long n, const double* __restrict__ a, float* __restrict__ b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+template <class T>
 __global__ void restrict_p_kernel(int nc, const double2* __restrict__ r, const double* __restrict__ w,
-                                  double* __restrict__ bp) {
+                                  T* __restrict__ bp) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   const double2 rr = r[c];
@@ -197,8 +203,9 @@ __global__ void ext_wells_kernel(OWView v, const double* __restrict__ wj, const 
 // Right-hand side of the well-augmented pressure system: perforated cells
 // lose g_i r_w[0:2]; well rows get r_ctrl - a r_w[0:2].  Cell rows were
 // written by restrict_p_kernel.
+template <class T>
 __global__ void restrict_wells_kernel(OWView v, const double* __restrict__ r, const double* __restrict__ g_perf,
-                                      const double* __restrict__ a_well, double* __restrict__ bp) {
+                                      const double* __restrict__ a_well, T* __restrict__ bp) {
   const double* rwb = r + 2LL * v.nc;
   for (int q = threadIdx.x; q < v.npc; q += blockDim.x) {
     const int c = v.pcell[q];
@@ -217,7 +224,8 @@ __global__ void restrict_wells_kernel(OWView v, const double* __restrict__ r, co
 }
 
 // z = P xp with well bhp: cells (xp, 0); wells (0, 0, xp[nc + k]).
-__global__ void prolong_pw_kernel(int nc, int nw, const double* __restrict__ xp, double* __restrict__ z) {
+template <class T>
+__global__ void prolong_pw_kernel(int nc, int nw, const T* __restrict__ xp, double* __restrict__ z) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < nc) reinterpret_cast<double2*>(z)[t] = make_double2(xp[t], 0.0);
   if (t < nw) {
@@ -228,7 +236,8 @@ __global__ void prolong_pw_kernel(int nc, int nw, const double* __restrict__ xp,
 }
 
 // z = P xp (cells: (xp, 0); wells: 0)
-__global__ void prolong_p_kernel(int nc, int nwv, const double* __restrict__ xp, double* __restrict__ z) {
+template <class T>
+__global__ void prolong_p_kernel(int nc, int nwv, const T* __restrict__ xp, double* __restrict__ z) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < nc) reinterpret_cast<double2*>(z)[t] = make_double2(xp ? xp[t] : 0.0, 0.0);
   if (t < nwv) z[2LL * nc + t] = 0.0;
@@ -292,6 +301,9 @@ __device__ __forceinline__ double4 mul2(double4 a, double4 b) {
 __device__ __forceinline__ double2 mv2(double4 a, double2 v) {
   return make_double2(a.x * v.x + a.y * v.y, a.z * v.x + a.w * v.y);
 }
+// Block loads in FP64 arithmetic from FP64 or FP32 storage.
+__device__ __forceinline__ double4 ld4(const double4& a) { return a; }
+__device__ __forceinline__ double4 ld4(const float4& a) { return make_double4(a.x, a.y, a.z, a.w); }
 
 // Line Gauss-Seidel for one colour of vertical lines, one warp per line:
 // the lanes form the block residual r - J z of the line's cells, then lane 0
@@ -300,13 +312,14 @@ __device__ __forceinline__ double2 mv2(double4 a, double2 v) {
 // correction to z.  Lines of one colour never touch, so every warp writes
 // only its own cells.  `ys` / `gs` are per-line-position scratch (the
 // forward-eliminated right-hand side and the inverted pivots).
+template <class BT>
 __global__ void __launch_bounds__(128) line_gs_kernel(OWView v, int lstart, int lend,
                                                       const int* __restrict__ clines,
                                                       const int* __restrict__ lptr,
                                                       const int* __restrict__ lcells,
                                                       const int* __restrict__ llo,
                                                       const int* __restrict__ lup,
-                                                      const double4* __restrict__ A,
+                                                      const BT* __restrict__ A,
                                                       const double* __restrict__ wj,
                                                       const double* __restrict__ r, double* __restrict__ z,
                                                       double2* __restrict__ ys, double4* __restrict__ gs,
@@ -321,7 +334,7 @@ __global__ void __launch_bounds__(128) line_gs_kernel(OWView v, int lstart, int 
     const int c = lcells[t];
     double2 rc = reinterpret_cast<const double2*>(r)[c];
     for (int k = v.row_ptr[c]; k < v.row_ptr[c + 1]; ++k) {
-      const double2 q = mv2(A[k], z2[v.col[k]]);
+      const double2 q = mv2(ld4(A[k]), z2[v.col[k]]);
       rc.x -= q.x;
       rc.y -= q.y;
     }
@@ -345,11 +358,11 @@ __global__ void __launch_bounds__(128) line_gs_kernel(OWView v, int lstart, int 
   double2 yp = make_double2(0, 0);
   for (int t = t0; t < t1; ++t) {
     const int c = lcells[t];
-    double4 D = A[v.diag_pos[c]];
+    double4 D = ld4(A[v.diag_pos[c]]);
     double2 y = ys[t];
     if (t > t0 && llo[t] >= 0 && lup[t - 1] >= 0) {
-      const double4 LG = mul2(A[llo[t]], Gp);
-      const double4 LGU = mul2(LG, A[lup[t - 1]]);
+      const double4 LG = mul2(ld4(A[llo[t]]), Gp);
+      const double4 LGU = mul2(LG, ld4(A[lup[t - 1]]));
       D.x -= LGU.x; D.y -= LGU.y; D.z -= LGU.z; D.w -= LGU.w;
       const double2 q = mv2(LG, yp);
       y.x -= q.x;
@@ -371,7 +384,7 @@ __global__ void __launch_bounds__(128) line_gs_kernel(OWView v, int lstart, int 
   for (int t = t1 - 1; t >= t0; --t) {
     double2 y = ys[t];
     if (t + 1 < t1 && lup[t] >= 0) {
-      const double2 q = mv2(A[lup[t]], dn);
+      const double2 q = mv2(ld4(A[lup[t]]), dn);
       y.x -= q.x;
       y.y -= q.y;
     }
@@ -422,7 +435,8 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   PMB_REQUIRE(o_.restart >= 1 && o_.restart <= 60, "restart must be in 1..60");
   PMB_REQUIRE(o_.maxiter >= 1, "maxiter must be positive");
   PMB_REQUIRE(o_.rtol > 0.0, "rtol must be positive");
-  PMB_REQUIRE(o_.precision == 0, "precision must be 0 (FP64)");
+  PMB_REQUIRE(o_.precision == 0 || o_.precision == 1, "precision must be 0 (FP64) or 1 (FP32 preconditioner)");
+  f32_ = o_.precision == 1;
   const long long n = m.nvec();
   const int mm = o_.restart;
   // Krylov vectors are stored with a stride padded to 32 doubles so that every
@@ -451,8 +465,13 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   h_pin_.resize(mm + 8);
   st_pin_.resize(1);
   st_pin_[0] = 0;
-  amg_.degree = std::max(1, o_.amg_smoother_degree);
-  amg_.k_levels = std::max(0, o_.amg_cycle);
+  amg_.degree = amg32_.degree = std::max(1, o_.amg_smoother_degree);
+  amg_.k_levels = amg32_.k_levels = std::max(0, o_.amg_cycle);
+  if (f32_) {
+    jac32_.resize(4LL * m.nnzb());
+    bp32_.resize(np_);
+    xp32_.resize(np_);
+  }
   PMB_CUDA(cudaStreamSynchronize(s_));
 }
 
@@ -559,24 +578,40 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
       PMB_CHECK_LAUNCH();
     }
   };
-  const bool rebuild = !amg_.built() || since_build_ >= std::max(1, o_.amg_rebuild_interval);
+  const bool built = f32_ ? amg32_.built() : amg_.built();
+  const bool rebuild = !built || since_build_ >= std::max(1, o_.amg_rebuild_interval);
+  auto build = [&](auto& amg) {
+    if (with_wells)
+      amg.build(np_, h_erp_, h_ecol_, erp_.get(), ecol_.get(), h_ap_, o_.amg_theta,
+                std::max(16, o_.amg_coarse_size), s_);
+    else
+      amg.build(v.nc, m_.h_row_ptr(), m_.h_col(), v.row_ptr, v.col, h_ap_, o_.amg_theta,
+                std::max(16, o_.amg_coarse_size), s_);
+  };
+  if (rebuild || f32_) values(ap_.get());
   if (rebuild) {
-    values(ap_.get());
     const size_t nnz = ap_.size();
     h_ap_.resize(nnz);
     PMB_CUDA(cudaMemcpyAsync(h_ap_.data(), ap_.get(), sizeof(double) * nnz, cudaMemcpyDeviceToHost, s_));
     PMB_CUDA(cudaStreamSynchronize(s_));
-    if (with_wells)
-      amg_.build(np_, h_erp_, h_ecol_, erp_.get(), ecol_.get(), h_ap_, o_.amg_theta,
-                 std::max(16, o_.amg_coarse_size), s_);
+    if (f32_)
+      build(amg32_);
     else
-      amg_.build(v.nc, m_.h_row_ptr(), m_.h_col(), v.row_ptr, v.col, h_ap_, o_.amg_theta,
-                 std::max(16, o_.amg_coarse_size), s_);
+      build(amg_);
     since_build_ = 0;
     drop_graph();  // the hierarchy's buffers are new
   }
-  values(amg_.level0_val());
-  amg_.refresh(s_, status_.get());
+  if (f32_) {
+    const long long nnz = (long long)ap_.size();
+    to_f32_kernel<<<grid_for(nnz, 256), 256, 0, s_>>>(nnz, ap_.get(), amg32_.level0_val());
+    PMB_CHECK_LAUNCH();
+    to_f32_kernel<<<grid_for(4 * nnzb, 256), 256, 0, s_>>>(4 * nnzb, jac, jac32_.get());
+    PMB_CHECK_LAUNCH();
+    amg32_.refresh(s_, status_.get());
+  } else {
+    values(amg_.level0_val());
+    amg_.refresh(s_, status_.get());
+  }
   ++since_build_;
 }
 
@@ -590,10 +625,17 @@ void CPRSolver::local_stage(const double* r, double* z) {
       for (int q = 0; q + 1 < (int)Ls.h_color_ptr.size(); ++q) {
         const int cnt = Ls.h_color_ptr[q + 1] - Ls.h_color_ptr[q];
         if (cnt <= 0) continue;
-        line_gs_kernel<<<grid_for(32LL * cnt, 128), 128, 0, s_>>>(
-            v, Ls.h_color_ptr[q], Ls.h_color_ptr[q + 1], Ls.color_lines.get(), Ls.line_ptr.get(),
-            Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(), A, well_, r, z,
-            reinterpret_cast<double2*>(line_y_.get()), reinterpret_cast<double4*>(line_g_.get()), status_.get());
+        if (f32_)
+          line_gs_kernel<<<grid_for(32LL * cnt, 128), 128, 0, s_>>>(
+              v, Ls.h_color_ptr[q], Ls.h_color_ptr[q + 1], Ls.color_lines.get(), Ls.line_ptr.get(),
+              Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(),
+              reinterpret_cast<const float4*>(jac32_.get()), well_, r, z,
+              reinterpret_cast<double2*>(line_y_.get()), reinterpret_cast<double4*>(line_g_.get()), status_.get());
+        else
+          line_gs_kernel<<<grid_for(32LL * cnt, 128), 128, 0, s_>>>(
+              v, Ls.h_color_ptr[q], Ls.h_color_ptr[q + 1], Ls.color_lines.get(), Ls.line_ptr.get(),
+              Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(), A, well_, r, z,
+              reinterpret_cast<double2*>(line_y_.get()), reinterpret_cast<double4*>(line_g_.get()), status_.get());
         PMB_CHECK_LAUNCH();
       }
       if (v.nw) {
@@ -683,26 +725,32 @@ void CPRSolver::precond(const double* r, double* z) {
 void CPRSolver::precond_body(const double* r, double* z) {
   const OWView v = m_.view();
   const int gpro = grid_for(std::max<long long>(v.nc, 3LL * v.nw), 256);
-  if (o_.use_pressure_stage) {
+  auto pressure_stage = [&](auto* bp, auto* xp, auto& amg) {
     restrict_p_kernel<<<grid_for(v.nc, 256), 256, 0, s_>>>(v.nc, reinterpret_cast<const double2*>(r), w_.get(),
-                                                           bp_.get());
+                                                           bp);
     PMB_CHECK_LAUNCH();
     if (np_ > v.nc) {
-      restrict_wells_kernel<<<1, 256, 0, s_>>>(v, r, g_perf_.get(), a_well_.get(), bp_.get());
+      restrict_wells_kernel<<<1, 256, 0, s_>>>(v, r, g_perf_.get(), a_well_.get(), bp);
       PMB_CHECK_LAUNCH();
     }
     {
       PhaseTimer pt("cpr.amg_cycle", s_);
-      amg_.apply(bp_.get(), xp_.get(), s_);
+      amg.apply(bp, xp, s_);
     }
     if (np_ > v.nc) {
-      prolong_pw_kernel<<<gpro, 256, 0, s_>>>(v.nc, v.nw, xp_.get(), z);
+      prolong_pw_kernel<<<gpro, 256, 0, s_>>>(v.nc, v.nw, xp, z);
     } else {
-      prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, xp_.get(), z);
+      prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, xp, z);
     }
     PMB_CHECK_LAUNCH();
+  };
+  if (o_.use_pressure_stage) {
+    if (f32_)
+      pressure_stage(bp32_.get(), xp32_.get(), amg32_);
+    else
+      pressure_stage(bp_.get(), xp_.get(), amg_);
   } else {
-    prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, nullptr, z);
+    prolong_p_kernel<double><<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, nullptr, z);
     PMB_CHECK_LAUNCH();
   }
   PhaseTimer pt("cpr.local_stage", s_);

@@ -46,6 +46,11 @@ class CPRSolver {
   const double* jac_ = nullptr;
   const double* well_ = nullptr;
   AMG<double> amg_;
+  // precision 1: the preconditioner works on FP32 copies of the matrices
+  // (AMG values and vectors, line-smoother blocks) inside the FP64 FGMRES
+  bool f32_ = false;
+  AMG<float> amg32_;
+  DArray<float> jac32_, bp32_, xp32_;
   int since_build_ = 0;
   long long ld_ = 0;       // padded stride of the Krylov bases
   long long setups_ = 0, total_its_ = 0;

@@ -112,11 +112,13 @@ def test_cpr_gmres_solves_the_reference_jacobian():
     assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("name", ["ow_newton_grav.npz", "ow_newton_nograv.npz"])
-def test_newton_history_matches_reference(name):
+def test_newton_history_matches_reference(name, precision):
     d = load(name)
     g, rock, fluid, wells = ow_case(d)
-    m = GpuOilWaterModel(g, rock, fluid, wells, gravity=float(d["gravity"]), cpr_options=TIGHT)
+    m = GpuOilWaterModel(g, rock, fluid, wells, gravity=float(d["gravity"]),
+                         cpr_options=dict(TIGHT, precision=precision))
     st0 = m.initial_state(float(d["p0"][0]), float(d["sw0"][0]))
     states, its = simulate_schedule_ad(st0, m, np.full(int(d["nsteps"]), float(d["dt_days"]) * 86400.0),
                                        verbose=False)
@@ -146,9 +148,11 @@ def test_phase5_matches_reference_and_matlab():
     assert np.abs(sw.ravel() - d["mat_sw_hist"].ravel()).max() <= 5e-6 * np.abs(d["mat_sw_hist"]).max()
 
 
-def test_five_spot_step_matches_oracle():
+@pytest.mark.parametrize("precision", [0, 1])
+def test_five_spot_step_matches_oracle(precision):
     case = cases.five_spot(dims=(16, 14, 4), nsteps=4, dt_days=10.0)
-    m = GpuOilWaterModel(case.grid, case.rock, case.fluid, case.wells, gravity=case.gravity, cpr_options=TIGHT)
+    m = GpuOilWaterModel(case.grid, case.rock, case.fluid, case.wells, gravity=case.gravity,
+                         cpr_options=dict(TIGHT, precision=precision))
     prob = oow.build_problem(case.grid, case.rock, case.fluid.params, case.wells, gravity=case.gravity)
     st_o = oow.initial_state(prob, case.p0, case.sw0)
     st_g = m.initial_state(case.p0, case.sw0)
