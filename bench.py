@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--cpr", default="", help="CPR option overrides, e.g. amg_cycle=2,local_sweeps=1")
+    ap.add_argument("--max-newton", type=int, default=25,
+                    help="Newton iterations per step before a timestep cut (the reference's default is 25)")
     return ap.parse_args()
 
 
@@ -263,7 +265,7 @@ def run_ours(args):
         k, v = kv.split("=")
         copts[k] = float(v) if k in ("rtol", "amg_theta", "inner_rtol") else int(v)
     model = GpuOilWaterModel(case.grid, case.rock, case.fluid, case.wells, gravity=case.gravity,
-                             cpr_options=copts)
+                             cpr_options=copts, max_iterations=args.max_newton)
     stream = torch.cuda.current_stream()
     x = model.to_device(model.initial_state(case.p0, case.sw0))
     backup = x.clone()
@@ -366,6 +368,7 @@ def run_ours(args):
             "data": "synthetic (seeded channelised permeability, five-spot wells)",
             "config": {"workload": WORKLOAD["name"], "cells": model.nc, "wells": model.nw,
                        "dt_days": dt / 86400.0, "precision": args.precision,
+                       "max_newton_iterations": args.max_newton,
                        "newton_iterations": its_total, "krylov_iterations": kry_total, "cuts": cuts_total,
                        "cpr": {k: copts[k] for k in copts}, "amg_levels": model.cpr_levels(),
                        "l2": "inputs larger than L2 (Jacobian %.0f MB)" % (model.sizes['nnzb'] * 32 / 1e6),
