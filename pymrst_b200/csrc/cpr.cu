@@ -312,8 +312,15 @@ __device__ __forceinline__ double4 ld4(const float4& a) { return make_double4(a.
 // correction to z.  Lines of one colour never touch, so every warp writes
 // only its own cells.  `ys` / `gs` are per-line-position scratch (the
 // forward-eliminated right-hand side and the inverted pivots).
+// Lines of up to kLineSmem cells are staged in shared memory (pivot blocks,
+// couplings and right-hand side), so that lane 0's sequential recurrence reads
+// shared memory instead of waiting on global loads; longer lines use the
+// global scratch.
+constexpr int kLineSmem = 96;
+constexpr int kLineWarps = 2;
+
 template <class BT>
-__global__ void __launch_bounds__(128) line_gs_kernel(OWView v, int lstart, int lend,
+__global__ void __launch_bounds__(32 * kLineWarps) line_gs_kernel(OWView v, int lstart, int lend,
                                                       const int* __restrict__ clines,
                                                       const int* __restrict__ lptr,
                                                       const int* __restrict__ lcells,
@@ -324,12 +331,95 @@ __global__ void __launch_bounds__(128) line_gs_kernel(OWView v, int lstart, int 
                                                       const double* __restrict__ r, double* __restrict__ z,
                                                       double2* __restrict__ ys, double4* __restrict__ gs,
                                                       int* status) {
-  const int lane = threadIdx.x & 31;
+  __shared__ double4 sD[kLineWarps][kLineSmem], sL[kLineWarps][kLineSmem], sU[kLineWarps][kLineSmem];
+  __shared__ double2 sY[kLineWarps][kLineSmem];
+  __shared__ int sBad[kLineWarps];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int li = lstart + (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
   if (li >= lend) return;  // uniform across the warp
   const int L = clines[li];
   const int t0 = lptr[L], t1 = lptr[L + 1];
   const double2* z2 = reinterpret_cast<const double2*>(z);
+  if (t1 - t0 <= kLineSmem) {
+    const int len = t1 - t0;
+    const double4 zero4 = make_double4(0, 0, 0, 0);
+    for (int u = lane; u < len; u += 32) {
+      const int t = t0 + u;
+      const int c = lcells[t];
+      double2 rc = reinterpret_cast<const double2*>(r)[c];
+      for (int k = v.row_ptr[c]; k < v.row_ptr[c + 1]; ++k) {
+        const double2 q = mv2(ld4(A[k]), z2[v.col[k]]);
+        rc.x -= q.x;
+        rc.y -= q.y;
+      }
+      const int q = v.cell_pc[c];
+      if (q >= 0) {
+        const double* zw = z + 2LL * v.nc;
+        for (int jj = v.pc_ptr[q]; jj < v.pc_ptr[q + 1]; ++jj) {
+          const int i = v.pc_perf[jj];
+          const int kw = v.perf_well[i];
+          const double* B = wj + v.wl.B + 6LL * i;
+          rc.x -= B[0] * zw[3 * kw] + B[1] * zw[3 * kw + 1] + B[2] * zw[3 * kw + 2];
+          rc.y -= B[3] * zw[3 * kw] + B[4] * zw[3 * kw + 1] + B[5] * zw[3 * kw + 2];
+        }
+      }
+      sY[wib][u] = rc;
+      sD[wib][u] = ld4(A[v.diag_pos[c]]);
+      sL[wib][u] = llo[t] >= 0 ? ld4(A[llo[t]]) : zero4;
+      sU[wib][u] = lup[t] >= 0 ? ld4(A[lup[t]]) : zero4;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      int bad = 0;
+      double4 Gp = zero4;
+      double2 yp = make_double2(0, 0);
+      for (int u = 0; u < len && !bad; ++u) {
+        double4 D = sD[wib][u];
+        double2 y = sY[wib][u];
+        if (u > 0) {
+          const double4 LG = mul2(sL[wib][u], Gp);
+          const double4 LGU = mul2(LG, sU[wib][u - 1]);
+          D.x -= LGU.x; D.y -= LGU.y; D.z -= LGU.z; D.w -= LGU.w;
+          const double2 qq = mv2(LG, yp);
+          y.x -= qq.x;
+          y.y -= qq.y;
+        }
+        bool ok;
+        const double4 G = inv2(D, ok);
+        if (!ok) bad = 1;
+        sD[wib][u] = G;
+        sY[wib][u] = y;
+        Gp = G;
+        yp = y;
+      }
+      if (!bad) {
+        double2 dn = make_double2(0, 0);
+        for (int u = len - 1; u >= 0; --u) {
+          double2 y = sY[wib][u];
+          if (u + 1 < len) {
+            const double2 qq = mv2(sU[wib][u], dn);
+            y.x -= qq.x;
+            y.y -= qq.y;
+          }
+          dn = mv2(sD[wib][u], y);
+          sY[wib][u] = dn;
+        }
+      } else {
+        atomicExch(status, PMB_ERR_PIVOT);
+      }
+      sBad[wib] = bad;
+    }
+    __syncwarp();
+    if (sBad[wib]) return;
+    for (int u = lane; u < len; u += 32) {
+      const int c = lcells[t0 + u];
+      double2 zc = z2[c];
+      zc.x += sY[wib][u].x;
+      zc.y += sY[wib][u].y;
+      reinterpret_cast<double2*>(z)[c] = zc;
+    }
+    return;
+  }
   for (int t = t0 + lane; t < t1; t += 32) {
     const int c = lcells[t];
     double2 rc = reinterpret_cast<const double2*>(r)[c];
@@ -626,13 +716,13 @@ void CPRSolver::local_stage(const double* r, double* z) {
         const int cnt = Ls.h_color_ptr[q + 1] - Ls.h_color_ptr[q];
         if (cnt <= 0) continue;
         if (f32_)
-          line_gs_kernel<<<grid_for(32LL * cnt, 128), 128, 0, s_>>>(
+          line_gs_kernel<<<grid_for(32LL * cnt, 32 * kLineWarps), 32 * kLineWarps, 0, s_>>>(
               v, Ls.h_color_ptr[q], Ls.h_color_ptr[q + 1], Ls.color_lines.get(), Ls.line_ptr.get(),
               Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(),
               reinterpret_cast<const float4*>(jac32_.get()), well_, r, z,
               reinterpret_cast<double2*>(line_y_.get()), reinterpret_cast<double4*>(line_g_.get()), status_.get());
         else
-          line_gs_kernel<<<grid_for(32LL * cnt, 128), 128, 0, s_>>>(
+          line_gs_kernel<<<grid_for(32LL * cnt, 32 * kLineWarps), 32 * kLineWarps, 0, s_>>>(
               v, Ls.h_color_ptr[q], Ls.h_color_ptr[q + 1], Ls.color_lines.get(), Ls.line_ptr.get(),
               Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(), A, well_, r, z,
               reinterpret_cast<double2*>(line_y_.get()), reinterpret_cast<double4*>(line_g_.get()), status_.get());
