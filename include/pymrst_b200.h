@@ -193,6 +193,22 @@ int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* h_sizes, int32
 int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_iterations,
                 double* h_stats8);
 
+/* ------------------------------------------------------------------------
+ * AMG-preconditioned conjugate gradients for a scalar SPD CSR system: the
+ * pressure solve of incomp_tpfa (pymrst/modules/incomp/incomp_tpfa.py:172-184,
+ * `spsolve` or the caller's LinSolve).  The pattern (host row_ptr / col,
+ * sorted, diagonal present) is fixed at creation; pmb_pcg_setup refreshes
+ * the values (device, one per entry); solves start from x = 0 and stop at
+ * ||b - A x|| <= rtol ||b||.  h_info3 = [iterations, relres, ok]. */
+typedef struct pmb_pcg pmb_pcg;
+int pmb_pcg_create(int32_t n, const int32_t* h_row_ptr, const int32_t* h_col, double amg_theta,
+                   int32_t amg_coarse_size, void* stream, pmb_pcg** out);
+int pmb_pcg_destroy(pmb_pcg* p);
+int pmb_pcg_setup(pmb_pcg* p, const double* d_vals);
+int pmb_pcg_solve(pmb_pcg* p, const double* d_b, double* d_x, double rtol, int32_t maxiter,
+                  double* h_info3);
+int pmb_pcg_levels(const pmb_pcg* p, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
+
 /* Host-side aggregation of the AMG hierarchy for a CSR matrix (no device
  * needed): unknowns per level into h_sizes (up to max_levels), count in
  * *n_levels.  Exposed for testing the set-up logic. */

@@ -297,3 +297,42 @@ def fluid_params(fluid) -> FluidParams:
         if not np.allclose(mine, theirs, rtol=1e-12, atol=1e-300):
             raise ValueError("fluid is not a simple exponential-b / power-law-kr fluid")
     return prm
+
+
+@dataclass
+class BoundaryCondition:
+    """Boundary conditions on faces (reference params/wells_and_bc/types.py)."""
+    face: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int64))
+    type: List[str] = field(default_factory=list)
+    value: np.ndarray = field(default_factory=lambda: np.zeros(0))
+
+
+@dataclass
+class Source:
+    """Volumetric cell sources, injection positive."""
+    cell: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int64))
+    rate: np.ndarray = field(default_factory=lambda: np.zeros(0))
+
+
+def add_bc(bc, faces, bctype, values) -> BoundaryCondition:
+    """Append boundary conditions of one type (reference add_bc.py:13-41)."""
+    faces = np.asarray(faces, dtype=np.int64).ravel()
+    if faces.size == 0:
+        return bc
+    bc = BoundaryCondition() if bc is None else bc
+    vals = np.broadcast_to(np.asarray(values, float), faces.shape).astype(float)
+    if np.isin(faces, bc.face).any():
+        raise ValueError("new boundary condition overlaps with existing conditions")
+    bc.face = np.concatenate([bc.face, faces])
+    bc.type = list(bc.type) + [str(bctype).lower()] * faces.size
+    bc.value = np.concatenate([bc.value, vals])
+    return bc
+
+
+def add_source(src, cells, rates) -> Source:
+    """Append cell sources (reference add_source)."""
+    cells = np.asarray(cells, dtype=np.int64).ravel()
+    src = Source() if src is None else src
+    src.cell = np.concatenate([src.cell, cells])
+    src.rate = np.concatenate([src.rate, np.broadcast_to(np.asarray(rates, float), cells.shape)])
+    return src
