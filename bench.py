@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--cpr", default="", help="CPR option overrides, e.g. amg_cycle=2,local_sweeps=1")
+    ap.add_argument("--probe", type=int, default=0,
+                    help="profiling probe: run this many Newton iterations of the first step and exit")
     ap.add_argument("--max-newton", type=int, default=25,
                     help="Newton iterations per step before a timestep cut (the reference's default is 25)")
     return ap.parse_args()
@@ -270,6 +272,15 @@ def run_ours(args):
     x = model.to_device(model.initial_state(case.p0, case.sw0))
     backup = x.clone()
     dt = case.dt
+    if args.probe:
+        model.max_iterations = args.probe
+        torch.cuda.synchronize()
+        ok, nit, st = model.step_device(x, dt)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"probe": True, "cells": model.nc, "newton": nit, "krylov": int(st[2]),
+                              "amg_levels": model.cpr_levels()}), flush=True)
+        return
 
     def one_step(xv):
         """One report step with the reference's halving cuts; returns
