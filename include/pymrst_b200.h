@@ -184,6 +184,30 @@ int pmb_cpr_solve(pmb_cpr* s, const double* d_b, double* d_x, double* h_info4);
 int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
 
 /* ------------------------------------------------------------------------
+ * CPR on a caller's CSR matrix: the device side of the drop-in for
+ * CPRSolver.solve(jac, rhs, model, state)
+ * (pymrst/modules/ad_core/solvers/linear_solvers.py:426-545).
+ * The n x n matrix is in the reference's variable-blocked ordering: nph
+ * blocks of nc cell unknowns (pressure first), then n - nph*nc facility
+ * unknowns (at most 4096).  h_row_ptr / h_col: canonical CSR (columns
+ * strictly increasing in a row), fixed for the handle's life; values are
+ * given per setup.  opts as for pmb_cpr_create; local_sweeps counts
+ * block-Jacobi sweeps of the second stage (1 = the reference's single
+ * application).  h_weights (nph doubles): the decoupling weights
+ * (_weighting, :155-190: 1/b_i at the mean pressure).  h_info4 =
+ * [iterations, relres, ok, setups]; PMB_ERR_NOCONV when rtol was not
+ * reached, PMB_ERR_PIVOT for a singular cell block. */
+typedef struct pmb_csr_cpr pmb_csr_cpr;
+int pmb_csr_cpr_create(int32_t n, int32_t nc, int32_t nph, const int32_t* h_row_ptr, const int32_t* h_col,
+                       const pmb_cpr_opts* opts, void* stream, pmb_csr_cpr** out);
+int pmb_csr_cpr_destroy(pmb_csr_cpr* h);
+int pmb_csr_cpr_setup(pmb_csr_cpr* h, const double* d_values, const double* h_weights);
+int pmb_csr_cpr_solve(pmb_csr_cpr* h, const double* d_b, double* d_x, double* h_info4);
+/* y = A x with the values d_values on the handle's pattern. */
+int pmb_csr_spmv(pmb_csr_cpr* h, const double* d_values, const double* d_x, double* d_y);
+int pmb_csr_cpr_levels(const pmb_csr_cpr* h, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
+
+/* ------------------------------------------------------------------------
  * One backward-Euler step solved by Newton on the device (step,
  * two_phase_oil_water_model.py:605-657): d_x holds the state at the start
  * of the step and receives the new state.  h_stats8 = [iterations,

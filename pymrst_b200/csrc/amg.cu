@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <type_traits>
 
 #include "pmb_amg.cuh"
 
@@ -221,15 +222,56 @@ __global__ void galerkin_kernel(int nnzc, const int* __restrict__ gptr, const in
   cv[K] = (T)s;
 }
 
+// Sum over a group of LANES consecutive lanes (a power of two); every lane of
+// the warp must take part.
+template <int LANES>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Calls f(std::integral_constant<int, L>) with L the row-group width.
+template <class F>
+void with_lanes(int lanes, F&& f) {
+  switch (lanes) {
+    case 32: f(std::integral_constant<int, 32>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    default: f(std::integral_constant<int, 1>{}); break;
+  }
+}
+
+// Row-group width for a level: enough lanes that a row is read in one or two
+// coalesced passes (coarse aggregation levels have long rows).
+inline int lanes_for(long long n, long long nnz) {
+  const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
+  if (avg > 24.0) return 32;
+  if (avg > 12.0) return 16;
+  if (avg > 5.0) return 8;
+  return 4;
+}
+
 // Chebyshev on D^{-1} A over [lmax/10, lmax]: step `step` of the
 // three-term recurrence; x_out = x_in + d, d = c1 d + c2 D^{-1}(b - A x_in).
-template <class T, bool ZERO>
-__global__ void cheb_step_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                 const T* __restrict__ a, const T* __restrict__ dinv,
-                                 const T* __restrict__ b, const T* __restrict__ xin,
-                                 T* __restrict__ xout, T* __restrict__ d, const double* lmax, int step) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// LANES threads share a row.
+template <class T, bool ZERO, int LANES>
+__global__ void __launch_bounds__(256) cheb_step_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                                        const T* __restrict__ a, const T* __restrict__ dinv,
+                                                        const T* __restrict__ b, const T* __restrict__ xin,
+                                                        T* __restrict__ xout, T* __restrict__ d, const double* lmax,
+                                                        int step) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long i = t / LANES;
+  const int sub = (int)(t % LANES);
+  double ax = 0.0;
+  if (!ZERO) {
+    if (i < n)
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) ax += (double)a[k] * (double)xin[ci[k]];
+    ax = group_sum<LANES>(ax);
+  }
+  if (i >= n || sub != 0) return;
   const double lm = lmax[0];
   const double lo = lm / 10.0;
   const double theta = 0.5 * (lm + lo), delta = 0.5 * (lm - lo), sigma = theta / delta;
@@ -240,32 +282,32 @@ __global__ void cheb_step_kernel(int n, const int* __restrict__ rp, const int* _
     c2 = 2.0 * rho1 / delta;
     rho = rho1;
   }
-  double r = (double)b[i];
-  if (!ZERO) {
-    for (int k = rp[i]; k < rp[i + 1]; ++k) r -= (double)a[k] * (double)xin[ci[k]];
-  }
-  r *= (double)dinv[i];
+  const double r = ((double)b[i] - ax) * (double)dinv[i];
   const double dn = (step == 0 ? 0.0 : c1 * (double)d[i]) + c2 * r;
   d[i] = (T)dn;
   xout[i] = (T)((ZERO ? 0.0 : (double)xin[i]) + dn);
 }
 
-// b_c[I] = sum over members i of (b_i - (A x)_i)
-template <class T>
-__global__ void restrict_residual_kernel(int nc, const int* __restrict__ cptr, const int* __restrict__ cmem,
-                                         const int* __restrict__ rp, const int* __restrict__ ci,
-                                         const T* __restrict__ a, const T* __restrict__ b,
-                                         const T* __restrict__ x, T* __restrict__ bc) {
-  const int I = blockIdx.x * blockDim.x + threadIdx.x;
-  if (I >= nc) return;
+// b_c[I] = sum over members i of (b_i - (A x)_i); LANES threads per aggregate
+// share each member row.
+template <class T, int LANES>
+__global__ void __launch_bounds__(256) restrict_residual_kernel(int nc, const int* __restrict__ cptr,
+                                                                const int* __restrict__ cmem,
+                                                                const int* __restrict__ rp, const int* __restrict__ ci,
+                                                                const T* __restrict__ a, const T* __restrict__ b,
+                                                                const T* __restrict__ x, T* __restrict__ bc) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long I = t / LANES;
+  const int sub = (int)(t % LANES);
   double s = 0.0;
-  for (int m = cptr[I]; m < cptr[I + 1]; ++m) {
-    const int i = cmem[m];
-    double r = (double)b[i];
-    for (int k = rp[i]; k < rp[i + 1]; ++k) r -= (double)a[k] * (double)x[ci[k]];
-    s += r;
-  }
-  bc[I] = (T)s;
+  if (I < nc)
+    for (int m = cptr[I]; m < cptr[I + 1]; ++m) {
+      const int i = cmem[m];
+      if (sub == 0) s += (double)b[i];
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s -= (double)a[k] * (double)x[ci[k]];
+    }
+  s = group_sum<LANES>(s);
+  if (I < nc && sub == 0) bc[I] = (T)s;
 }
 
 template <class T>
@@ -365,15 +407,18 @@ __global__ void dense_apply_kernel(int n, const double* __restrict__ Inv, const 
 
 // K-cycle pieces ------------------------------------------------------------
 
-template <class T>
+template <class T, int LANES>
 __global__ void __launch_bounds__(256) csr_spmv_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                                                        const T* __restrict__ a, const T* __restrict__ x,
                                                        T* __restrict__ y) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long i = t / LANES;
+  const int sub = (int)(t % LANES);
   double s = 0.0;
-  for (int k = rp[i]; k < rp[i + 1]; ++k) s += (double)a[k] * (double)x[ci[k]];
-  y[i] = (T)s;
+  if (i < n)
+    for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s += (double)a[k] * (double)x[ci[k]];
+  s = group_sum<LANES>(s);
+  if (i < n && sub == 0) y[i] = (T)s;
 }
 
 // NDOT = 2: [v1.v1, v1.rc]; NDOT = 5: [v1.v1, v1.v2, v2.v2, v1.rc, v2.rc]
@@ -404,13 +449,20 @@ __global__ void __launch_bounds__(256) kdots_kernel(int n, const T* __restrict__
 }
 
 // mode 0: coef[0] = (v1.rc)/(v1.v1); mode 1: least-squares pair
-// [coef[1], coef[2]] minimising |rc - y0 v1 - y1 v2|.
+// [coef[1], coef[2]] minimising |rc - y0 v1 - y1 v2|.  One warp sums each
+// dot's G block partials; launched with 5 warps.
 __global__ void kcoef_kernel(int G, int mode, const double* __restrict__ part, double* __restrict__ coef) {
-  if (threadIdx.x != 0) return;
+  __shared__ double d[5];
   const int nd = mode == 0 ? 2 : 5;
-  double d[5] = {0, 0, 0, 0, 0};
-  for (int q = 0; q < nd; ++q)
-    for (int b = 0; b < G; ++b) d[q] += part[q * G + b];
+  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+  if (q < nd) {
+    double s = 0.0;
+    for (int b = lane; b < G; b += 32) s += part[q * G + b];
+    s = warp_sum(s);
+    if (lane == 0) d[q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   if (mode == 0) {
     coef[0] = d[0] > 0.0 ? d[1] / d[0] : 0.0;
   } else {
@@ -467,6 +519,7 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
       L.row_ptr = L.own_row_ptr.get();
       L.col = L.own_col.get();
     }
+    L.lanes = lanes_for(L.n, L.nnz);
     L.val.resize(L.nnz);
     L.dinv.resize(L.n);
     L.x.resize(L.n);
@@ -535,25 +588,33 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
 
 template <class T>
 void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start) {
-  // ping-pong between x and L.t; the result ends in x
-  const int g = grid_for(L.n, 256);
+  // degree steps ping-pong between x and L.t, ordered so that the last one
+  // writes x; only an odd step count from a non-zero start needs a copy
+  const int steps = std::max(1, degree);
+  T* t = L.t.get();
   T* cur = x;
-  T* nxt = L.t.get();
   int step = 0;
-  if (zero_start) {
-    cheb_step_kernel<T, true><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, nullptr,
-                                                cur, L.r.get(), L.lmax.get(), 0);
-    PMB_CHECK_LAUNCH();
-    step = 1;
-  }
-  for (; step < degree; ++step) {
-    cheb_step_kernel<T, false><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, cur,
-                                                 nxt, L.r.get(), L.lmax.get(), step);
-    PMB_CHECK_LAUNCH();
-    std::swap(cur, nxt);
-  }
+  with_lanes(L.lanes, [&](auto ln) {
+    constexpr int LN = decltype(ln)::value;
+    const int g = grid_for((long long)L.n * LN, 256);
+    if (zero_start) {
+      T* out = (steps % 2 == 1) ? x : t;
+      cheb_step_kernel<T, true, LN><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, nullptr,
+                                                      out, L.r.get(), L.lmax.get(), 0);
+      PMB_CHECK_LAUNCH();
+      cur = out;
+      step = 1;
+    }
+    for (; step < steps; ++step) {
+      T* out = (cur == x) ? t : x;
+      cheb_step_kernel<T, false, LN><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, cur,
+                                                       out, L.r.get(), L.lmax.get(), step);
+      PMB_CHECK_LAUNCH();
+      cur = out;
+    }
+  });
   if (cur != x) {
-    copy_kernel<T><<<g, 256, 0, s>>>(L.n, cur, x);
+    copy_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, cur, x);
     PMB_CHECK_LAUNCH();
   }
 }
@@ -571,9 +632,12 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
   T* bc = next_is_coarsest ? co_b_.get() : levels_[l + 1].b.get();
   T* xc = next_is_coarsest ? co_x_.get() : levels_[l + 1].x.get();
   smooth(L, b, x, s, true);
-  restrict_residual_kernel<T><<<grid_for(nc, 256), 256, 0, s>>>(nc, L.cptr.get(), L.cmem.get(), L.row_ptr,
-                                                                 L.col, L.val.get(), b, x, bc);
-  PMB_CHECK_LAUNCH();
+  with_lanes(L.lanes, [&](auto ln) {
+    constexpr int LN = decltype(ln)::value;
+    restrict_residual_kernel<T, LN><<<grid_for((long long)nc * LN, 256), 256, 0, s>>>(
+        nc, L.cptr.get(), L.cmem.get(), L.row_ptr, L.col, L.val.get(), b, x, bc);
+    PMB_CHECK_LAUNCH();
+  });
   coarse_correction(l, bc, xc, s);
   prolong_add_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.agg.get(), xc, x);
   PMB_CHECK_LAUNCH();
@@ -595,20 +659,28 @@ void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
   const int n = C.n, g = grid_for(n, 256);
   const int G = std::min(2 * kNumSM, g);
   cycle(l + 1, rc, C.kc1.get(), s);
-  csr_spmv_kernel<T><<<g, 256, 0, s>>>(n, C.row_ptr, C.col, C.val.get(), C.kc1.get(), C.kv1.get());
-  PMB_CHECK_LAUNCH();
+  with_lanes(C.lanes, [&](auto ln) {
+    constexpr int LN = decltype(ln)::value;
+    csr_spmv_kernel<T, LN><<<grid_for((long long)n * LN, 256), 256, 0, s>>>(n, C.row_ptr, C.col, C.val.get(),
+                                                                            C.kc1.get(), C.kv1.get());
+    PMB_CHECK_LAUNCH();
+  });
   kdots_kernel<T, 2><<<G, 256, 0, s>>>(n, C.kv1.get(), nullptr, rc, C.kpart.get());
   PMB_CHECK_LAUNCH();
-  kcoef_kernel<<<1, 32, 0, s>>>(G, 0, C.kpart.get(), C.kcoef.get());
+  kcoef_kernel<<<1, 160, 0, s>>>(G, 0, C.kpart.get(), C.kcoef.get());
   PMB_CHECK_LAUNCH();
   kaxpy_kernel<T><<<g, 256, 0, s>>>(n, rc, C.kv1.get(), C.kcoef.get(), C.kr2.get());
   PMB_CHECK_LAUNCH();
   cycle(l + 1, C.kr2.get(), C.kc2.get(), s);
-  csr_spmv_kernel<T><<<g, 256, 0, s>>>(n, C.row_ptr, C.col, C.val.get(), C.kc2.get(), C.kv2.get());
-  PMB_CHECK_LAUNCH();
+  with_lanes(C.lanes, [&](auto ln) {
+    constexpr int LN = decltype(ln)::value;
+    csr_spmv_kernel<T, LN><<<grid_for((long long)n * LN, 256), 256, 0, s>>>(n, C.row_ptr, C.col, C.val.get(),
+                                                                            C.kc2.get(), C.kv2.get());
+    PMB_CHECK_LAUNCH();
+  });
   kdots_kernel<T, 5><<<G, 256, 0, s>>>(n, C.kv1.get(), C.kv2.get(), rc, C.kpart.get());
   PMB_CHECK_LAUNCH();
-  kcoef_kernel<<<1, 32, 0, s>>>(G, 1, C.kpart.get(), C.kcoef.get());
+  kcoef_kernel<<<1, 160, 0, s>>>(G, 1, C.kpart.get(), C.kcoef.get());
   PMB_CHECK_LAUNCH();
   kcombine_kernel<T><<<g, 256, 0, s>>>(n, C.kc1.get(), C.kc2.get(), C.kcoef.get(), ec);
   PMB_CHECK_LAUNCH();

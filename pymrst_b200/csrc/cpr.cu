@@ -18,85 +18,6 @@ namespace pmb {
 
 constexpr int kRedBlocks = 2 * kNumSM;
 
-// ---- reductions -----------------------------------------------------------
-
-// part[i * G + blk] = partial dot(V_i, w) over this block's contiguous chunk.
-__global__ void __launch_bounds__(256) mdot_kernel(long long n, const double* __restrict__ V, long long ld,
-                                                   int nv, const double* __restrict__ w,
-                                                   double* __restrict__ part) {
-  __shared__ double sh[32];
-  const long long chunk = (n + gridDim.x - 1) / gridDim.x;
-  const long long e0 = blockIdx.x * chunk;
-  const long long e1 = min(n, e0 + chunk);
-  for (int i = 0; i < nv; ++i) {
-    const double* vi = V + i * ld;
-    double s = 0.0;
-    for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) s += vi[e] * w[e];
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) part[(long long)i * gridDim.x + blockIdx.x] = s;
-  }
-}
-
-// out[i] = sum_b part[i*G+b] (fixed order); acc[i] += out[i] when given;
-// out[0] = sqrt(out[0]) when do_sqrt.
-__global__ void mdot_final_kernel(int nv, int G, const double* __restrict__ part, double* __restrict__ out,
-                                  double* __restrict__ acc, int do_sqrt) {
-  const int i = threadIdx.x;
-  if (i >= nv) return;
-  double s = 0.0;
-  for (int b = 0; b < G; ++b) s += part[(long long)i * G + b];
-  if (do_sqrt) s = sqrt(s);
-  out[i] = s;
-  if (acc) acc[i] += s;
-}
-
-// w -= sum_i h[i] V_i
-__global__ void __launch_bounds__(256) vupdate_kernel(long long n, const double* __restrict__ V, long long ld,
-                                                      int nv, const double* __restrict__ h,
-                                                      double* __restrict__ w) {
-  __shared__ double hs[64];
-  for (int i = threadIdx.x; i < nv; i += blockDim.x) hs[i] = h[i];
-  __syncthreads();
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
-    double s = w[e];
-    for (int i = 0; i < nv; ++i) s -= hs[i] * V[i * ld + e];
-    w[e] = s;
-  }
-}
-
-// x += sum_i y[i] Z_i
-__global__ void __launch_bounds__(256) xupdate_kernel(long long n, const double* __restrict__ Z, long long ld,
-                                                      int nv, const double* __restrict__ y,
-                                                      double* __restrict__ x) {
-  __shared__ double ys[64];
-  for (int i = threadIdx.x; i < nv; i += blockDim.x) ys[i] = y[i];
-  __syncthreads();
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
-    double s = x[e];
-    for (int i = 0; i < nv; ++i) s += ys[i] * Z[i * ld + e];
-    x[e] = s;
-  }
-}
-
-// out = a / s[0]
-__global__ void scale_kernel(long long n, const double* __restrict__ a, const double* __restrict__ s,
-                             double* __restrict__ out) {
-  const double inv = 1.0 / s[0];
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x)
-    out[e] = a[e] * inv;
-}
-
-// r = b - y
-__global__ void sub_kernel(long long n, const double* __restrict__ b, const double* __restrict__ y,
-                           double* __restrict__ r) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x)
-    r[e] = b[e] - y[e];
-}
-
 // ---- CPR pieces -----------------------------------------------------------
 
 __global__ void __launch_bounds__(256) psum_kernel(int nc, const double2* __restrict__ x, double* part) {
@@ -522,19 +443,15 @@ __global__ void gs_well_kernel(OWView v, const double* __restrict__ wj, const do
 // ---- host -------------------------------------------------------------------
 
 CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.stream()) {
-  PMB_REQUIRE(o_.restart >= 1 && o_.restart <= 60, "restart must be in 1..60");
+  PMB_REQUIRE(o_.restart >= 1 && o_.restart <= kMaxRestart, "restart must be in 1..60");
   PMB_REQUIRE(o_.maxiter >= 1, "maxiter must be positive");
   PMB_REQUIRE(o_.rtol > 0.0, "rtol must be positive");
   PMB_REQUIRE(o_.precision == 0 || o_.precision == 1, "precision must be 0 (FP64) or 1 (FP32 preconditioner)");
   f32_ = o_.precision == 1;
-  const long long n = m.nvec();
-  const int mm = o_.restart;
-  // Krylov vectors are stored with a stride padded to 32 doubles so that every
-  // slice V_j / Z_j stays 256-byte aligned for the double2 / double4 kernels.
-  ld_ = (n + 31) / 32 * 32;
+  kry_.init(m.nvec(), o_.restart, s_);
   w_.resize(2);
-  part_.resize((size_t)kRedBlocks * (mm + 2));
-  status_.resize(1);
+  part_.resize((size_t)kRedBlocks);
+  status_.resize(1);  // device error status
   status_.zero(s_);
   np_ = m.nc();
   if (m.nw() > 0) build_pressure_pattern();
@@ -545,14 +462,6 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
     line_g_.resize(4LL * m.nc());
   }
   ap_.resize(np_ > m.nc() ? h_ecol_.size() : (size_t)m.nnzb());
-  V_.resize((size_t)(mm + 1) * ld_);
-  Z_.resize((size_t)mm * ld_);
-  wv_.resize(n);
-  r_.resize(n);
-  hcol_.resize(mm + 2);
-  htmp_.resize(mm + 2);
-  y_.resize(mm + 1);
-  h_pin_.resize(mm + 8);
   st_pin_.resize(1);
   st_pin_[0] = 0;
   amg_.degree = amg32_.degree = std::max(1, o_.amg_smoother_degree);
@@ -689,7 +598,7 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
     else
       build(amg_);
     since_build_ = 0;
-    drop_graph();  // the hierarchy's buffers are new
+    graph_.invalidate();  // the hierarchy's buffers are new
   }
   if (f32_) {
     const long long nnz = (long long)ap_.size();
@@ -750,66 +659,14 @@ void CPRSolver::local_stage(const double* r, double* z) {
   }
 }
 
-CPRSolver::~CPRSolver() {
-  drop_graph();
-  if (cap_s_) cudaStreamDestroy(cap_s_);
-}
-
-void CPRSolver::drop_graph() {
-  if (pg_exec_) cudaGraphExecDestroy(pg_exec_);
-  pg_exec_ = nullptr;
-  pg_valid_ = false;
-}
-
 void CPRSolver::precond(const double* r, double* z) {
-  static const bool use_graph = [] {
-    const char* e = std::getenv("PMB_NO_GRAPH");
-    return !(e && e[0] == '1');
-  }();
-  if (!use_graph || PhaseTimer::enabled()) {
-    precond_body(r, z);
-    return;
-  }
-  const long long n = m_.nvec();
-  if (!pin_.size()) {
-    pin_.resize(n);
-    pout_.resize(n);
-  }
-  if (!pg_valid_ || pg_jac_ != jac_ || pg_well_ != well_) {
-    drop_graph();
-    // capture on a private stream (the legacy default stream cannot be
-    // captured); the graph is then launched on the solver's stream
-    if (!cap_s_) PMB_CUDA(cudaStreamCreateWithFlags(&cap_s_, cudaStreamNonBlocking));
-    PMB_CUDA(cudaStreamSynchronize(s_));
-    const long long before = launch_count();
-    const cudaStream_t saved = s_;
-    s_ = cap_s_;
-    PMB_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-    cudaGraph_t g = nullptr;
-    try {
-      precond_body(pin_.get(), pout_.get());
-    } catch (...) {
-      cudaStreamEndCapture(s_, &g);
-      if (g) cudaGraphDestroy(g);
-      s_ = saved;
-      throw;
-    }
-    const cudaError_t ce = cudaStreamEndCapture(s_, &g);
-    s_ = saved;
-    PMB_CUDA(ce);
-    pg_nodes_ = launch_count() - before;
-    count_launch(-pg_nodes_);  // captured, not launched
-    const cudaError_t e = cudaGraphInstantiate(&pg_exec_, g, 0);
-    cudaGraphDestroy(g);
-    PMB_CUDA(e);
-    pg_valid_ = true;
+  // the graph holds the operator's buffer addresses: re-capture when they move
+  if (pg_jac_ != jac_ || pg_well_ != well_) {
+    graph_.invalidate();
     pg_jac_ = jac_;
     pg_well_ = well_;
   }
-  PMB_CUDA(cudaMemcpyAsync(pin_.get(), r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s_));
-  PMB_CUDA(cudaGraphLaunch(pg_exec_, s_));
-  count_launch(pg_nodes_);
-  PMB_CUDA(cudaMemcpyAsync(z, pout_.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, s_));
+  graph_.run(m_.nvec(), r, z, s_, [this](const double* a, double* b) { precond_body(a, b); });
 }
 
 void CPRSolver::precond_body(const double* r, double* z) {
@@ -847,123 +704,17 @@ void CPRSolver::precond_body(const double* r, double* z) {
   local_stage(r, z);
 }
 
-double CPRSolver::norm(const double* a) {
-  const long long n = m_.nvec();
-  mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, a, n, 1, a, part_.get());
-  PMB_CHECK_LAUNCH();
-  mdot_final_kernel<<<1, 32, 0, s_>>>(1, kRedBlocks, part_.get(), htmp_.get(), nullptr, 1);
-  PMB_CHECK_LAUNCH();
-  PMB_CUDA(cudaMemcpyAsync(h_pin_.get(), htmp_.get(), sizeof(double), cudaMemcpyDeviceToHost, s_));
-  PMB_CUDA(cudaStreamSynchronize(s_));
-  return h_pin_[0];
-}
-
 bool CPRSolver::solve(const double* b, double* x, double* info) {
-  const long long n = m_.nvec();
-  const int mm = o_.restart;
-  const int gv = 4 * kNumSM;
   PMB_REQUIRE(jac_ != nullptr, "pmb_cpr_setup must run before pmb_cpr_solve");
-  PMB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, s_));
-  const double beta0 = norm(b);
-  info[0] = 0; info[1] = 0; info[2] = 1; info[3] = (double)setups_;
-  if (!std::isfinite(beta0)) throw Error(PMB_ERR_NONFINITE, "non-finite right-hand side");
-  if (beta0 == 0.0) return true;
-  const double target = o_.rtol * beta0;
-  PMB_CUDA(cudaMemcpyAsync(r_.get(), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s_));
-  double beta = beta0;
-  int its = 0;
-  std::vector<double> H((size_t)(mm + 1) * mm), cs(mm), sn(mm), g(mm + 1), y(mm);
-  bool converged = false;
-  while (its < o_.maxiter) {
-    h_pin_[0] = beta;
-    PMB_CUDA(cudaMemcpyAsync(htmp_.get(), h_pin_.get(), sizeof(double), cudaMemcpyHostToDevice, s_));
-    scale_kernel<<<gv, 256, 0, s_>>>(n, r_.get(), htmp_.get(), V_.get());
-    PMB_CHECK_LAUNCH();
-    std::fill(g.begin(), g.end(), 0.0);
-    g[0] = beta;
-    int j = 0;
-    bool stop = false;
-    for (; j < mm && !stop; ++j) {
-      double* vj = V_.get() + (size_t)j * ld_;
-      double* zj = Z_.get() + (size_t)j * ld_;
-      precond(vj, zj);
-      {
-        PhaseTimer pt("gmres.spmv", s_);
-        m_.spmv(jac_, well_, zj, wv_.get());
-      }
-      // classical Gram-Schmidt, twice
-      const int nv = j + 1;
-      PhaseTimer pt_orth("gmres.orthogonalise", s_);
-      mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, V_.get(), ld_, nv, wv_.get(), part_.get());
-      PMB_CHECK_LAUNCH();
-      mdot_final_kernel<<<1, 64, 0, s_>>>(nv, kRedBlocks, part_.get(), hcol_.get(), nullptr, 0);
-      PMB_CHECK_LAUNCH();
-      vupdate_kernel<<<gv, 256, 0, s_>>>(n, V_.get(), ld_, nv, hcol_.get(), wv_.get());
-      PMB_CHECK_LAUNCH();
-      mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, V_.get(), ld_, nv, wv_.get(), part_.get());
-      PMB_CHECK_LAUNCH();
-      mdot_final_kernel<<<1, 64, 0, s_>>>(nv, kRedBlocks, part_.get(), htmp_.get(), hcol_.get(), 0);
-      PMB_CHECK_LAUNCH();
-      vupdate_kernel<<<gv, 256, 0, s_>>>(n, V_.get(), ld_, nv, htmp_.get(), wv_.get());
-      PMB_CHECK_LAUNCH();
-      mdot_kernel<<<kRedBlocks, 256, 0, s_>>>(n, wv_.get(), n, 1, wv_.get(), part_.get());
-      PMB_CHECK_LAUNCH();
-      mdot_final_kernel<<<1, 32, 0, s_>>>(1, kRedBlocks, part_.get(), hcol_.get() + nv, nullptr, 1);
-      PMB_CHECK_LAUNCH();
-      scale_kernel<<<gv, 256, 0, s_>>>(n, wv_.get(), hcol_.get() + nv, V_.get() + (size_t)(j + 1) * ld_);
-      PMB_CHECK_LAUNCH();
-      PMB_CUDA(cudaMemcpyAsync(h_pin_.get(), hcol_.get(), sizeof(double) * (nv + 1), cudaMemcpyDeviceToHost, s_));
-      PMB_CUDA(cudaMemcpyAsync(st_pin_.get(), status_.get(), sizeof(int), cudaMemcpyDeviceToHost, s_));
-      PMB_CUDA(cudaStreamSynchronize(s_));
-      if (st_pin_[0] != 0) check_status();
-      for (int i = 0; i <= nv; ++i) {
-        if (!std::isfinite(h_pin_[i])) throw Error(PMB_ERR_NONFINITE, "non-finite Krylov scalar in GMRES");
-        H[(size_t)i * mm + j] = h_pin_[i];
-      }
-      for (int i = 0; i < j; ++i) {
-        const double t0 = cs[i] * H[(size_t)i * mm + j] + sn[i] * H[(size_t)(i + 1) * mm + j];
-        H[(size_t)(i + 1) * mm + j] = -sn[i] * H[(size_t)i * mm + j] + cs[i] * H[(size_t)(i + 1) * mm + j];
-        H[(size_t)i * mm + j] = t0;
-      }
-      const double a = H[(size_t)j * mm + j], bb = H[(size_t)(j + 1) * mm + j];
-      const double den = std::hypot(a, bb);
-      cs[j] = den == 0.0 ? 1.0 : a / den;
-      sn[j] = den == 0.0 ? 0.0 : bb / den;
-      H[(size_t)j * mm + j] = den;
-      H[(size_t)(j + 1) * mm + j] = 0.0;
-      g[j + 1] = -sn[j] * g[j];
-      g[j] = cs[j] * g[j];
-      ++its;
-      if (std::fabs(g[j + 1]) <= target || its >= o_.maxiter || bb == 0.0) stop = true;
-    }
-    // y = H^{-1} g (upper triangular, j x j), x += Z y
-    for (int i = j - 1; i >= 0; --i) {
-      double s = g[i];
-      for (int k = i + 1; k < j; ++k) s -= H[(size_t)i * mm + k] * y[k];
-      const double d = H[(size_t)i * mm + i];
-      y[i] = d == 0.0 ? 0.0 : s / d;
-    }
-    for (int i = 0; i < j; ++i) h_pin_[i] = y[i];
-    PMB_CUDA(cudaMemcpyAsync(y_.get(), h_pin_.get(), sizeof(double) * j, cudaMemcpyHostToDevice, s_));
-    xupdate_kernel<<<gv, 256, 0, s_>>>(n, Z_.get(), ld_, j, y_.get(), x);
-    PMB_CHECK_LAUNCH();
-    // true residual
-    m_.spmv(jac_, well_, x, wv_.get());
-    sub_kernel<<<gv, 256, 0, s_>>>(n, b, wv_.get(), r_.get());
-    PMB_CHECK_LAUNCH();
-    beta = norm(r_.get());
-    if (!std::isfinite(beta)) throw Error(PMB_ERR_NONFINITE, "non-finite residual in GMRES");
-    if (beta <= target) {
-      converged = true;
-      break;
-    }
-  }
-  total_its_ += its;
-  info[0] = its;
-  info[1] = beta / beta0;
-  info[2] = converged ? 1 : 0;
+  auto op = [this](const double* in, double* out) {
+    PhaseTimer pt("gmres.spmv", s_);
+    m_.spmv(jac_, well_, in, out);
+  };
+  auto pc = [this](const double* in, double* out) { precond(in, out); };
+  const bool ok = kry_.solve(op, pc, b, x, o_.rtol, o_.maxiter, info, status_.get(), [this] { check_status(); });
+  total_its_ += (long long)info[0];
   info[3] = (double)setups_;
-  return converged;
+  return ok;
 }
 
 }  // namespace pmb

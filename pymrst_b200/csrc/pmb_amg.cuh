@@ -32,6 +32,7 @@ std::vector<AMGHostLevel> amg_build_hierarchy(int n, const int* row_ptr, const i
 template <class T>
 struct AMGLevel {
   int n = 0, nnz = 0;
+  int lanes = 1;  // threads per row in the row-wise kernels (from the mean row length)
   const int* row_ptr = nullptr;  // device (level 0 borrows the operator pattern)
   const int* col = nullptr;
   DArray<int> own_row_ptr, own_col;

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "pmb_amg.cuh"
+#include "pmb_krylov.cuh"
 #include "pmb_ow.cuh"
 
 namespace pmb {
@@ -21,30 +22,20 @@ class CPRSolver {
  private:
   void precond(const double* r, double* z);
   void precond_body(const double* r, double* z);
-  // The preconditioner replayed as one CUDA graph on fixed input/output
-  // vectors; re-captured when the hierarchy or the operator buffers change.
-  cudaGraphExec_t pg_exec_ = nullptr;
-  bool pg_valid_ = false;
-  long long pg_nodes_ = 0;
-  const double* pg_jac_ = nullptr;
-  const double* pg_well_ = nullptr;
-  DArray<double> pin_, pout_;
-  cudaStream_t cap_s_ = nullptr;
-  void drop_graph();
-
- public:
-  ~CPRSolver();
-
- private:
   void local_stage(const double* r, double* z);
   void check_status();
-  double norm(const double* v);
 
   OWModel& m_;
   pmb_cpr_opts o_;
   cudaStream_t s_;
   const double* jac_ = nullptr;
   const double* well_ = nullptr;
+  Fgmres kry_;
+  // The preconditioner replayed as one CUDA graph; re-captured when the
+  // hierarchy or the operator buffers change.
+  GraphedApply graph_;
+  const double* pg_jac_ = nullptr;
+  const double* pg_well_ = nullptr;
   AMG<double> amg_;
   // precision 1: the preconditioner works on FP32 copies of the matrices
   // (AMG values and vectors, line-smoother blocks) inside the FP64 FGMRES
@@ -52,13 +43,11 @@ class CPRSolver {
   AMG<float> amg32_;
   DArray<float> jac32_, bp32_, xp32_;
   int since_build_ = 0;
-  long long ld_ = 0;       // padded stride of the Krylov bases
   long long setups_ = 0, total_its_ = 0;
   DArray<double> w_;        // quasi-IMPES weights (2)
   DArray<double> part_;     // reduction partials
   DArray<int> status_;
   DArray<double> bp_, xp_, ap_;  // pressure system rhs / solution / values for aggregation
-  DArray<double> V_, Z_, wv_, r_, hcol_, htmp_, y_;
   DArray<double> line_y_, line_g_;  // line Gauss-Seidel scratch (per line position)
   // Pressure system with one bhp unknown per well (np_ = nc + nw): CSR
   // pattern, the position of every cell block in it (bsr2ext), of each
@@ -70,7 +59,6 @@ class CPRSolver {
   DArray<double> g_perf_, a_well_;
   void build_pressure_pattern();
   void pressure_values(double* ext);
-  PinnedArray<double> h_pin_;
   PinnedArray<int> st_pin_;
   std::vector<double> h_ap_;
 };

@@ -1,0 +1,227 @@
+"""`GpuCPRSolver`: the reference's `CPRSolver` protocol on the GPU.
+
+Drop-in for `CPRSolver` (pymrst/modules/ad_core/solvers/linear_solvers.py:
+110-545): same constructor arguments, `solve(jac, rhs, model=None,
+state=None, dt=None) -> ndarray`, `last_iterations`, `last_local_stage`,
+`last_fallback`, and `RuntimeError` when GMRES does not converge (which the
+nonlinear drivers turn into a timestep cut).  The host CSR is copied to the
+device each call; the pattern analysis and the AMG aggregation are kept while
+the sparsity pattern is unchanged.
+
+Differences, all of them loud:
+  * no host fallback.  The reference solves with SuperLU when the model does
+    not meet CPR's contract (`.G`, `.n_phases`, `.fluid.{disgas, vapoil,
+    b}`, :396-459); here that is a `ValueError` naming what is missing.
+  * the local stage is block-Jacobi on the device.  `local_stage="ilu"` and
+    an `elliptic_solver` (a host solver) are refused with `ValueError`;
+    "auto" is block-Jacobi for every model.  `fallback_to_ilu` retries a
+    failed solve with three block-Jacobi sweeps instead of an ILU.
+  * the pressure stage is always the device aggregation AMG (`use_amg` and
+    `amg_tol` are accepted and have no effect); `amg_cycles` must be 1.
+"""
+
+from __future__ import annotations
+
+from typing import Any, Optional
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _native as N
+
+
+def _value(x):
+    return getattr(x, "val", x)
+
+
+def _get(state, name):
+    try:
+        return state[name]
+    except (TypeError, KeyError):
+        return getattr(state, name)
+
+
+class GpuCPRSolver:
+    """Two-stage CPR preconditioner with an FGMRES outer iteration, on the GPU."""
+
+    def __init__(self, rtol: float = 1e-8, maxiter: int = 200, restart: int = 50,
+                 ilu_drop_tol: float = 1e-2, ilu_fill_factor: float = 1.5, use_amg: bool = True,
+                 amg_tol: float = 1e-3, use_pressure_stage: bool = True, local_stage: str = "auto",
+                 amg_cycles: int = 1, fallback_to_ilu: bool = True, amg_rebuild_interval: int = 8,
+                 elliptic_solver: Optional[Any] = None, precision: str = "fp64", local_sweeps: int = 1):
+        if local_stage not in ("auto", "block_jacobi", "ilu"):
+            raise ValueError(f"unknown local_stage {local_stage!r}")
+        if local_stage == "ilu":
+            raise ValueError("the device solver has no ILU local stage; use 'block_jacobi' or 'auto'")
+        if elliptic_solver is not None:
+            raise ValueError("an injected host elliptic_solver cannot run inside the device preconditioner")
+        if int(amg_rebuild_interval) < 1:
+            raise ValueError("amg_rebuild_interval must be positive")
+        if int(amg_cycles) != 1:
+            raise ValueError("the device pressure stage applies exactly one AMG cycle (amg_cycles=1)")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        if not 1 <= int(restart) <= 60:
+            raise ValueError("restart must be in 1..60")
+        self.rtol = float(rtol)
+        self.maxiter = int(maxiter)
+        self.restart = int(restart)
+        self.ilu_drop_tol = ilu_drop_tol
+        self.ilu_fill_factor = ilu_fill_factor
+        self.use_amg = use_amg
+        self.amg_tol = amg_tol
+        self.use_pressure_stage = bool(use_pressure_stage)
+        self.local_stage = local_stage
+        self.amg_cycles = int(amg_cycles)
+        self.fallback_to_ilu = bool(fallback_to_ilu)
+        self.amg_rebuild_interval = int(amg_rebuild_interval)
+        self.elliptic_solver = None
+        self.precision = precision
+        self.local_sweeps = max(1, int(local_sweeps))
+        self.last_iterations = 0
+        self.last_local_stage: Optional[str] = None
+        self.last_fallback: tuple = ()
+        self.last_relres = float("nan")
+        self._pattern = None      # (n, nc, nph, indptr, indices) of the cached handles
+        self._handles = {}        # local sweeps -> handle
+
+    # -- the reference's contract --------------------------------------------
+    @staticmethod
+    def _unmet_requirements(model) -> list:
+        """What a model lacks before CPR can build its pressure stage
+        (CPRSolver._unmet_requirements, linear_solvers.py:396-424)."""
+        if model is None:
+            return ["no model was supplied"]
+        missing = []
+        if not hasattr(model, "G"):
+            missing.append("model has no .G (a grid under that exact name)"
+                           + (" - it has .g" if hasattr(model, "g") else ""))
+        fluid = getattr(model, "fluid", None)
+        if fluid is None:
+            missing.append("model has no .fluid")
+        else:
+            for attribute in ("disgas", "vapoil", "b"):
+                if not hasattr(fluid, attribute):
+                    missing.append(f"model.fluid has no .{attribute}")
+        return missing
+
+    @staticmethod
+    def weights(model, state) -> np.ndarray:
+        """1/b_i at the mean pressure (CPRSolver._weighting,
+        linear_solvers.py:155-190), one per phase equation block."""
+        nph = int(model.n_phases)
+        fl = model.fluid
+        p_mean = float(np.mean(np.asarray(_value(_get(state, "pressure")), dtype=float)))
+        rs = np.asarray(_value(_get(state, "rs")), float).mean() if fl.disgas else None
+        sat = np.ones(1, dtype=bool) if fl.disgas else None
+        rv = np.asarray(_value(_get(state, "rv")), float).mean() if fl.vapoil else None
+        oil_present = np.ones(1, dtype=bool) if fl.vapoil else None
+        b = fl.b(np.array([p_mean]), rs, sat, rv, oil_present)
+        return np.array([1.0 / float(np.asarray(_value(bi)).ravel()[0]) for bi in b[:nph]])
+
+    def get_description(self) -> str:
+        return (f"GPU CPR-FGMRES(rtol={self.rtol:g}, restart={self.restart}, "
+                f"pressure stage {'aggregation AMG' if self.use_pressure_stage else 'off'}, "
+                f"block-Jacobi local stage, {self.precision})")
+
+    # -- device handles ---------------------------------------------------------
+    def _handle(self, n, nc, nph, a: sp.csr_array, sweeps: int, stream):
+        rp = np.ascontiguousarray(a.indptr, dtype=np.int32)
+        ci = np.ascontiguousarray(a.indices, dtype=np.int32)
+        pat = self._pattern
+        same = (pat is not None and pat[:3] == (n, nc, nph) and pat[3].size == rp.size and
+                pat[4].size == ci.size and np.array_equal(pat[3], rp) and np.array_equal(pat[4], ci))
+        if not same:
+            self.close()
+            self._pattern = (n, nc, nph, rp, ci)
+        h = self._handles.get(sweeps)
+        if h is None:
+            o = N.CPROpts()
+            N.check(N.lib().pmb_cpr_default_opts(N.C.byref(o)))
+            o.rtol = self.rtol
+            o.maxiter = self.maxiter
+            o.restart = self.restart
+            o.precision = 1 if self.precision == "mixed" else 0
+            o.use_pressure_stage = int(self.use_pressure_stage)
+            o.local_sweeps = sweeps
+            o.amg_rebuild_interval = self.amg_rebuild_interval
+            h = N.c_vp()
+            rp, ci = self._pattern[3], self._pattern[4]
+            N.check(N.lib().pmb_csr_cpr_create(n, nc, nph, N.as_p(rp, N.C.c_int32), N.as_p(ci, N.C.c_int32),
+                                               N.C.byref(o), stream, N.C.byref(h)))
+            self._handles[sweeps] = h
+        return h
+
+    def close(self) -> None:
+        """Release the device handles (they are also released with the solver)."""
+        handles, self._handles = self._handles, {}
+        self._pattern = None
+        for h in handles.values():
+            N.lib().pmb_csr_cpr_destroy(h)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the solve ------------------------------------------------------------------
+    def solve(self, jac, rhs, model=None, state=None, dt: Optional[float] = None) -> np.ndarray:
+        import torch
+        missing = self._unmet_requirements(model)
+        if missing:
+            self.last_fallback = tuple(missing)
+            raise ValueError("GpuCPRSolver needs the CPR model contract and has no host fallback: "
+                             + "; ".join(missing))
+        self.last_fallback = ()
+        if not torch.cuda.is_available():
+            raise RuntimeError("GpuCPRSolver needs a CUDA device")
+        a = sp.csr_array(jac, dtype=np.float64)
+        if not a.has_canonical_format:
+            a = a.copy()
+            a.sum_duplicates()
+        n = a.shape[0]
+        nc = int(model.G.cells.num)
+        nph = int(model.n_phases)
+        rhs = np.ascontiguousarray(np.asarray(rhs, dtype=np.float64).ravel())
+        if rhs.size != n or a.shape[1] != n:
+            raise ValueError(f"matrix {a.shape} and right-hand side ({rhs.size}) do not match")
+        w = self.weights(model, state) if self.use_pressure_stage else np.ones(nph)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        stream = torch.cuda.current_stream().cuda_stream
+        vals = torch.from_numpy(np.ascontiguousarray(a.data)).to("cuda")
+        bd = torch.from_numpy(rhs).to("cuda")
+        xd = torch.empty_like(bd)
+        info = (N.C.c_double * 4)()
+
+        def attempt(sweeps):
+            h = self._handle(n, nc, nph, a, sweeps, stream)
+            N.check(N.lib().pmb_csr_cpr_setup(h, N.ptr(vals), N.as_p(w, N.C.c_double)))
+            rc = N.lib().pmb_csr_cpr_solve(h, N.ptr(bd), N.ptr(xd), info)
+            if rc not in (N.PMB_OK, 5):
+                N.check(rc)
+            return rc == N.PMB_OK
+
+        stage = "block_jacobi"
+        ok = attempt(self.local_sweeps)
+        iterations = int(info[0])
+        if not ok and self.fallback_to_ilu and self.local_sweeps < 3:
+            stage = "block_jacobi x3"
+            ok = attempt(3)
+            iterations = int(info[0])
+        self.last_local_stage = stage
+        self.last_iterations = iterations
+        self.last_relres = float(info[1])
+        if not ok:
+            raise RuntimeError(
+                f"CPR did not converge (gmres info={iterations} after {iterations} "
+                f"iterations, local stage {stage!r}). Loosen rtol, or use the direct solver.")
+        return xd.cpu().numpy()
+
+    def solve_linear_system(self, A, b, model=None, state=None):
+        """AD-OO spelling (`LinearSolverAD.solve_linear_system`); needs the
+        model contract as `solve` does."""
+        return self.solve(A, b, model, state)
+
+
+CPRSolver = GpuCPRSolver

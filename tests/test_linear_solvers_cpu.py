@@ -1,0 +1,93 @@
+"""Host logic of the drop-in CPR solver (no GPU needed): the reference's
+constructor validation and model contract (linear_solvers.py:113-140,
+396-424), the decoupling weights (:155-190), and the C-ABI's pattern checks,
+which reject a bad matrix before any device work."""
+
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+from pymrst_b200 import _native as N
+from pymrst_b200.build import build
+from pymrst_b200.grid import cartesian_grid
+from pymrst_b200.linear_solvers import GpuCPRSolver
+from pymrst_b200.params import BARSA, CENTI, POISE, init_simple_adi_fluid
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build()
+    return N.lib()
+
+
+def _fluid():
+    return init_simple_adi_fluid(mu=np.array([1.0, 5.0]) * CENTI * POISE, rho=[1000.0, 800.0], n=[2, 2],
+                                 c=[1e-5 / BARSA, 1e-4 / BARSA], p_ref=200 * BARSA)
+
+
+@pytest.mark.parametrize("kwargs,match", [
+    (dict(local_stage="lu"), "unknown local_stage"),
+    (dict(local_stage="ilu"), "no ILU"),
+    (dict(amg_rebuild_interval=0), "amg_rebuild_interval"),
+    (dict(amg_cycles=2), "amg_cycles"),
+    (dict(elliptic_solver=object()), "elliptic_solver"),
+    (dict(precision="fp16"), "precision"),
+    (dict(restart=61), "restart"),
+])
+def test_constructor_rejects_what_the_device_path_cannot_do(kwargs, match):
+    with pytest.raises(ValueError, match=match):
+        GpuCPRSolver(**kwargs)
+
+
+def test_reference_defaults():
+    s = GpuCPRSolver()
+    assert (s.rtol, s.maxiter, s.restart, s.amg_rebuild_interval) == (1e-8, 200, 50, 8)
+    assert s.last_iterations == 0 and s.last_local_stage is None
+
+
+def test_missing_model_contract_is_loud():
+    g = cartesian_grid([3, 2, 1], [3.0, 2.0, 1.0])
+    J = np.eye(12)
+    with pytest.raises(ValueError, match="no model was supplied"):
+        GpuCPRSolver().solve(J, np.ones(12))
+    with pytest.raises(ValueError, match=r"has no \.G.*it has \.g"):
+        GpuCPRSolver().solve(J, np.ones(12), SimpleNamespace(g=g, fluid=_fluid(), n_phases=2))
+    with pytest.raises(ValueError, match=r"fluid has no \.b"):
+        GpuCPRSolver().solve(J, np.ones(12), SimpleNamespace(G=g, fluid=SimpleNamespace(disgas=False, vapoil=False),
+                                                             n_phases=2))
+
+
+def test_weights_are_inverse_shrinkage_at_mean_pressure():
+    fl = _fluid()
+    model = SimpleNamespace(G=None, fluid=fl, n_phases=2)
+    p = np.array([150.0, 210.0, 240.0]) * BARSA
+    w = GpuCPRSolver.weights(model, {"pressure": p})
+    pm = p.mean()
+    expect = [1.0 / float(fl.b_w(np.array([pm]))[0]), 1.0 / float(fl.b_o(np.array([pm]))[0])]
+    np.testing.assert_allclose(w, expect, rtol=1e-15)
+    # attribute-style states work too
+    w2 = GpuCPRSolver.weights(model, SimpleNamespace(pressure=p))
+    np.testing.assert_array_equal(w, w2)
+
+
+def _create(lib, n, nc, nph, rp, ci):
+    o = N.CPROpts()
+    N.check(lib.pmb_cpr_default_opts(N.C.byref(o)))
+    h = N.c_vp()
+    rp = np.asarray(rp, dtype=np.int32)
+    ci = np.asarray(ci, dtype=np.int32)
+    rc = lib.pmb_csr_cpr_create(n, nc, nph, N.as_p(rp, N.C.c_int32), N.as_p(ci, N.C.c_int32), N.C.byref(o), None,
+                                N.C.byref(h))
+    return rc, lib.pmb_last_error().decode()
+
+
+def test_csr_create_rejects_bad_patterns(lib):
+    rc, msg = _create(lib, 2, 1, 2, [0, 2, 3], [1, 0, 1])
+    assert rc == 2 and "strictly increasing" in msg
+    rc, msg = _create(lib, 2, 1, 2, [0, 1, 2], [0, 5])
+    assert rc == 2 and "out of range" in msg
+    rc, msg = _create(lib, 3, 2, 2, [0, 1, 2, 3], [0, 1, 2])
+    assert rc == 2 and "nph * nc" in msg
+    rc, msg = _create(lib, 4, 1, 4, [0, 1, 2, 3, 4], [0, 1, 2, 3])
+    assert rc == 2 and "nph must be" in msg
