@@ -182,6 +182,13 @@ int pmb_cpr_setup(pmb_cpr* s, const double* d_jac, const double* d_well, const d
 int pmb_cpr_solve(pmb_cpr* s, const double* d_b, double* d_x, double* h_info4);
 /* Unknowns per level of the current pressure hierarchy. */
 int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
+/* Measurement aid, no counterpart in the reference: mean milliseconds of one
+ * application of a preconditioner stage on the solver's stream (CUDA events,
+ * after one untimed application).  stage 0: the second stage (all local
+ * sweeps, updating d_z in place); 1: one AMG cycle on the restricted d_r;
+ * 2: the whole preconditioner z = M^{-1} r.  Needs pmb_cpr_setup first. */
+int pmb_cpr_time_stage(pmb_cpr* s, int32_t stage, const double* d_r, double* d_z, int32_t reps,
+                       double* h_ms);
 
 /* ------------------------------------------------------------------------
  * CPR on a caller's CSR matrix: the device side of the drop-in for

@@ -320,6 +320,18 @@ int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* sizes, int32_t
   });
 }
 
+int pmb_cpr_time_stage(pmb_cpr* s, int32_t stage, const double* d_r, double* d_z, int32_t reps,
+                       double* h_ms) {
+  return guarded([&] {
+    PMB_REQUIRE(s && d_r && d_z && h_ms, "NULL argument");
+    PMB_REQUIRE(stage >= 0 && stage <= 2, "stage must be 0, 1 or 2");
+    PMB_REQUIRE(reps >= 1, "reps must be positive");
+    require_aligned(d_r, 16, "r");
+    require_aligned(d_z, 16, "z");
+    *h_ms = s->s->time_stage(stage, d_r, d_z, reps);
+  });
+}
+
 int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_iterations, double* stats) {
   return guarded([&] {
     PMB_REQUIRE(h && s && stats, "NULL argument");

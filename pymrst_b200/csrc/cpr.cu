@@ -226,6 +226,42 @@ __device__ __forceinline__ double2 mv2(double4 a, double2 v) {
 __device__ __forceinline__ double4 ld4(const double4& a) { return a; }
 __device__ __forceinline__ double4 ld4(const float4& a) { return make_double4(a.x, a.y, a.z, a.w); }
 
+// rc -= sum over the cell's block row [kb, ke) of A[k] z[col[k]], in row
+// order.  The column indices, z values and blocks of the first kRowPrefetch
+// entries are all loaded before any is used, so that a row costs two
+// dependent memory round trips (column, then z) rather than one per block.
+constexpr int kRowPrefetch = 8;
+template <class BT>
+__device__ __forceinline__ void sub_row(const int* __restrict__ col, const BT* __restrict__ A,
+                                        const double2* __restrict__ z2, int kb, int ke, double2& rc) {
+  int cj[kRowPrefetch];
+#pragma unroll
+  for (int q = 0; q < kRowPrefetch; ++q) cj[q] = kb + q < ke ? col[kb + q] : 0;
+  double2 zq[kRowPrefetch];
+  double4 aq[kRowPrefetch];
+#pragma unroll
+  for (int q = 0; q < kRowPrefetch; ++q) {
+    zq[q] = make_double2(0.0, 0.0);
+    aq[q] = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (kb + q < ke) {
+      zq[q] = z2[cj[q]];
+      aq[q] = ld4(A[kb + q]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kRowPrefetch; ++q)
+    if (kb + q < ke) {
+      const double2 t = mv2(aq[q], zq[q]);
+      rc.x -= t.x;
+      rc.y -= t.y;
+    }
+  for (int k = kb + kRowPrefetch; k < ke; ++k) {
+    const double2 t = mv2(ld4(A[k]), z2[col[k]]);
+    rc.x -= t.x;
+    rc.y -= t.y;
+  }
+}
+
 // Line Gauss-Seidel for one colour of vertical lines, one warp per line:
 // the lanes form the block residual r - J z of the line's cells, then lane 0
 // solves the line's block-tridiagonal system (its couplings to the previous
@@ -268,11 +304,7 @@ __global__ void __launch_bounds__(32 * kLineWarps) line_gs_kernel(OWView v, int 
       const int t = t0 + u;
       const int c = lcells[t];
       double2 rc = reinterpret_cast<const double2*>(r)[c];
-      for (int k = v.row_ptr[c]; k < v.row_ptr[c + 1]; ++k) {
-        const double2 q = mv2(ld4(A[k]), z2[v.col[k]]);
-        rc.x -= q.x;
-        rc.y -= q.y;
-      }
+      sub_row(v.col, A, z2, v.row_ptr[c], v.row_ptr[c + 1], rc);
       const int q = v.cell_pc[c];
       if (q >= 0) {
         const double* zw = z + 2LL * v.nc;
@@ -344,11 +376,7 @@ __global__ void __launch_bounds__(32 * kLineWarps) line_gs_kernel(OWView v, int 
   for (int t = t0 + lane; t < t1; t += 32) {
     const int c = lcells[t];
     double2 rc = reinterpret_cast<const double2*>(r)[c];
-    for (int k = v.row_ptr[c]; k < v.row_ptr[c + 1]; ++k) {
-      const double2 q = mv2(ld4(A[k]), z2[v.col[k]]);
-      rc.x -= q.x;
-      rc.y -= q.y;
-    }
+    sub_row(v.col, A, z2, v.row_ptr[c], v.row_ptr[c + 1], rc);
     const int q = v.cell_pc[c];
     if (q >= 0) {
       const double* zw = z + 2LL * v.nc;
@@ -702,6 +730,46 @@ void CPRSolver::precond_body(const double* r, double* z) {
   }
   PhaseTimer pt("cpr.local_stage", s_);
   local_stage(r, z);
+}
+
+double CPRSolver::time_stage(int stage, const double* r, double* z, int reps) {
+  PMB_REQUIRE(jac_ != nullptr, "pmb_cpr_setup must run before timing a stage");
+  PMB_REQUIRE(stage != 1 || o_.use_pressure_stage, "the pressure stage is switched off");
+  const OWView v = m_.view();
+  auto amg_once = [&]() {
+    if (f32_)
+      amg32_.apply(bp32_.get(), xp32_.get(), s_);
+    else
+      amg_.apply(bp_.get(), xp_.get(), s_);
+  };
+  if (stage == 1) {
+    if (f32_)
+      restrict_p_kernel<<<grid_for(v.nc, 256), 256, 0, s_>>>(v.nc, reinterpret_cast<const double2*>(r), w_.get(),
+                                                             bp32_.get());
+    else
+      restrict_p_kernel<<<grid_for(v.nc, 256), 256, 0, s_>>>(v.nc, reinterpret_cast<const double2*>(r), w_.get(),
+                                                             bp_.get());
+    PMB_CHECK_LAUNCH();
+  }
+  auto once = [&]() {
+    if (stage == 0) local_stage(r, z);
+    else if (stage == 1) amg_once();
+    else precond_body(r, z);
+  };
+  once();
+  cudaEvent_t e0, e1;
+  PMB_CUDA(cudaEventCreate(&e0));
+  PMB_CUDA(cudaEventCreate(&e1));
+  PMB_CUDA(cudaEventRecord(e0, s_));
+  for (int i = 0; i < reps; ++i) once();
+  PMB_CUDA(cudaEventRecord(e1, s_));
+  PMB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  PMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  check_status();
+  return ms / reps;
 }
 
 bool CPRSolver::solve(const double* b, double* x, double* info) {

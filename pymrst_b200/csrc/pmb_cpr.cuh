@@ -18,6 +18,11 @@ class CPRSolver {
   int level_size(int l) const { return amg_.level_size(l); }
   long long setups() const { return setups_; }
   long long total_iterations() const { return total_its_; }
+  // Mean milliseconds of one application of a preconditioner stage (0: the
+  // second stage, every sweep; 1: the AMG cycle on the restricted r; 2: the
+  // whole preconditioner, not replayed from a graph), by CUDA events on the
+  // solver's stream, after one untimed application.
+  double time_stage(int stage, const double* r, double* z, int reps);
 
  private:
   void precond(const double* r, double* z);
