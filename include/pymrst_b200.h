@@ -110,6 +110,12 @@ int pmb_ow_pattern(const pmb_ow* h, int32_t* h_row_ptr, int32_t* h_col);
 int pmb_ow_compute_cdp(pmb_ow* h, const double* d_x0, double* d_cdp);
 /* Forget the previous-step cdp (a fresh model). */
 int pmb_ow_reset_cdp(pmb_ow* h);
+/* New well targets, one per well: bhp for bhp wells, total surface rate for
+ * rate wells (_set_controls, pymrst/modules/optimization/adjoint.py:63-65,
+ * which sets w.val between timesteps).  Also rescales the well convergence
+ * test, whose rate reference is the largest rate target (_converged,
+ * two_phase_oil_water_model.py:549-567). */
+int pmb_ow_set_controls(pmb_ow* h, const double* h_well_val);
 
 /* Residual and Jacobian at d_x for the step from d_x0 over dt
  * (assemble, two_phase_oil_water_model.py:493-546).  d_jac: nnzb 2x2
@@ -158,10 +164,11 @@ typedef struct pmb_cpr_opts {
   double rtol;              /* relative residual target, ||b - A x|| <= rtol ||b|| */
   int32_t maxiter;          /* total Krylov iterations */
   int32_t restart;          /* GMRES restart length */
-  int32_t precision;        /* 0: FP64 throughout; 1: FP32 Krylov + preconditioner
-                               inside FP64 iterative refinement */
+  int32_t precision;        /* 0: FP64 throughout; 1: FP32 AMG and FP32 smoother blocks
+                               inside the FP64 FGMRES */
   int32_t use_pressure_stage;
-  int32_t local_sweeps;     /* red-black block Gauss-Seidel sweeps of the second stage */
+  int32_t local_sweeps;     /* second-stage sweeps: vertical-line block Gauss-Seidel where
+                               the model has vertical lines, else red-black block GS */
   int32_t amg_smoother_degree; /* Chebyshev degree on each level */
   int32_t amg_cycle;        /* 0: V-cycle; k > 0: K-cycle, the coarse corrections of the
                                first k levels accelerated by two Krylov steps */
@@ -171,6 +178,9 @@ typedef struct pmb_cpr_opts {
   double inner_rtol;        /* mixed precision: FP32 inner solve target */
 } pmb_cpr_opts;
 
+/* Defaults: rtol 1e-8, maxiter 200, restart 50 (CPRSolver's,
+ * linear_solvers.py:113-116); local_sweeps 3, Chebyshev degree 2, K-cycle on
+ * 3 levels, theta 0.1, coarse size 200, re-aggregation every 8 setups. */
 int pmb_cpr_default_opts(pmb_cpr_opts* out);
 int pmb_cpr_create(pmb_ow* model, const pmb_cpr_opts* opts, pmb_cpr** out);
 int pmb_cpr_destroy(pmb_cpr* s);
@@ -203,10 +213,14 @@ int pmb_cpr_time_stage(pmb_cpr* s, int32_t stage, const double* d_r, double* d_z
  * application).  h_weights (nph doubles): the decoupling weights
  * (_weighting, :155-190: 1/b_i at the mean pressure).  h_info4 =
  * [iterations, relres, ok, setups]; PMB_ERR_NOCONV when rtol was not
- * reached, PMB_ERR_PIVOT for a singular cell block. */
+ * reached, PMB_ERR_PIVOT for a singular cell block.  transposed != 0: the
+ * matrix given is J^T (the adjoint system of compute_gradient_adjoint,
+ * pymrst/modules/optimization/adjoint.py:209) and the CPR transfer
+ * operators are transposed with it (restriction to the pressure rows,
+ * prolongation by the weights). */
 typedef struct pmb_csr_cpr pmb_csr_cpr;
 int pmb_csr_cpr_create(int32_t n, int32_t nc, int32_t nph, const int32_t* h_row_ptr, const int32_t* h_col,
-                       const pmb_cpr_opts* opts, void* stream, pmb_csr_cpr** out);
+                       int32_t transposed, const pmb_cpr_opts* opts, void* stream, pmb_csr_cpr** out);
 int pmb_csr_cpr_destroy(pmb_csr_cpr* h);
 int pmb_csr_cpr_setup(pmb_csr_cpr* h, const double* d_values, const double* h_weights);
 int pmb_csr_cpr_solve(pmb_csr_cpr* h, const double* d_b, double* d_x, double* h_info4);

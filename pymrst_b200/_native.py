@@ -63,6 +63,7 @@ SIGNATURES = {
     "pmb_ow_pattern": (c_int, [c_vp, P_i32, P_i32]),
     "pmb_ow_compute_cdp": (c_int, [c_vp, c_vp, c_vp]),
     "pmb_ow_reset_cdp": (c_int, [c_vp]),
+    "pmb_ow_set_controls": (c_int, [c_vp, P_dbl]),
     "pmb_ow_assemble": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp, c_vp, c_int]),
     "pmb_ow_spmv": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_ow_convergence": (c_int, [c_vp, c_vp, c_vp, c_dbl, P_dbl]),
@@ -76,7 +77,7 @@ SIGNATURES = {
     "pmb_cpr_levels": (c_int, [c_vp, c_int, P_i64, P_i32]),
     "pmb_cpr_time_stage": (c_int, [c_vp, c_int, c_vp, c_vp, c_int, P_dbl]),
     "pmb_ow_step": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_int, P_dbl]),
-    "pmb_csr_cpr_create": (c_int, [c_int, c_int, c_int, P_i32, P_i32, C.POINTER(CPROpts), c_vp,
+    "pmb_csr_cpr_create": (c_int, [c_int, c_int, c_int, P_i32, P_i32, c_int, C.POINTER(CPROpts), c_vp,
                                    C.POINTER(c_vp)]),
     "pmb_csr_cpr_destroy": (c_int, [c_vp]),
     "pmb_csr_cpr_setup": (c_int, [c_vp, c_vp, P_dbl]),

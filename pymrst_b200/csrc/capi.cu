@@ -203,6 +203,13 @@ int pmb_ow_reset_cdp(pmb_ow* h) {
   });
 }
 
+int pmb_ow_set_controls(pmb_ow* h, const double* h_well_val) {
+  return guarded([&] {
+    PMB_REQUIRE(h && (h_well_val || h->m->view().nw == 0), "NULL argument");
+    h->m->set_well_values(h_well_val);
+  });
+}
+
 int pmb_ow_assemble(pmb_ow* h, const double* d_x, const double* d_x0, double dt, const double* d_cdp,
                     double* d_res, double* d_jac, double* d_well, int32_t want_jac) {
   return guarded([&] {
@@ -262,10 +269,10 @@ int pmb_cpr_default_opts(pmb_cpr_opts* o) {
     o->restart = 50;
     o->precision = 0;
     o->use_pressure_stage = 1;
-    o->local_sweeps = 2;
+    o->local_sweeps = 3;
     o->amg_smoother_degree = 2;
-    o->amg_cycle = 0;
-    o->amg_theta = 0.25;
+    o->amg_cycle = 3;
+    o->amg_theta = 0.1;
     o->amg_coarse_size = 200;
     o->amg_rebuild_interval = 8;
     o->inner_rtol = 1e-4;

@@ -436,21 +436,156 @@ __global__ void __launch_bounds__(32 * kLineWarps) line_gs_kernel(OWView v, int 
   }
 }
 
-// Well unknowns: z_w += inv(D_k) (r_w - C z_cells - D_k z_w).
-__global__ void gs_well_kernel(OWView v, const double* __restrict__ wj, const double* __restrict__ r,
-                               double* __restrict__ z) {
-  for (int k = threadIdx.x; k < v.nw; k += blockDim.x) {
-    const double* D = wj + v.wl.D + 9LL * k;
-    double* zw = z + 2LL * v.nc + 3LL * k;
-    const double* rw = r + 2LL * v.nc + 3LL * k;
-    double e0 = rw[0], e1 = rw[1], e2 = rw[2];
-    for (int i = v.perf_ptr[k]; i < v.perf_ptr[k + 1]; ++i) {
+// Line Gauss-Seidel for one colour of vertical lines by parallel cyclic
+// reduction: one CTA per line, one thread per cell of the line.  Each thread
+// forms its cell's block residual r - J z (the whole block row and the well
+// columns) and loads its diagonal block and its couplings to the previous and
+// next cell of the line; the CTA then solves the line's block-tridiagonal
+// system
+//   L_u x_{u-1} + D_u x_u + U_u x_{u+1} = y_u
+// in ceil(log2(len)) steps, each eliminating the couplings at distance s from
+// every equation at once:
+//   a = -L_u inv(D_{u-s}),  g = -U_u inv(D_{u+s}),
+//   D_u += a U_{u-s} + g L_{u+s},  L_u = a L_{u-s},  U_u = g U_{u+s},
+//   y_u += a y_{u-s} + g y_{u+s},
+// after which x_u = inv(D_u) y_u is added to z.  Lines of one colour never
+// touch, so every CTA writes only its own cells.  Needs blockDim.x >= the
+// line's length; shared memory 144 B per thread.
+constexpr int kPcrMaxLen = 256;
+
+__device__ __forceinline__ double4 add4(double4 a, double4 b) {
+  return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ double4 neg4(double4 a) { return make_double4(-a.x, -a.y, -a.z, -a.w); }
+
+template <class BT>
+__global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lstart, const int* __restrict__ clines,
+                                                              const int* __restrict__ lptr,
+                                                              const int* __restrict__ lcells,
+                                                              const int* __restrict__ llo,
+                                                              const int* __restrict__ lup,
+                                                              const BT* __restrict__ A,
+                                                              const double* __restrict__ wj,
+                                                              const double* __restrict__ r, double* __restrict__ z,
+                                                              int* status) {
+  extern __shared__ double4 pcr_sm[];
+  const int nb = blockDim.x;
+  double4* sD = pcr_sm;
+  double4* sL = pcr_sm + nb;
+  double4* sU = pcr_sm + 2 * nb;
+  double4* sI = pcr_sm + 3 * nb;
+  double2* sY = reinterpret_cast<double2*>(pcr_sm + 4 * nb);
+  __shared__ int sBad;
+  const int line = clines[lstart + blockIdx.x];
+  const int t0 = lptr[line];
+  const int len = lptr[line + 1] - t0;
+  const int u = threadIdx.x;
+  const bool act = u < len;
+  if (u == 0) sBad = 0;
+  const double4 zero4 = make_double4(0, 0, 0, 0);
+  const double2* z2 = reinterpret_cast<const double2*>(z);
+  double4 D = make_double4(1, 0, 0, 1), Lb = zero4, Ub = zero4;
+  double2 y = make_double2(0, 0);
+  int c = 0;
+  if (act) {
+    const int t = t0 + u;
+    c = lcells[t];
+    double2 rc = reinterpret_cast<const double2*>(r)[c];
+    sub_row(v.col, A, z2, v.row_ptr[c], v.row_ptr[c + 1], rc);
+    const int q = v.cell_pc[c];
+    if (q >= 0) {
+      const double* zw = z + 2LL * v.nc;
+      for (int jj = v.pc_ptr[q]; jj < v.pc_ptr[q + 1]; ++jj) {
+        const int i = v.pc_perf[jj];
+        const int kw = v.perf_well[i];
+        const double* B = wj + v.wl.B + 6LL * i;
+        rc.x -= B[0] * zw[3 * kw] + B[1] * zw[3 * kw + 1] + B[2] * zw[3 * kw + 2];
+        rc.y -= B[3] * zw[3 * kw] + B[4] * zw[3 * kw + 1] + B[5] * zw[3 * kw + 2];
+      }
+    }
+    y = rc;
+    D = ld4(A[v.diag_pos[c]]);
+    if (u > 0 && llo[t] >= 0) Lb = ld4(A[llo[t]]);
+    if (u + 1 < len && lup[t] >= 0) Ub = ld4(A[lup[t]]);
+  }
+  for (int s = 1; s < len; s <<= 1) {
+    bool ok = true;
+    const double4 I = inv2(D, ok);
+    if (act && !ok) sBad = 1;
+    if (act) {
+      sD[u] = D;
+      sL[u] = Lb;
+      sU[u] = Ub;
+      sI[u] = I;
+      sY[u] = y;
+    }
+    __syncthreads();
+    if (sBad) break;  // uniform: read after the barrier by every thread
+    if (act) {
+      double4 nD = D, nL = zero4, nU = zero4;
+      double2 ny = y;
+      if (u - s >= 0) {
+        const double4 a = neg4(mul2(Lb, sI[u - s]));
+        nD = add4(nD, mul2(a, sU[u - s]));
+        nL = mul2(a, sL[u - s]);
+        const double2 q = mv2(a, sY[u - s]);
+        ny.x += q.x;
+        ny.y += q.y;
+      }
+      if (u + s < len) {
+        const double4 g = neg4(mul2(Ub, sI[u + s]));
+        nD = add4(nD, mul2(g, sL[u + s]));
+        nU = mul2(g, sU[u + s]);
+        const double2 q = mv2(g, sY[u + s]);
+        ny.x += q.x;
+        ny.y += q.y;
+      }
+      D = nD;
+      Lb = nL;
+      Ub = nU;
+      y = ny;
+    }
+    __syncthreads();
+  }
+  if (sBad) {
+    if (u == 0) atomicExch(status, PMB_ERR_PIVOT);
+    return;
+  }
+  if (!act) return;
+  bool ok = true;
+  const double4 I = inv2(D, ok);
+  if (!ok) {
+    atomicExch(status, PMB_ERR_PIVOT);
+    return;
+  }
+  const double2 x = mv2(I, y);
+  double2 zc = z2[c];
+  zc.x += x.x;
+  zc.y += x.y;
+  reinterpret_cast<double2*>(z)[c] = zc;
+}
+
+// Well unknowns: z_w += inv(D_k) (r_w - C z_cells - D_k z_w); one warp per
+// well, the lanes over its perforations.
+__global__ void __launch_bounds__(256) gs_well_kernel(OWView v, const double* __restrict__ wj,
+                                                      const double* __restrict__ r, double* __restrict__ z) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int k = warp; k < v.nw; k += nwarp) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int i = v.perf_ptr[k] + lane; i < v.perf_ptr[k + 1]; i += 32) {
       const int c = v.perf_cell[i];
       const double* C = wj + v.wl.C + 4LL * i;
       const double zp = z[2LL * c], zs = z[2LL * c + 1];
-      e0 -= C[0] * zp + C[1] * zs;
-      e1 -= C[2] * zp + C[3] * zs;
+      s0 += C[0] * zp + C[1] * zs;
+      s1 += C[2] * zp + C[3] * zs;
     }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    if (lane != 0) continue;
+    const double* D = wj + v.wl.D + 9LL * k;
+    double* zw = z + 2LL * v.nc + 3LL * k;
+    const double* rw = r + 2LL * v.nc + 3LL * k;
+    double e0 = rw[0] - s0, e1 = rw[1] - s1, e2 = rw[2];
     e0 -= D[0] * zw[0] + D[1] * zw[1] + D[2] * zw[2];
     e1 -= D[3] * zw[0] + D[4] * zw[1] + D[5] * zw[2];
     e2 -= D[6] * zw[0] + D[7] * zw[1] + D[8] * zw[2];
@@ -652,6 +787,21 @@ void CPRSolver::local_stage(const double* r, double* z) {
       for (int q = 0; q + 1 < (int)Ls.h_color_ptr.size(); ++q) {
         const int cnt = Ls.h_color_ptr[q + 1] - Ls.h_color_ptr[q];
         if (cnt <= 0) continue;
+        if (Ls.max_len <= kPcrMaxLen) {
+          const int nb = std::max(32, (Ls.max_len + 31) / 32 * 32);
+          const size_t smem = (size_t)nb * (4 * sizeof(double4) + sizeof(double2));
+          if (f32_)
+            line_pcr_kernel<<<cnt, nb, smem, s_>>>(v, Ls.h_color_ptr[q], Ls.color_lines.get(), Ls.line_ptr.get(),
+                                                   Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(),
+                                                   reinterpret_cast<const float4*>(jac32_.get()), well_, r, z,
+                                                   status_.get());
+          else
+            line_pcr_kernel<<<cnt, nb, smem, s_>>>(v, Ls.h_color_ptr[q], Ls.color_lines.get(), Ls.line_ptr.get(),
+                                                   Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(), A, well_,
+                                                   r, z, status_.get());
+          PMB_CHECK_LAUNCH();
+          continue;
+        }
         if (f32_)
           line_gs_kernel<<<grid_for(32LL * cnt, 32 * kLineWarps), 32 * kLineWarps, 0, s_>>>(
               v, Ls.h_color_ptr[q], Ls.h_color_ptr[q + 1], Ls.color_lines.get(), Ls.line_ptr.get(),
@@ -666,7 +816,7 @@ void CPRSolver::local_stage(const double* r, double* z) {
         PMB_CHECK_LAUNCH();
       }
       if (v.nw) {
-        gs_well_kernel<<<1, 128, 0, s_>>>(v, well_, r, z);
+        gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z);
         PMB_CHECK_LAUNCH();
       }
     }
@@ -681,7 +831,7 @@ void CPRSolver::local_stage(const double* r, double* z) {
       PMB_CHECK_LAUNCH();
     }
     if (v.nw) {
-      gs_well_kernel<<<1, 128, 0, s_>>>(v, well_, r, z);
+      gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z);
       PMB_CHECK_LAUNCH();
     }
   }

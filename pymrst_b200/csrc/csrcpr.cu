@@ -13,6 +13,11 @@
 // block-Jacobi stage (:316-363): each cell's nph x nph block inverted, the
 // facility block inverted as a whole (regularised by sqrt(eps) where it is
 // exactly singular, as the reference does after equilibration, :345-357).
+// In transposed mode the caller passes A' = J^T (the adjoint system,
+// optimization/adjoint.py:209) and the transfer operators are the
+// transposes of the forward ones: restriction P^T (the pressure rows of r),
+// prolongation W^T (x[i*nc + c] = w_i xp[c]), so that the pressure matrix is
+// P^T J^T W^T = (W J P)^T.
 // The Ruiz equilibration the reference applies before its factorisations
 // (:206-224) is not applied: block inverses are invariant under it, and the
 // AMG's strength measure and Jacobi-scaled smoother are invariant under the
@@ -185,26 +190,38 @@ __global__ void __launch_bounds__(256) csr_tail_invert_kernel(int nt, double* __
   for (long long idx = t; idx < (long long)nt * nt; idx += nthr) Inv[idx] *= rs[idx % nt];
 }
 
-// bp[c] = sum_i w[i] r[i*nc + c]
+// bp[c] = sum_i rw[i] r[i*nc + c]  (rw = w, or (1, 0, ..) when transposed)
 template <class T>
-__global__ void csr_restrict_kernel(int nc, int nph, const double* __restrict__ r, const double* __restrict__ w,
+__global__ void csr_restrict_kernel(int nc, int nph, const double* __restrict__ r, const double* __restrict__ rw,
                                     T* __restrict__ bp) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
   double s = 0.0;
-  for (int i = 0; i < nph; ++i) s += w[i] * r[(long long)i * nc + c];
+  for (int i = 0; i < nph; ++i) s += rw[i] * r[(long long)i * nc + c];
   bp[c] = (T)s;
 }
 
-// Cell rows of the second stage in one pass: with x = P xp (zero when xp is
+// x = Q xp evaluated at column j: the injection into the pressure block
+// (Q = P), or the weighted spread into every cell block (Q = W^T).
+template <bool TR, class T>
+__device__ __forceinline__ double prolonged(int j, int nc, int nph, const T* __restrict__ xp,
+                                            const double* __restrict__ pw) {
+  if (!TR) return j < nc ? (double)xp[j] : 0.0;
+  if (j >= nph * nc) return 0.0;
+  const int blk = j / nc;
+  return pw[blk] * (double)xp[j - blk * nc];
+}
+
+// Cell rows of the second stage in one pass: with x = Q xp (zero when xp is
 // null), t_i = r_i - (A x)_i for the cell's nph rows, then
-// z_i = x_i + inv_c t.  Only columns < nc of A meet a nonzero of x.
-template <class T>
+// z_i = x_i + inv_c t.
+template <bool TR, class T>
 __global__ void __launch_bounds__(256) csr_local_cells_kernel(int nc, int nph, const int* __restrict__ rp,
                                                               const int* __restrict__ ci,
                                                               const double* __restrict__ a,
                                                               const double* __restrict__ r,
                                                               const T* __restrict__ xp,
+                                                              const double* __restrict__ pw,
                                                               const double* __restrict__ inv,
                                                               double* __restrict__ z) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -214,15 +231,12 @@ __global__ void __launch_bounds__(256) csr_local_cells_kernel(int nc, int nph, c
     const long long row = (long long)i * nc + c;
     double s = r[row];
     if (xp)
-      for (int k = rp[row]; k < rp[row + 1]; ++k) {
-        const int j = ci[k];
-        if (j < nc) s -= a[k] * (double)xp[j];
-      }
+      for (int k = rp[row]; k < rp[row + 1]; ++k) s -= a[k] * prolonged<TR>(ci[k], nc, nph, xp, pw);
     t[i] = s;
   }
   const double* B = inv + (long long)c * nph * nph;
   for (int i = 0; i < nph; ++i) {
-    double s = (i == 0 && xp) ? (double)xp[c] : 0.0;
+    double s = xp ? prolonged<TR>(i * nc + c, nc, nph, xp, pw) : 0.0;
     for (int j = 0; j < nph; ++j) s += B[i * nph + j] * t[j];
     z[(long long)i * nc + c] = s;
   }
@@ -230,23 +244,22 @@ __global__ void __launch_bounds__(256) csr_local_cells_kernel(int nc, int nph, c
 
 // Facility rows of the second stage (one CTA): t = r - A x over the nt rows,
 // z = Inv t (x is zero there).
-template <class T>
-__global__ void __launch_bounds__(256) csr_local_tail_kernel(int nc, int base, int nt, const int* __restrict__ rp,
+template <bool TR, class T>
+__global__ void __launch_bounds__(256) csr_local_tail_kernel(int nc, int nph, int nt, const int* __restrict__ rp,
                                                              const int* __restrict__ ci,
                                                              const double* __restrict__ a,
                                                              const double* __restrict__ r,
                                                              const T* __restrict__ xp,
+                                                             const double* __restrict__ pw,
                                                              const double* __restrict__ Inv,
                                                              double* __restrict__ z) {
   extern __shared__ double ts[];
+  const int base = nph * nc;
   for (int q = threadIdx.x; q < nt; q += blockDim.x) {
     const int row = base + q;
     double s = r[row];
     if (xp)
-      for (int k = rp[row]; k < rp[row + 1]; ++k) {
-        const int j = ci[k];
-        if (j < nc) s -= a[k] * (double)xp[j];
-      }
+      for (int k = rp[row]; k < rp[row + 1]; ++k) s -= a[k] * prolonged<TR>(ci[k], nc, nph, xp, pw);
     ts[q] = s;
   }
   __syncthreads();
@@ -299,7 +312,8 @@ __global__ void __launch_bounds__(256) csr_jacobi_tail_kernel(int base, int nt, 
 
 class CsrCPR {
  public:
-  CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, const pmb_cpr_opts& o, cudaStream_t s);
+  CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, bool transposed, const pmb_cpr_opts& o,
+         cudaStream_t s);
   void setup(const double* d_val, const double* h_w);
   bool solve(const double* b, double* x, double* info);
   void spmv(const double* val, const double* x, double* y);
@@ -311,6 +325,7 @@ class CsrCPR {
   void check_status();
 
   int n_, nc_, nph_, nt_ = 0, nnz_ = 0;
+  bool tr_ = false;
   pmb_cpr_opts o_;
   cudaStream_t s_;
   bool f32_ = false;
@@ -321,7 +336,7 @@ class CsrCPR {
   std::vector<int> h_prp_, h_pcol_;
   DArray<int> prp_, pcol_, gptr_, gsrc_;
   DArray<unsigned char> gph_;
-  DArray<double> ap_, w_;
+  DArray<double> ap_, w_, rw_, pw_;  // weights; restriction and prolongation weights
   DArray<double> bp_, xp_;
   DArray<float> bp32_, xp32_;
   AMG<double> amg_;
@@ -340,8 +355,9 @@ class CsrCPR {
   long long setups_ = 0;
 };
 
-CsrCPR::CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, const pmb_cpr_opts& o, cudaStream_t s)
-    : n_(n), nc_(nc), nph_(nph), o_(o), s_(s) {
+CsrCPR::CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, bool transposed, const pmb_cpr_opts& o,
+               cudaStream_t s)
+    : n_(n), nc_(nc), nph_(nph), tr_(transposed), o_(o), s_(s) {
   PMB_REQUIRE(h_rp && h_col, "row_ptr and col are required");
   PMB_REQUIRE(nph >= 1 && nph <= kMaxPhases, "nph must be 1, 2 or 3");
   PMB_REQUIRE(nc >= 1 && (long long)nph * nc <= n, "need 1 <= nc and nph * nc <= n");
@@ -375,9 +391,16 @@ CsrCPR::CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, const 
   std::vector<std::pair<int, std::pair<int, int>>> ent;  // (column, (position, phase))
   for (int c = 0; c < nc; ++c) {
     ent.clear();
-    for (int i = 0; i < nph; ++i) {
-      const int row = i * nc + c;
-      for (int k = h_rp[row]; k < h_rp[row + 1] && h_col[k] < nc; ++k) ent.push_back({h_col[k], {k, i}});
+    if (!tr_) {
+      // W A P: the pressure columns of the cell's nph rows, weighted by row phase
+      for (int i = 0; i < nph; ++i) {
+        const int row = i * nc + c;
+        for (int k = h_rp[row]; k < h_rp[row + 1] && h_col[k] < nc; ++k) ent.push_back({h_col[k], {k, i}});
+      }
+    } else {
+      // P^T A' W^T: the cell's pressure row, every cell column, weighted by column phase
+      for (int k = h_rp[c]; k < h_rp[c + 1] && h_col[k] < nph * nc; ++k)
+        ent.push_back({h_col[k] % nc, {k, h_col[k] / nc}});
     }
     ent.push_back({c, {-1, 0}});  // the diagonal is always in the pattern
     std::sort(ent.begin(), ent.end());
@@ -427,7 +450,9 @@ CsrCPR::CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, const 
     trs_.resize(nt_);
   }
   w_.resize(nph);
-  w_pin_.resize(nph);
+  rw_.resize(nph);
+  pw_.resize(nph);
+  w_pin_.resize(3 * nph);
   bp_.resize(nc);
   xp_.resize(nc);
   if (f32_) {
@@ -482,8 +507,13 @@ void CsrCPR::setup(const double* d_val, const double* h_w) {
     for (int i = 0; i < nph_; ++i) {
       PMB_REQUIRE(std::isfinite(h_w[i]), "non-finite phase weight");
       w_pin_[i] = h_w[i];
+      w_pin_[nph_ + i] = tr_ ? (i == 0 ? 1.0 : 0.0) : h_w[i];   // restriction
+      w_pin_[2 * nph_ + i] = tr_ ? h_w[i] : (i == 0 ? 1.0 : 0.0);  // prolongation
     }
     PMB_CUDA(cudaMemcpyAsync(w_.get(), w_pin_.get(), sizeof(double) * nph_, cudaMemcpyHostToDevice, s_));
+    PMB_CUDA(cudaMemcpyAsync(rw_.get(), w_pin_.get() + nph_, sizeof(double) * nph_, cudaMemcpyHostToDevice, s_));
+    PMB_CUDA(cudaMemcpyAsync(pw_.get(), w_pin_.get() + 2 * nph_, sizeof(double) * nph_, cudaMemcpyHostToDevice,
+                             s_));
     const int pn = (int)h_pcol_.size();
     const int g = grid_for(pn, 256);
     const bool built = f32_ ? amg32_.built() : amg_.built();
@@ -521,18 +551,26 @@ void CsrCPR::setup(const double* d_val, const double* h_w) {
 
 void CsrCPR::precond_body(const double* r, double* z) {
   auto second_stage = [&](auto* xp) {
-    csr_local_cells_kernel<<<grid_for(nc_, 256), 256, 0, s_>>>(nc_, nph_, rp_.get(), col_.get(), val_, r, xp,
-                                                                inv_.get(), z);
-    PMB_CHECK_LAUNCH();
-    if (nt_ > 0) {
-      csr_local_tail_kernel<<<1, 256, sizeof(double) * nt_, s_>>>(nc_, nph_ * nc_, nt_, rp_.get(), col_.get(), val_,
-                                                                   r, xp, tInv_.get(), z);
+    using T = std::remove_const_t<std::remove_pointer_t<decltype(xp)>>;
+    auto launch = [&](auto trc) {
+      constexpr bool TR = decltype(trc)::value;
+      csr_local_cells_kernel<TR, T><<<grid_for(nc_, 256), 256, 0, s_>>>(nc_, nph_, rp_.get(), col_.get(), val_, r,
+                                                                        xp, pw_.get(), inv_.get(), z);
       PMB_CHECK_LAUNCH();
-    }
+      if (nt_ > 0) {
+        csr_local_tail_kernel<TR, T><<<1, 256, sizeof(double) * nt_, s_>>>(nc_, nph_, nt_, rp_.get(), col_.get(),
+                                                                           val_, r, xp, pw_.get(), tInv_.get(), z);
+        PMB_CHECK_LAUNCH();
+      }
+    };
+    if (tr_)
+      launch(std::true_type{});
+    else
+      launch(std::false_type{});
   };
   if (o_.use_pressure_stage) {
     auto pressure_stage = [&](auto* bp, auto* xp, auto& amg) {
-      csr_restrict_kernel<<<grid_for(nc_, 256), 256, 0, s_>>>(nc_, nph_, r, w_.get(), bp);
+      csr_restrict_kernel<<<grid_for(nc_, 256), 256, 0, s_>>>(nc_, nph_, r, rw_.get(), bp);
       PMB_CHECK_LAUNCH();
       {
         PhaseTimer pt("cpr.amg_cycle", s_);
@@ -588,12 +626,13 @@ struct pmb_csr_cpr {
 extern "C" {
 
 int pmb_csr_cpr_create(int32_t n, int32_t nc, int32_t nph, const int32_t* h_row_ptr, const int32_t* h_col,
-                       const pmb_cpr_opts* opts, void* stream, pmb_csr_cpr** out) {
+                       int32_t transposed, const pmb_cpr_opts* opts, void* stream, pmb_csr_cpr** out) {
   return pmb::guarded([&] {
     PMB_REQUIRE(out != nullptr && opts != nullptr, "NULL argument");
     *out = nullptr;
     auto h = std::make_unique<pmb_csr_cpr>();
-    h->impl = std::make_unique<pmb::CsrCPR>(n, nc, nph, h_row_ptr, h_col, *opts, (cudaStream_t)stream);
+    h->impl = std::make_unique<pmb::CsrCPR>(n, nc, nph, h_row_ptr, h_col, transposed != 0, *opts,
+                                            (cudaStream_t)stream);
     *out = h.release();
   });
 }

@@ -801,6 +801,7 @@ OWModel::OWModel(const pmb_ow_desc& d, cudaStream_t s) : stream_(s) {
   v_.cell_pc = cell_pc_.get();
   v_.wl = WellLayout::make(nperf, nw);
   v_.gravity = d.gravity;
+  h_well_type_.assign(d.h_well_type, d.h_well_type + nw);
   double qmax = 0.0;
   bool any_rate = false;
   for (int k = 0; k < nw; ++k)
@@ -817,6 +818,18 @@ OWModel::OWModel(const pmb_ow_desc& d, cudaStream_t s) : stream_(s) {
   x0_.resize(nvec());
   dx_.resize(nvec());
   PMB_CUDA(cudaStreamSynchronize(s));
+}
+
+void OWModel::set_well_values(const double* h_val) {
+  const int nw = v_.nw;
+  for (int k = 0; k < nw; ++k) PMB_REQUIRE(std::isfinite(h_val[k]), "non-finite well target");
+  if (nw) well_val_.upload(h_val, nw, stream_);
+  double qmax = 0.0;
+  bool any_rate = false;
+  for (int k = 0; k < nw; ++k)
+    if (h_well_type_[k] == 1) { any_rate = true; qmax = std::max(qmax, std::fabs(h_val[k])); }
+  v_.q_ref = any_rate ? std::max(qmax, 1e-12) : 1.0;
+  PMB_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void OWModel::compute_cdp(const double* x0, double* cdp) {

@@ -96,6 +96,9 @@ class OWModel {
 
   void compute_cdp(const double* x0, double* cdp);
   void reset_cdp() { have_last_cdp_ = false; }
+  // New well targets (bhp or total rate per well), and the rate scale of
+  // the well convergence test that depends on them.
+  void set_well_values(const double* h_val);
   void assemble(const double* x, const double* x0, double dt, const double* cdp, double* res,
                 double* jac, double* well, bool want_jac);
   void spmv(const double* jac, const double* well, const double* x, double* y);
@@ -122,6 +125,7 @@ class OWModel {
   DArray<int> row_ptr_, col_, nz_face_, diag_pos_, perf_ptr_, perf_cell_, well_type_, perf_well_;
   DArray<int> pcell_, pc_ptr_, pc_perf_, color_cells_, cell_pc_;
   DArray<double> T_, gdz_, pv_, perf_WI_, perf_dZ_, well_val_, compi_;
+  std::vector<int> h_well_type_;
   // scratch / state
   DArray<double> pf_cq_, pf_dloc_, last_cdp_, conv_part_, conv_out_;
   DArray<double> jac_, well_, res_, cdp_, x0_, dx_;

@@ -82,8 +82,8 @@ class GpuCPRSolver:
         self.last_local_stage: Optional[str] = None
         self.last_fallback: tuple = ()
         self.last_relres = float("nan")
-        self._pattern = None      # (n, nc, nph, indptr, indices) of the cached handles
-        self._handles = {}        # local sweeps -> handle
+        self._pattern = {}        # transposed -> (n, nc, nph, indptr, indices) of its cached handles
+        self._handles = {}        # (transposed, local sweeps) -> handle
 
     # -- the reference's contract --------------------------------------------
     @staticmethod
@@ -125,16 +125,16 @@ class GpuCPRSolver:
                 f"block-Jacobi local stage, {self.precision})")
 
     # -- device handles ---------------------------------------------------------
-    def _handle(self, n, nc, nph, a: sp.csr_array, sweeps: int, stream):
+    def _handle(self, n, nc, nph, a: sp.csr_array, sweeps: int, stream, transposed: bool = False):
         rp = np.ascontiguousarray(a.indptr, dtype=np.int32)
         ci = np.ascontiguousarray(a.indices, dtype=np.int32)
-        pat = self._pattern
+        pat = self._pattern.get(transposed)
         same = (pat is not None and pat[:3] == (n, nc, nph) and pat[3].size == rp.size and
                 pat[4].size == ci.size and np.array_equal(pat[3], rp) and np.array_equal(pat[4], ci))
         if not same:
-            self.close()
-            self._pattern = (n, nc, nph, rp, ci)
-        h = self._handles.get(sweeps)
+            self._release(transposed)
+            self._pattern[transposed] = (n, nc, nph, rp, ci)
+        h = self._handles.get((transposed, sweeps))
         if h is None:
             o = N.CPROpts()
             N.check(N.lib().pmb_cpr_default_opts(N.C.byref(o)))
@@ -146,18 +146,21 @@ class GpuCPRSolver:
             o.local_sweeps = sweeps
             o.amg_rebuild_interval = self.amg_rebuild_interval
             h = N.c_vp()
-            rp, ci = self._pattern[3], self._pattern[4]
+            rp, ci = self._pattern[transposed][3], self._pattern[transposed][4]
             N.check(N.lib().pmb_csr_cpr_create(n, nc, nph, N.as_p(rp, N.C.c_int32), N.as_p(ci, N.C.c_int32),
-                                               N.C.byref(o), stream, N.C.byref(h)))
-            self._handles[sweeps] = h
+                                               int(transposed), N.C.byref(o), stream, N.C.byref(h)))
+            self._handles[(transposed, sweeps)] = h
         return h
+
+    def _release(self, transposed: bool) -> None:
+        for key in [k for k in self._handles if k[0] == transposed]:
+            N.lib().pmb_csr_cpr_destroy(self._handles.pop(key))
+        self._pattern.pop(transposed, None)
 
     def close(self) -> None:
         """Release the device handles (they are also released with the solver)."""
-        handles, self._handles = self._handles, {}
-        self._pattern = None
-        for h in handles.values():
-            N.lib().pmb_csr_cpr_destroy(h)
+        for tr in (False, True):
+            self._release(tr)
 
     def __del__(self):
         try:
@@ -167,6 +170,17 @@ class GpuCPRSolver:
 
     # -- the solve ------------------------------------------------------------------
     def solve(self, jac, rhs, model=None, state=None, dt: Optional[float] = None) -> np.ndarray:
+        """x with jac x = rhs (CPRSolver.solve, linear_solvers.py:426-545)."""
+        return self._solve(jac, rhs, model, state, transposed=False)
+
+    def solve_transposed(self, jac, rhs, model=None, state=None) -> np.ndarray:
+        """x with jac^T x = rhs: the adjoint solve of compute_gradient_adjoint
+        (optimization/adjoint.py:209), which the reference does with spsolve.
+        `jac` is the forward Jacobian; the CPR transfer operators are
+        transposed with it."""
+        return self._solve(jac, rhs, model, state, transposed=True)
+
+    def _solve(self, jac, rhs, model, state, transposed: bool) -> np.ndarray:
         import torch
         missing = self._unmet_requirements(model)
         if missing:
@@ -177,6 +191,8 @@ class GpuCPRSolver:
         if not torch.cuda.is_available():
             raise RuntimeError("GpuCPRSolver needs a CUDA device")
         a = sp.csr_array(jac, dtype=np.float64)
+        if transposed:
+            a = sp.csr_array(a.T)
         if not a.has_canonical_format:
             a = a.copy()
             a.sum_duplicates()
@@ -195,7 +211,7 @@ class GpuCPRSolver:
         info = (N.C.c_double * 4)()
 
         def attempt(sweeps):
-            h = self._handle(n, nc, nph, a, sweeps, stream)
+            h = self._handle(n, nc, nph, a, sweeps, stream, transposed)
             N.check(N.lib().pmb_csr_cpr_setup(h, N.ptr(vals), N.as_p(w, N.C.c_double)))
             rc = N.lib().pmb_csr_cpr_solve(h, N.ptr(bd), N.ptr(xd), info)
             if rc not in (N.PMB_OK, 5):

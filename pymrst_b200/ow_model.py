@@ -335,6 +335,18 @@ class GpuOilWaterModel:
         self.last_stats = stats
         return self.unpack(pin.numpy().copy()), ok, its
 
+    def set_controls(self, u) -> None:
+        """New well targets, one per well (the reference's `_set_controls`,
+        optimization/adjoint.py:63-65): `w.val` on the well objects and the
+        device model's targets."""
+        u = np.ascontiguousarray(np.asarray(u, dtype=np.float64).ravel())
+        if u.size != self.nw:
+            raise ValueError(f"{u.size} controls for {self.nw} wells")
+        for w, v in zip(self.wells, u):
+            w.val = float(v)
+        if self.nw:
+            N.check(N.lib().pmb_ow_set_controls(self._handle, N.as_p(u, N.C.c_double)))
+
     # -- assembly export (parity / protocol) ---------------------------------
     def compute_cdp(self, st0: OWState):
         torch = _torch()

@@ -6,7 +6,7 @@ Run once, where the reference's Python package is importable:
 
 It writes small .npz files holding inputs and the reference's own outputs
 (grid arrays, transmissibilities, oil-water residuals and Jacobians, Newton
-histories, incompressible pressure solves) plus the reference's MATLAB golden
+histories, incompressible pressure solves, adjoint gradients) plus the reference's MATLAB golden
 arrays (examples/validation/ref_p2_*.mat, ref_p5_ow.mat) copied as data.  The
 tests read only the .npz files, so they run without the reference.
 """
@@ -226,6 +226,44 @@ def incomp_fixtures():
          wflux0=st.wellSol[0].flux, wflux1=st.wellSol[1].flux, **wells_arrays("w", w))
 
 
+def adjoint_fixture(name, dims, phys, seed, fluid_kind, gravity, nsteps, dt_days):
+    """compute_gradient_adjoint (optimization/adjoint.py:161-225) with the NPV
+    objective on a small model with per-step well controls."""
+    from pymrst.modules.optimization.adjoint import compute_gradient_adjoint, npv_objective
+    g = compute_geometry(cart_grid(dims, phys))
+    perm = lognormal_perm(dims, seed)
+    rock = make_rock(g, perm[:, None], 0.2)
+    fluid = ow_fluid(fluid_kind)
+    nx, ny, nz = dims
+    col = lambda i, j: i + nx * (j + ny * np.arange(nz))
+    gvec = np.array([0, 0, gravity]) if gravity else None
+    pvtot = float(np.sum(0.2 * g.cells.volumes))
+    rate = 0.3 * pvtot / (nsteps * dt_days * DAY) / 2
+    w = add_well(None, g, rock, col(0, 0), well_type="rate", val=rate,
+                 compi=np.array([1.0, 0.0]), sign=1, gravity=gvec)
+    w = add_well(w, g, rock, col(nx - 1, 0), well_type="rate", val=rate,
+                 compi=np.array([1.0, 0.0]), sign=1, gravity=gvec)
+    w = add_well(w, g, rock, col(nx // 2, ny - 1), well_type="bhp", val=150 * BARSA,
+                 compi=np.array([0.0, 1.0]), sign=-1, gravity=gvec)
+    model = TwoPhaseOilWaterModelAD(g, rock, fluid, w, gravity=gravity)
+    st0 = model.initial_state(200 * BARSA, 0.1 if fluid_kind == "cfg" else 0.2)
+    rng = np.random.default_rng(seed)
+    controls = np.column_stack([rate * rng.uniform(0.7, 1.3, nsteps), rate * rng.uniform(0.7, 1.3, nsteps),
+                                BARSA * rng.uniform(140.0, 160.0, nsteps)])
+    dts = np.full(nsteps, dt_days * DAY)
+    wells0 = wells_arrays("w", w)  # before the sweep sets w.val to each step's controls
+    res = compute_gradient_adjoint(model, st0, dts, controls, npv_objective())
+    save(name, dims=np.array(dims), phys=np.array(phys, float), perm=perm, poro=np.array(0.2),
+         gravity=np.array(float(gravity)), fluid_kind=np.array(fluid_kind),
+         p0=st0.pressure, sw0=st0.sW, qws0=st0.qWs, qos0=st0.qOs, bhp0=st0.bhp, dts=dts, controls=controls,
+         value=np.array(res.value), gradient=res.gradient, dx0=res.initial_state_gradient,
+         p_hist=np.vstack([s.pressure for s in res.states[1:]]),
+         sw_hist=np.vstack([s.sW for s in res.states[1:]]),
+         qws_hist=np.vstack([s.qWs for s in res.states[1:]]),
+         qos_hist=np.vstack([s.qOs for s in res.states[1:]]),
+         bhp_hist=np.vstack([s.bhp for s in res.states[1:]]), **wells0)
+
+
 if __name__ == "__main__":
     grid_fixture()
     assemble_fixture("ow_assemble_nograv.npz", [6, 5, 3], [60.0, 50.0, 6.0], 3, "p5", 0.0, False)
@@ -235,3 +273,5 @@ if __name__ == "__main__":
     newton_fixture("ow_newton_nograv.npz", [10, 8, 3], [100.0, 80.0, 6.0], 7, "p5", 0.0, 4, 20.0)
     phase5_fixture()
     incomp_fixtures()
+    adjoint_fixture("adjoint_grav.npz", [7, 6, 3], [70.0, 60.0, 6.0], 8, "cfg", 9.80665, 4, 15.0)
+    adjoint_fixture("adjoint_nograv.npz", [8, 5, 2], [80.0, 50.0, 4.0], 9, "p5", 0.0, 3, 20.0)

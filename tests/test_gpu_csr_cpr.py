@@ -56,7 +56,7 @@ def test_spmv_matches_the_reference_jacobian(name):
     N.check(N.lib().pmb_cpr_default_opts(N.C.byref(o)))
     h = N.c_vp()
     N.check(N.lib().pmb_csr_cpr_create(n, model.G.cells.num, 2, N.as_p(rp, N.C.c_int32), N.as_p(ci, N.C.c_int32),
-                                       N.C.byref(o), None, N.C.byref(h)))
+                                       0, N.C.byref(o), None, N.C.byref(h)))
     try:
         x = np.random.default_rng(0).standard_normal(n)
         vals = torch.as_tensor(J.data, device="cuda")
@@ -99,7 +99,7 @@ def test_pattern_reuse_and_duplicate_entries():
                         (np.concatenate([coo.row, coo.row]), np.concatenate([coo.col, coo.col]))),
                        shape=J.shape).tocsr()
     x2 = solver.solve(dup, rhs, model, {"pressure": d["p"]})
-    assert solver._handles == h1  # same pattern after summing duplicates: handle kept
+    assert solver._handles == h1  # same pattern after summing duplicates: handles kept
     assert np.abs(x2 - x1).max() <= 1e-8 * np.abs(x1).max()
 
 
@@ -144,3 +144,19 @@ def test_newton_through_the_drop_in_matches_reference(name):
         assert its == int(d["its"][k])
         assert np.abs(st.pressure - d["p_hist"][k]).max() <= 1e-8 * np.abs(d["p_hist"][k]).max()
         assert np.abs(st.sW - d["sw_hist"][k]).max() <= 1e-7
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["ow_assemble_grav.npz", "ow_assemble_nograv.npz", "ow_assemble_xflow.npz"])
+def test_transposed_solve_matches_the_direct_adjoint_solve(name, precision):
+    """J^T x = b, the adjoint solve that compute_gradient_adjoint does with
+    spsolve (optimization/adjoint.py:209), to the same 1e-7 bar."""
+    d = load(name)
+    J, rhs = _jacobian(d)
+    model, _ = _model(d)
+    solver = GpuCPRSolver(rtol=1e-10, precision=precision)
+    got = solver.solve_transposed(J, rhs, model, {"pressure": d["p"]})
+    exact = spla.spsolve(sp.csc_matrix(J.T), rhs)
+    err = np.abs(got - exact).max() / np.abs(exact).max()
+    assert err < 1e-7, f"transposed CPR is not the direct solution: {err:.2e}"
+    assert solver.last_relres <= 1e-10

@@ -77,8 +77,8 @@ def _create(lib, n, nc, nph, rp, ci):
     h = N.c_vp()
     rp = np.asarray(rp, dtype=np.int32)
     ci = np.asarray(ci, dtype=np.int32)
-    rc = lib.pmb_csr_cpr_create(n, nc, nph, N.as_p(rp, N.C.c_int32), N.as_p(ci, N.C.c_int32), N.C.byref(o), None,
-                                N.C.byref(h))
+    rc = lib.pmb_csr_cpr_create(n, nc, nph, N.as_p(rp, N.C.c_int32), N.as_p(ci, N.C.c_int32), 0, N.C.byref(o),
+                                None, N.C.byref(h))
     return rc, lib.pmb_last_error().decode()
 
 

@@ -112,3 +112,24 @@ def test_oracle_phase5_matches_reference_and_matlab():
         mine = np.asarray(mine).ravel()
         ref = np.asarray(ref).ravel()
         assert np.abs(mine - ref).max() <= 5e-6 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", ["adjoint_grav.npz", "adjoint_nograv.npz"])
+def test_oracle_adjoint_matches_reference(name):
+    """compute_gradient_adjoint (optimization/adjoint.py:161-225) restated over
+    the oracle model, against the reference's own run."""
+    from oracle import adjoint as oadj
+    d = load(name)
+    g, rock, fluid, wells = ow_case(d)
+    prob = oow.build_problem(g, rock, fluid.params, wells, gravity=float(d["gravity"]))
+    st0 = oow.State(pressure=d["p0"].copy(), sW=d["sw0"].copy(), qWs=d["qws0"].copy(), qOs=d["qos0"].copy(),
+                    bhp=d["bhp0"].copy())
+    res = oadj.compute_gradient_adjoint(prob, st0, d["dts"], d["controls"])
+    for k, s in enumerate(res.states[1:]):
+        assert np.abs(s.pressure - d["p_hist"][k]).max() <= 1e-8 * np.abs(d["p_hist"][k]).max()
+        assert np.abs(s.sW - d["sw_hist"][k]).max() <= 1e-7
+    assert abs(res.value - float(d["value"])) <= 1e-9 * abs(float(d["value"]))
+    for j in range(d["gradient"].shape[1]):
+        ref = d["gradient"][:, j]
+        assert np.abs(res.gradient[:, j] - ref).max() <= 1e-6 * np.abs(ref).max()
+    assert np.abs(res.initial_state_gradient - d["dx0"]).max() <= 1e-6 * np.abs(d["dx0"]).max()
