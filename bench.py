@@ -279,7 +279,7 @@ def run_ours(args):
     n_smooth = int(round(dims[2] * 35 / 85))
     case = cases.channelised(dims=dims, cell_size=WORKLOAD["cell_size"], n_smooth=n_smooth)
     copts = dict(rtol=1e-8, maxiter=400, restart=50, amg_rebuild_interval=1_000_000,
-                 precision=1 if args.precision == "mixed" else 0, amg_cycle=3, local_sweeps=3, amg_theta=0.1)
+                 precision=1 if args.precision == "mixed" else 0, amg_cycle=3, local_sweeps=4, amg_theta=0.1)
     for kv in filter(None, args.cpr.split(",")):
         k, v = kv.split("=")
         copts[k] = float(v) if k in ("rtol", "amg_theta", "inner_rtol") else int(v)

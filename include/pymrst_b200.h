@@ -179,7 +179,7 @@ typedef struct pmb_cpr_opts {
 } pmb_cpr_opts;
 
 /* Defaults: rtol 1e-8, maxiter 200, restart 50 (CPRSolver's,
- * linear_solvers.py:113-116); local_sweeps 3, Chebyshev degree 2, K-cycle on
+ * linear_solvers.py:113-116); local_sweeps 4, Chebyshev degree 2, K-cycle on
  * 3 levels, theta 0.1, coarse size 200, re-aggregation every 8 setups. */
 int pmb_cpr_default_opts(pmb_cpr_opts* out);
 int pmb_cpr_create(pmb_ow* model, const pmb_cpr_opts* opts, pmb_cpr** out);
@@ -199,6 +199,23 @@ int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* h_sizes, int32
  * 2: the whole preconditioner z = M^{-1} r.  Needs pmb_cpr_setup first. */
 int pmb_cpr_time_stage(pmb_cpr* s, int32_t stage, const double* d_r, double* d_z, int32_t reps,
                        double* h_ms);
+
+/* A batch of independent models (an ensemble of realisations, run_ensemble,
+ * pymrst/modules/ensemble/ensemble_impl.py:49-67, which runs them one after
+ * another) stored as one model whose members share no interface: member m
+ * owns cells [h_cell_ptr[m], h_cell_ptr[m+1]) and wells [h_well_ptr[m],
+ * h_well_ptr[m+1]).  One backward-Euler step of every member with h_state[m]
+ * = 1, by one Newton loop whose kernels cover all members, with the
+ * convergence test of step (two_phase_oil_water_model.py:605-657) applied
+ * to each member alone: a converged member is frozen (zero right-hand side,
+ * zero correction) while the others iterate.  Members with h_state[m] = 0
+ * are left as they are.  On return h_state[m] = 1 converged, 0 failed (its
+ * state restored to the start of the step), -1 frozen; h_its[m] its Newton
+ * iterations; h_stats4 = [krylov iterations, setups, Newton iterations of
+ * the batch, 0]. */
+int pmb_ow_step_members(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_iterations, int32_t nmem,
+                        const int32_t* h_cell_ptr, const int32_t* h_well_ptr, int32_t* h_state, int32_t* h_its,
+                        double* h_stats4);
 
 /* ------------------------------------------------------------------------
  * CPR on a caller's CSR matrix: the device side of the drop-in for

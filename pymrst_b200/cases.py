@@ -141,3 +141,19 @@ def channelised(dims=(60, 220, 85), cell_size=(6.1, 3.05, 0.61), seed=2, n_smoot
     wells = _five_spot_wells(g, rock, rate, 100 * BARSA, gravity)
     return OWCase(f"channelised_{nx}x{ny}x{nz}", g, rock, ow_fluid(), wells,
                   200 * BARSA, 0.1, dt_days * DAY, nsteps, gravity)
+
+
+def ensemble_realisations(n: int = 256, seed: int = 3, nx_range=(16, 64), nz_range=(2, 8),
+                          cell_size=(10.0, 10.0, 2.0), nsteps: int = 15, dt_days: float = 30.0,
+                          gravity: float = 9.80665, pv_fraction: float = 0.25) -> list:
+    """Oil-water realisations of varying size: nx, ny uniform in nx_range and
+    nz in nz_range (seeded), an independent lognormal permeability each, a
+    five-spot each, the shared fluid; 15 steps of 30 days by default."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nx, ny = (int(v) for v in rng.integers(nx_range[0], nx_range[1] + 1, size=2))
+        nz = int(rng.integers(nz_range[0], nz_range[1] + 1))
+        out.append(five_spot(dims=(nx, ny, nz), cell_size=cell_size, seed=int(rng.integers(1 << 30)),
+                             nsteps=nsteps, dt_days=dt_days, gravity=gravity, pv_fraction=pv_fraction))
+    return out

@@ -90,6 +90,11 @@ using namespace pmb;
 struct pmb_ow {
   std::unique_ptr<OWModel> m;
   PinnedArray<double> conv;
+  // batch-of-members stepping: member ranges, flags and per-member values
+  DArray<int> mem_cell, mem_well, mem_flag;
+  DArray<double> mem_conv;
+  PinnedArray<double> mem_conv_h;
+  PinnedArray<int> mem_flag_h;
 };
 
 struct pmb_cpr {
@@ -269,7 +274,7 @@ int pmb_cpr_default_opts(pmb_cpr_opts* o) {
     o->restart = 50;
     o->precision = 0;
     o->use_pressure_stage = 1;
-    o->local_sweeps = 3;
+    o->local_sweeps = 4;
     o->amg_smoother_degree = 2;
     o->amg_cycle = 3;
     o->amg_theta = 0.1;
@@ -414,6 +419,129 @@ int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_itera
     stats[4] = h->conv[0];
     stats[5] = h->conv[1];
     stats[6] = h->conv[6];
+  });
+}
+
+int pmb_ow_step_members(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_iterations, int32_t nmem,
+                        const int32_t* h_cell_ptr, const int32_t* h_well_ptr, int32_t* h_state, int32_t* h_its,
+                        double* h_stats4) {
+  return guarded([&] {
+    PMB_REQUIRE(h && s && h_cell_ptr && h_well_ptr && h_state && h_its && h_stats4, "NULL argument");
+    PMB_REQUIRE(s->owner == h, "solver belongs to another model");
+    PMB_REQUIRE(dt > 0.0, "dt must be positive");
+    PMB_REQUIRE(max_iterations >= 0, "negative iteration limit");
+    PMB_REQUIRE(nmem >= 1, "need at least one member");
+    require_aligned(d_x, 16, "x");
+    OWModel& m = *h->m;
+    const OWView v = m.view();
+    PMB_REQUIRE(h_cell_ptr[0] == 0 && h_cell_ptr[nmem] == v.nc, "member cell ranges must cover the cells");
+    PMB_REQUIRE(h_well_ptr[0] == 0 && h_well_ptr[nmem] == v.nw, "member well ranges must cover the wells");
+    for (int k = 0; k < nmem; ++k) {
+      PMB_REQUIRE(h_cell_ptr[k + 1] > h_cell_ptr[k], "every member needs cells");
+      PMB_REQUIRE(h_well_ptr[k + 1] >= h_well_ptr[k], "member well ranges must be non-decreasing");
+    }
+    CPRSolver& cpr = *s->s;
+    cudaStream_t st = m.stream();
+    const long long n = m.nvec();
+    if ((int)h->mem_flag.size() != nmem) {
+      h->mem_cell.resize(nmem + 1);
+      h->mem_well.resize(nmem + 1);
+      h->mem_flag.resize(nmem);
+      h->mem_conv.resize(8LL * nmem);
+      h->mem_conv_h.resize(8LL * nmem);
+      h->mem_flag_h.resize(nmem);
+    }
+    PMB_CUDA(cudaMemcpyAsync(h->mem_cell.get(), h_cell_ptr, sizeof(int) * (nmem + 1), cudaMemcpyHostToDevice, st));
+    PMB_CUDA(cudaMemcpyAsync(h->mem_well.get(), h_well_ptr, sizeof(int) * (nmem + 1), cudaMemcpyHostToDevice, st));
+    // h_state in: 1 take the step, 0 frozen.  Working state: 1 active,
+    // 2 converged, 3 failed, 0 frozen.
+    std::vector<int> state(nmem);
+    for (int k = 0; k < nmem; ++k) {
+      state[k] = h_state[k] != 0 ? 1 : 0;
+      h_its[k] = 0;
+    }
+    for (int i = 0; i < 4; ++i) h_stats4[i] = 0.0;
+    PMB_CUDA(cudaMemcpyAsync(m.x0(), d_x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    m.compute_cdp(m.x0(), m.cdp());
+    double krylov = 0.0;
+    auto evaluate = [&](bool want_jac) {
+      m.assemble(d_x, m.x0(), dt, m.cdp(), m.res(), m.jac(), m.well(), want_jac);
+      m.member_convergence_async(nmem, h->mem_cell.get(), h->mem_well.get(), m.res(), d_x, dt, h->mem_conv.get());
+      PMB_CUDA(cudaMemcpyAsync(h->mem_conv_h.get(), h->mem_conv.get(), sizeof(double) * 8 * nmem,
+                               cudaMemcpyDeviceToHost, st));
+      PMB_CUDA(cudaStreamSynchronize(st));
+    };
+    auto classify = [&](int it) {  // returns the number of members still active
+      int active = 0;
+      for (int k = 0; k < nmem; ++k) {
+        if (state[k] != 1) continue;
+        const double* c = h->mem_conv_h.get() + 8LL * k;
+        if (c[5] != 0.0) {
+          state[k] = 2;
+          h_its[k] = it;
+        } else if (c[6] != 0.0) {
+          state[k] = 3;  // non-finite residual: the member's step fails
+          h_its[k] = it;
+        } else {
+          ++active;
+        }
+      }
+      return active;
+    };
+    int it = 0;
+    int active = 0;
+    for (; it < max_iterations; ++it) {
+      evaluate(true);
+      active = classify(it);
+      if (active == 0) break;
+      for (int k = 0; k < nmem; ++k) h->mem_flag_h[k] = state[k] == 1 ? 1 : 0;
+      PMB_CUDA(cudaMemcpyAsync(h->mem_flag.get(), h->mem_flag_h.get(), sizeof(int) * nmem, cudaMemcpyHostToDevice,
+                               st));
+      // members that are not active get a zero right-hand side, hence a zero
+      // correction: the preconditioner never couples members
+      m.mask_members(nmem, h->mem_cell.get(), h->mem_well.get(), h->mem_flag.get(), m.res());
+      cpr.setup(m.jac(), m.well(), d_x);
+      double info[4];
+      const bool ok = cpr.solve(m.res(), m.dx(), info);
+      krylov += info[0];
+      if (!ok) {
+        for (int k = 0; k < nmem; ++k)
+          if (state[k] == 1) {
+            state[k] = 3;
+            h_its[k] = it;
+          }
+        active = 0;
+        break;
+      }
+      m.mask_members(nmem, h->mem_cell.get(), h->mem_well.get(), h->mem_flag.get(), m.dx());
+      m.update(d_x, m.dx(), -1.0);
+    }
+    if (active > 0) {  // iteration limit: one more check, as the reference's step makes
+      evaluate(false);
+      for (int k = 0; k < nmem; ++k)
+        if (state[k] == 1) {
+          const double* c = h->mem_conv_h.get() + 8LL * k;
+          state[k] = c[5] != 0.0 ? 2 : 3;
+          h_its[k] = max_iterations;
+        }
+    }
+    // failed members go back to the start of the step
+    for (int k = 0; k < nmem; ++k) {
+      if (state[k] != 3) continue;
+      const long long c0 = h_cell_ptr[k], c1 = h_cell_ptr[k + 1];
+      PMB_CUDA(cudaMemcpyAsync(d_x + 2 * c0, m.x0() + 2 * c0, sizeof(double) * 2 * (c1 - c0),
+                               cudaMemcpyDeviceToDevice, st));
+      const long long w0 = h_well_ptr[k], w1 = h_well_ptr[k + 1];
+      if (w1 > w0)
+        PMB_CUDA(cudaMemcpyAsync(d_x + 2LL * v.nc + 3 * w0, m.x0() + 2LL * v.nc + 3 * w0,
+                                 sizeof(double) * 3 * (w1 - w0), cudaMemcpyDeviceToDevice, st));
+    }
+    PMB_CUDA(cudaStreamSynchronize(st));
+    for (int k = 0; k < nmem; ++k) h_state[k] = state[k] == 2 ? 1 : (state[k] == 3 ? 0 : -1);
+    h_stats4[0] = krylov;
+    h_stats4[1] = (double)cpr.setups();
+    h_stats4[2] = it;
+    h_stats4[3] = 0.0;
   });
 }
 

@@ -605,6 +605,87 @@ __global__ void __launch_bounds__(256) ow_conv_final_kernel(OWView v, const doub
   }
 }
 
+// Convergence of each member of a batch of independent models stored as one
+// (block m: cells [cell_ptr[m], cell_ptr[m+1]), wells [well_ptr[m],
+// well_ptr[m+1])): the values of ow_conv_final_kernel computed over the
+// member alone, its pore volume and rate scale included.
+__global__ void __launch_bounds__(256) ow_member_conv_kernel(OWView v, const int* __restrict__ cell_ptr,
+                                                             const int* __restrict__ well_ptr,
+                                                             const double* __restrict__ res,
+                                                             const double* __restrict__ x, double dt,
+                                                             double* __restrict__ out) {
+  __shared__ double sh[32];
+  const int m = blockIdx.x;
+  const int c0 = cell_ptr[m], c1 = cell_ptr[m + 1];
+  const double2* r2 = reinterpret_cast<const double2*>(res);
+  const double2* x2 = reinterpret_cast<const double2*>(x);
+  double mw = 0, mo = 0, sw = 0, so = 0, iw = 0, io = 0, bad = 0, pvs = 0;
+  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    const double2 r = r2[c];
+    const double pv = v.pv[c];
+    const double aw = fabs(r.x / pv), ao = fabs(r.y / pv);
+    if (!(isfinite(aw) && isfinite(ao))) bad += 1.0;
+    mw = fmax(mw, aw);
+    mo = fmax(mo, ao);
+    sw += r.x;
+    so += r.y;
+    pvs += pv;
+    double b, db;
+    shrink(v.fl, 0, x2[c].x, b, db);
+    iw += 1.0 / b;
+    shrink(v.fl, 1, x2[c].x, b, db);
+    io += 1.0 / b;
+  }
+  mw = block_max(mw, sh); mo = block_max(mo, sh);
+  sw = block_sum(sw, sh); so = block_sum(so, sh);
+  iw = block_sum(iw, sh); io = block_sum(io, sh);
+  bad = block_sum(bad, sh); pvs = block_sum(pvs, sh);
+  if (threadIdx.x != 0) return;
+  const int nc = c1 - c0, w0 = well_ptr[m], w1 = well_ptr[m + 1];
+  double qmax = 0.0;
+  bool any_rate = false;
+  for (int k = w0; k < w1; ++k)
+    if (v.well_type[k] == 1) { any_rate = true; qmax = fmax(qmax, fabs(v.well_val[k])); }
+  const double q_ref = any_rate ? fmax(qmax, 1e-12) : 1.0;
+  const double bw = iw / nc, bo = io / nc;
+  const double cnv = fmax(bw * dt * mw, bo * dt * mo);
+  const double mb = fmax(bw * dt * fabs(sw) / pvs, bo * dt * fabs(so) / pvs);
+  double ew = 0.0, eo = 0.0;
+  bool ctrl_ok = true, finite = bad == 0.0 && isfinite(cnv) && isfinite(mb);
+  const double* rw = res + 2LL * v.nc;
+  for (int k = w0; k < w1; ++k) {
+    const double a = fabs(rw[3 * k]), b = fabs(rw[3 * k + 1]), c = fabs(rw[3 * k + 2]);
+    finite = finite && isfinite(a) && isfinite(b) && isfinite(c);
+    ew = fmax(ew, a);
+    eo = fmax(eo, b);
+    const double scale = v.well_type[k] == 0 ? 1.0e5 : q_ref;
+    ctrl_ok = ctrl_ok && (c <= v.tol_well * scale);
+  }
+  const bool well_ok = w1 == w0 || (ew <= v.tol_well * q_ref && eo <= v.tol_well * q_ref);
+  const bool conv = finite && cnv <= v.tol_cnv && mb <= v.tol_mb && well_ok && ctrl_ok;
+  double* o = out + 8LL * m;
+  o[0] = cnv;
+  o[1] = mb;
+  o[2] = ew / q_ref;
+  o[3] = eo / q_ref;
+  o[4] = ctrl_ok ? 1.0 : 0.0;
+  o[5] = conv ? 1.0 : 0.0;
+  o[6] = finite ? 0.0 : 1.0;
+  o[7] = 0.0;
+}
+
+// Zero the entries (cells and wells) of every member whose flag is 0.
+__global__ void __launch_bounds__(256) ow_member_mask_kernel(OWView v, const int* __restrict__ cell_ptr,
+                                                             const int* __restrict__ well_ptr,
+                                                             const int* __restrict__ flag,
+                                                             double* __restrict__ vec) {
+  const int m = blockIdx.x;
+  if (flag[m] != 0) return;
+  for (int c = cell_ptr[m] + threadIdx.x; c < cell_ptr[m + 1]; c += blockDim.x)
+    reinterpret_cast<double2*>(vec)[c] = make_double2(0.0, 0.0);
+  for (int t = 3 * well_ptr[m] + threadIdx.x; t < 3 * well_ptr[m + 1]; t += blockDim.x) vec[2LL * v.nc + t] = 0.0;
+}
+
 __global__ void __launch_bounds__(256) ow_update_kernel(OWView v, double* __restrict__ x,
                                                         const double* __restrict__ dx, double sgn) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -885,6 +966,17 @@ void OWModel::spmv(const double* jac, const double* well, const double* x, doubl
     ow_well_spmv_kernel<<<1, 256, sizeof(double) * 2 * v_.nw, stream_>>>(v_, well, x, y);
     PMB_CHECK_LAUNCH();
   }
+}
+
+void OWModel::member_convergence_async(int nmem, const int* cell_ptr, const int* well_ptr, const double* res,
+                                       const double* x, double dt, double* d_out) {
+  ow_member_conv_kernel<<<nmem, 256, 0, stream_>>>(v_, cell_ptr, well_ptr, res, x, dt, d_out);
+  PMB_CHECK_LAUNCH();
+}
+
+void OWModel::mask_members(int nmem, const int* cell_ptr, const int* well_ptr, const int* flag, double* vec) {
+  ow_member_mask_kernel<<<nmem, 256, 0, stream_>>>(v_, cell_ptr, well_ptr, flag, vec);
+  PMB_CHECK_LAUNCH();
 }
 
 void OWModel::convergence_async(const double* res, const double* x, double dt, double* d_out) {

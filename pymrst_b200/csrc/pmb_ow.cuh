@@ -99,6 +99,13 @@ class OWModel {
   // New well targets (bhp or total rate per well), and the rate scale of
   // the well convergence test that depends on them.
   void set_well_values(const double* h_val);
+  // A batch of independent models stored as one (member m: cells
+  // [cell_ptr[m], cell_ptr[m+1]), wells [well_ptr[m], well_ptr[m+1]), device
+  // arrays): the convergence values of each member (8 per member, the layout
+  // of convergence_async), and zeroing the entries of members whose flag is 0.
+  void member_convergence_async(int nmem, const int* cell_ptr, const int* well_ptr, const double* res,
+                                const double* x, double dt, double* d_out);
+  void mask_members(int nmem, const int* cell_ptr, const int* well_ptr, const int* flag, double* vec);
   void assemble(const double* x, const double* x0, double dt, const double* cdp, double* res,
                 double* jac, double* well, bool want_jac);
   void spmv(const double* jac, const double* well, const double* x, double* y);

@@ -202,6 +202,17 @@ class GpuCPRSolver:
         rhs = np.ascontiguousarray(np.asarray(rhs, dtype=np.float64).ravel())
         if rhs.size != n or a.shape[1] != n:
             raise ValueError(f"matrix {a.shape} and right-hand side ({rhs.size}) do not match")
+        if transposed:
+            # Rows of J^T span many orders of magnitude (well-control columns of
+            # J are O(1), cell columns O(1e-10)); scaling each row to unit max
+            # norm makes the GMRES residual criterion uniform over the
+            # unknowns.  The solution is unchanged, and so is the CPR: block
+            # inverses and the pressure AMG do not see a row scaling.
+            rmax = np.asarray(abs(a).max(axis=1).todense()).ravel()
+            d = np.where(rmax > 0.0, 1.0 / np.where(rmax > 0.0, rmax, 1.0), 1.0)
+            a = sp.csr_array(sp.diags_array(d) @ a)
+            a.sum_duplicates()
+            rhs = np.ascontiguousarray(d * rhs)
         w = self.weights(model, state) if self.use_pressure_stage else np.ones(nph)
         w = np.ascontiguousarray(w, dtype=np.float64)
         stream = torch.cuda.current_stream().cuda_stream

@@ -199,8 +199,10 @@ class GpuOilWaterModel:
         )
         # vertical interfaces (|n_z| dominant) chain cells into the lines the
         # CPR second stage solves along
-        normals = getattr(self.g.faces, "normals", None)
-        if normals is not None and np.asarray(normals).shape[1] == 3 and self.N.shape[0]:
+        normals = getattr(getattr(self.g, "faces", None), "normals", None)
+        if getattr(self, "_line_face", None) is not None:
+            self._h["line_face"] = np.ascontiguousarray(self._line_face, dtype=np.int32)
+        elif normals is not None and np.asarray(normals).shape[1] == 3 and self.N.shape[0]:
             nrm = np.abs(np.asarray(normals)[self._internal])
             line = (nrm[:, 2] > nrm[:, 0]) & (nrm[:, 2] > nrm[:, 1])
             self._h["line_face"] = np.ascontiguousarray(line, dtype=np.int32)
