@@ -110,6 +110,16 @@ int pmb_ow_pattern(const pmb_ow* h, int32_t* h_row_ptr, int32_t* h_col);
 int pmb_ow_compute_cdp(pmb_ow* h, const double* d_x0, double* d_cdp);
 /* Forget the previous-step cdp (a fresh model). */
 int pmb_ow_reset_cdp(pmb_ow* h);
+/* The flux terms of assemble at state d_x (two_phase_oil_water_model.py:
+ * 520-546 and the perforation rates of :286-491): d_face_flux (nf x 2,
+ * water then oil) holds what interface f adds to the residual rows of
+ * N[f,0] and subtracts from those of N[f,1]; d_perf_rate (nperf x 2) the
+ * surface rates each perforation subtracts from its cell's rows and from its
+ * well's rate equations.  Both are linear in T[f] and in the perforation's
+ * well index (for wells without cross-flow), which is what the adjoint
+ * gradient with respect to permeability uses.  Uses the model's residual
+ * workspace (not during a step on the same handle). */
+int pmb_ow_fluxes(pmb_ow* h, const double* d_x, const double* d_cdp, double* d_face_flux, double* d_perf_rate);
 /* New well targets, one per well: bhp for bhp wells, total surface rate for
  * rate wells (_set_controls, pymrst/modules/optimization/adjoint.py:63-65,
  * which sets w.val between timesteps).  Also rescales the well convergence

@@ -64,6 +64,7 @@ SIGNATURES = {
     "pmb_ow_compute_cdp": (c_int, [c_vp, c_vp, c_vp]),
     "pmb_ow_reset_cdp": (c_int, [c_vp]),
     "pmb_ow_set_controls": (c_int, [c_vp, P_dbl]),
+    "pmb_ow_fluxes": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_ow_assemble": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp, c_vp, c_int]),
     "pmb_ow_spmv": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_ow_convergence": (c_int, [c_vp, c_vp, c_vp, c_dbl, P_dbl]),

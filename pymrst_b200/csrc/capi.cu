@@ -208,6 +208,19 @@ int pmb_ow_reset_cdp(pmb_ow* h) {
   });
 }
 
+int pmb_ow_fluxes(pmb_ow* h, const double* d_x, const double* d_cdp, double* d_face_flux, double* d_perf_rate) {
+  return guarded([&] {
+    PMB_REQUIRE(h && d_x && d_face_flux, "NULL argument");
+    const OWView v = h->m->view();
+    PMB_REQUIRE(v.nw == 0 || (d_cdp && d_perf_rate), "wells need cdp and a rate buffer");
+    require_aligned(d_x, 16, "x");
+    require_aligned(d_face_flux, 16, "face_flux");
+    if (v.nw) require_aligned(d_perf_rate, 16, "perf_rate");
+    h->m->fluxes(d_x, d_cdp, d_face_flux, d_perf_rate);
+    PMB_CUDA(cudaStreamSynchronize(h->m->stream()));
+  });
+}
+
 int pmb_ow_set_controls(pmb_ow* h, const double* h_well_val) {
   return guarded([&] {
     PMB_REQUIRE(h && (h_well_val || h->m->view().nw == 0), "NULL argument");

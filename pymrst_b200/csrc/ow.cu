@@ -163,6 +163,30 @@ __global__ void __launch_bounds__(256) ow_cell_kernel(OWView v, const double2* _
   if (JAC) jac[v.diag_pos[c]] = make_double4(d00, d01, d10, d11);
 }
 
+// Phase fluxes of every interface, written by its N0 cell with the arithmetic
+// of ow_cell_kernel: face f adds flux[f] to the residual rows (water, oil) of
+// N[f,0] and subtracts it from those of N[f,1].
+__global__ void __launch_bounds__(256) ow_face_flux_kernel(OWView v, const double2* __restrict__ x,
+                                                           double2* __restrict__ flux) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= v.nc) return;
+  const FluidDev& f = v.fl;
+  const double2 xs = x[c];
+  const CellProps P = cell_props(f, xs.x, xs.y);
+  for (int k = v.row_ptr[c]; k < v.row_ptr[c + 1]; ++k) {
+    const int code = v.nz_face[k];
+    if (code == INT_MIN || code < 0) continue;  // diagonal, or this cell is N[f,1]
+    const int nb = v.col[k];
+    const double T = v.T[code], g = v.gdz[code];
+    const double2 xn = x[nb];
+    const CellProps Q = cell_props(f, xn.x, xn.y);
+    const double dp = xn.x - xs.x;
+    const PhaseFlux W = phase_flux(f.rhoS[0], T, g, dp, P.bw, P.dbw, P.mw, P.dmw, Q.bw, Q.dbw, Q.mw, Q.dmw);
+    const PhaseFlux O = phase_flux(f.rhoS[1], T, g, dp, P.bo, P.dbo, P.mo, P.dmo, Q.bo, Q.dbo, Q.mo, Q.dmo);
+    flux[code] = make_double2(W.F, O.F);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // wells: one warp per well inside a single CTA (standard well model,
 // _well_contributions_batched, two_phase_oil_water_model.py:286-491)
@@ -926,6 +950,22 @@ void OWModel::compute_cdp(const double* x0, double* cdp) {
   PMB_CHECK_LAUNCH();
   PMB_CUDA(cudaMemcpyAsync(last_cdp_.get(), cdp, sizeof(double) * np_, cudaMemcpyDeviceToDevice, stream_));
   have_last_cdp_ = true;
+}
+
+void OWModel::fluxes(const double* x, const double* cdp, double* face_flux, double* perf_rate) {
+  ow_face_flux_kernel<<<grid_for(v_.nc, 256), 256, 0, stream_>>>(v_, reinterpret_cast<const double2*>(x),
+                                                                 reinterpret_cast<double2*>(face_flux));
+  PMB_CHECK_LAUNCH();
+  if (v_.nw) {
+    // the well kernel also subtracts the rates from a residual: give it the
+    // model's residual workspace
+    ow_well_kernel<false><<<1, 256, 0, stream_>>>(v_, reinterpret_cast<const double2*>(x), cdp, res_.get(),
+                                                  nullptr, nullptr, reinterpret_cast<double2*>(pf_cq_.get()),
+                                                  reinterpret_cast<double4*>(pf_dloc_.get()));
+    PMB_CHECK_LAUNCH();
+    PMB_CUDA(cudaMemcpyAsync(perf_rate, pf_cq_.get(), sizeof(double) * 2 * v_.nperf, cudaMemcpyDeviceToDevice,
+                             stream_));
+  }
 }
 
 void OWModel::assemble(const double* x, const double* x0, double dt, const double* cdp, double* res,

@@ -106,6 +106,11 @@ class OWModel {
   void member_convergence_async(int nmem, const int* cell_ptr, const int* well_ptr, const double* res,
                                 const double* x, double dt, double* d_out);
   void mask_members(int nmem, const int* cell_ptr, const int* well_ptr, const int* flag, double* vec);
+  // Phase fluxes of every interface (what face f adds to the rows of N[f,0]
+  // and subtracts from those of N[f,1]) and every perforation's surface
+  // rates (what it subtracts from its cell's rows and its well's rate rows)
+  // at state x; uses the model's residual workspace.
+  void fluxes(const double* x, const double* cdp, double* face_flux, double* perf_rate);
   void assemble(const double* x, const double* x0, double dt, const double* cdp, double* res,
                 double* jac, double* well, bool want_jac);
   void spmv(const double* jac, const double* well, const double* x, double* y);
