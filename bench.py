@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
+                    help="mixed: FP32 AMG and smoother blocks inside the FP64 FGMRES (the benchmark's method); fp64: all FP64")
     ap.add_argument("--dims", default=None, help="override grid dims, e.g. 30,110,40")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)

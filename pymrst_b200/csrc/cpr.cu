@@ -491,6 +491,12 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
     const int t = t0 + u;
     c = lcells[t];
     double2 rc = reinterpret_cast<const double2*>(r)[c];
+    // the line blocks first, so that their loads overlap the row gather
+    const int kl = u > 0 ? llo[t] : -1;
+    const int ku = u + 1 < len ? lup[t] : -1;
+    D = ld4(A[v.diag_pos[c]]);
+    if (kl >= 0) Lb = ld4(A[kl]);
+    if (ku >= 0) Ub = ld4(A[ku]);
     sub_row(v.col, A, z2, v.row_ptr[c], v.row_ptr[c + 1], rc);
     const int q = v.cell_pc[c];
     if (q >= 0) {
@@ -504,9 +510,6 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
       }
     }
     y = rc;
-    D = ld4(A[v.diag_pos[c]]);
-    if (u > 0 && llo[t] >= 0) Lb = ld4(A[llo[t]]);
-    if (u + 1 < len && lup[t] >= 0) Ub = ld4(A[lup[t]]);
   }
   for (int s = 1; s < len; s <<= 1) {
     bool ok = true;
