@@ -2,6 +2,7 @@
 // smoothing, V-cycle, dense coarsest solve.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <numeric>
 #include <type_traits>
 
@@ -253,6 +254,21 @@ inline int lanes_for(long long n, long long nnz) {
   return 4;
 }
 
+// Coefficients of step `step` of the Chebyshev recurrence on [lm/10, lm].
+__device__ __forceinline__ void cheb_coeffs(double lm, int step, double& c1, double& c2) {
+  const double lo = lm / 10.0;
+  const double theta = 0.5 * (lm + lo), delta = 0.5 * (lm - lo), sigma = theta / delta;
+  double rho = 1.0 / sigma;
+  c1 = 0.0;
+  c2 = 1.0 / theta;
+  for (int k = 1; k <= step; ++k) {
+    const double rho1 = 1.0 / (2.0 * sigma - rho);
+    c1 = rho1 * rho;
+    c2 = 2.0 * rho1 / delta;
+    rho = rho1;
+  }
+}
+
 // Chebyshev on D^{-1} A over [lmax/10, lmax]: step `step` of the
 // three-term recurrence; x_out = x_in + d, d = c1 d + c2 D^{-1}(b - A x_in).
 // LANES threads share a row.
@@ -272,16 +288,8 @@ __global__ void __launch_bounds__(256) cheb_step_kernel(int n, const int* __rest
     ax = group_sum<LANES>(ax);
   }
   if (i >= n || sub != 0) return;
-  const double lm = lmax[0];
-  const double lo = lm / 10.0;
-  const double theta = 0.5 * (lm + lo), delta = 0.5 * (lm - lo), sigma = theta / delta;
-  double rho = 1.0 / sigma, c1 = 0.0, c2 = 1.0 / theta;
-  for (int k = 1; k <= step; ++k) {
-    const double rho1 = 1.0 / (2.0 * sigma - rho);
-    c1 = rho1 * rho;
-    c2 = 2.0 * rho1 / delta;
-    rho = rho1;
-  }
+  double c1, c2;
+  cheb_coeffs(lmax[0], step, c1, c2);
   const double r = ((double)b[i] - ax) * (double)dinv[i];
   const double dn = (step == 0 ? 0.0 : c1 * (double)d[i]) + c2 * r;
   d[i] = (T)dn;
@@ -403,6 +411,157 @@ __global__ void dense_apply_kernel(int n, const double* __restrict__ Inv, const 
   for (int j = lane; j < n; j += 32) s += Inv[(size_t)row * n + j] * (double)b[j];
   s = warp_sum(s);
   if (lane == 0) x[row] = (T)s;
+}
+
+// Fused coarse cycle ---------------------------------------------------------
+//
+// The V-cycle from level `first` down to the dense coarsest solve in one
+// cooperative launch, the steps separated by a grid barrier: the same
+// arithmetic, row grouping and buffer order as the per-step kernels, so the
+// result is identical; what goes is one launch per step on levels of a few
+// thousand rows, where launch latency is the whole cost.
+
+constexpr long long kBarrierSpins = 1LL << 24;  // with 64 ns sleeps: about a second
+
+// Grid barrier for a cooperative launch.  Bounded: a block that waits too
+// long records PMB_ERR_INTERNAL in *status and goes on; once the status is
+// set, every later barrier returns at once, so a fault cannot hang the GPU.
+__device__ __forceinline__ void grid_barrier(unsigned int* bar, int* status) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* gen = bar + 1;
+    volatile int* st = status;
+    if (*st == 0) {
+      const unsigned int g = *gen;
+      __threadfence();
+      if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+        bar[0] = 0;
+        __threadfence();
+        atomicAdd(bar + 1, 1u);
+      } else {
+        long long spins = 0;
+        while (*gen == g) {
+          if (*st != 0) break;
+          if (++spins > kBarrierSpins) {
+            atomicExch(status, PMB_ERR_INTERNAL);
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+}
+
+// Sum over a group of `lanes` consecutive lanes (a power of two <= 32), the
+// order of group_sum<LANES>.
+__device__ __forceinline__ double group_sum_rt(double v, int lanes) {
+  for (int o = lanes >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <class T, bool ZERO>
+__device__ void fused_cheb_rows(const CoopLevel<T>& L, const T* b, const T* xin, T* xout, int step, long long tid,
+                                long long nthr) {
+  double c1, c2;
+  cheb_coeffs(L.lmax[0], step, c1, c2);
+  const long long total = ((long long)L.n * L.lanes + 31) / 32 * 32;
+  for (long long t = tid; t < total; t += nthr) {
+    const long long i = t / L.lanes;
+    const int sub = (int)(t % L.lanes);
+    double ax = 0.0;
+    if (!ZERO) {
+      if (i < L.n)
+        for (int k = L.rp[i] + sub; k < L.rp[i + 1]; k += L.lanes) ax += (double)L.val[k] * (double)xin[L.ci[k]];
+      ax = group_sum_rt(ax, L.lanes);
+    }
+    if (i < L.n && sub == 0) {
+      const double r = ((double)b[i] - ax) * (double)L.dinv[i];
+      const double dn = (step == 0 ? 0.0 : c1 * (double)L.d[i]) + c2 * r;
+      L.d[i] = (T)dn;
+      xout[i] = (T)((ZERO ? 0.0 : (double)xin[i]) + dn);
+    }
+  }
+}
+
+template <class T>
+__device__ void fused_smooth(const CoopLevel<T>& L, const T* b, T* x, bool zero_start, int degree, long long tid,
+                             long long nthr, unsigned int* bar, int* status) {
+  const int steps = degree < 1 ? 1 : degree;
+  T* cur = x;
+  int step = 0;
+  if (zero_start) {
+    T* out = (steps % 2 == 1) ? x : L.t;
+    fused_cheb_rows<T, true>(L, b, nullptr, out, 0, tid, nthr);
+    grid_barrier(bar, status);
+    cur = out;
+    step = 1;
+  }
+  for (; step < steps; ++step) {
+    T* out = (cur == x) ? L.t : x;
+    fused_cheb_rows<T, false>(L, b, cur, out, step, tid, nthr);
+    grid_barrier(bar, status);
+    cur = out;
+  }
+  if (cur != x) {
+    for (long long i = tid; i < L.n; i += nthr) x[i] = cur[i];
+    grid_barrier(bar, status);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) amg_fused_cycle_kernel(const CoopLevel<T>* __restrict__ lv, int nlev,
+                                                              int degree, int nco, const double* __restrict__ co_inv,
+                                                              T* co_b, T* co_x, const T* b_top, T* x_top,
+                                                              unsigned int* bar, int* status) {
+  const long long nthr = (long long)gridDim.x * blockDim.x;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (int j = 0; j < nlev; ++j) {
+    const CoopLevel<T> L = lv[j];
+    const T* b = j == 0 ? b_top : L.b;
+    T* x = j == 0 ? x_top : L.x;
+    fused_smooth(L, b, x, true, degree, tid, nthr, bar, status);
+    // residual restricted to the next level
+    T* bc = j + 1 < nlev ? lv[j + 1].b : co_b;
+    const int nn = j + 1 < nlev ? lv[j + 1].n : nco;
+    const long long total = ((long long)nn * L.lanes + 31) / 32 * 32;
+    for (long long t = tid; t < total; t += nthr) {
+      const long long I = t / L.lanes;
+      const int sub = (int)(t % L.lanes);
+      double sres = 0.0;
+      if (I < nn)
+        for (int m = L.cptr[I]; m < L.cptr[I + 1]; ++m) {
+          const int i = L.cmem[m];
+          if (sub == 0) sres += (double)b[i];
+          for (int k = L.rp[i] + sub; k < L.rp[i + 1]; k += L.lanes) sres -= (double)L.val[k] * (double)x[L.ci[k]];
+        }
+      sres = group_sum_rt(sres, L.lanes);
+      if (I < nn && sub == 0) bc[I] = (T)sres;
+    }
+    grid_barrier(bar, status);
+  }
+  // dense coarsest solve: one warp per row
+  {
+    const long long lane = tid & 31, nwarp = nthr >> 5;
+    for (long long row = tid >> 5; row < nco; row += nwarp) {
+      double sv = 0.0;
+      for (long long jj = lane; jj < nco; jj += 32) sv += co_inv[row * nco + jj] * (double)co_b[jj];
+      sv = warp_sum(sv);
+      if (lane == 0) co_x[row] = (T)sv;
+    }
+    grid_barrier(bar, status);
+  }
+  for (int j = nlev - 1; j >= 0; --j) {
+    const CoopLevel<T> L = lv[j];
+    const T* b = j == 0 ? b_top : L.b;
+    T* x = j == 0 ? x_top : L.x;
+    const T* xc = j + 1 < nlev ? lv[j + 1].x : co_x;
+    for (long long i = tid; i < L.n; i += nthr) x[i] = (T)((double)x[i] + (double)xc[L.agg[i]]);
+    grid_barrier(bar, status);
+    fused_smooth(L, b, x, false, degree, tid, nthr, bar, status);
+  }
 }
 
 // K-cycle pieces ------------------------------------------------------------
@@ -560,11 +719,13 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
   co_x_.resize(nco_);
   co_b_.resize(nco_);
   bits_.resize(std::max<size_t>(levels_.size(), 1));
+  build_fused(s);
   PMB_CUDA(cudaStreamSynchronize(s));
 }
 
 template <class T>
 void AMG<T>::refresh(cudaStream_t s, int* d_status) {
+  coop_status_ = d_status;
   for (size_t l = 0; l < levels_.size(); ++l) {
     AMGLevel<T>& L = levels_[l];
     PMB_CUDA(cudaMemsetAsync(bits_.get() + l, 0, sizeof(unsigned long long), s));
@@ -619,8 +780,89 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
   }
 }
 
+constexpr int kFusedMaxRows = 65536;
+
+template <class T>
+void AMG<T>::build_fused(cudaStream_t s) {
+  coop_start_ = -1;
+  static const bool disabled = [] {
+    const char* e = std::getenv("PMB_NO_FUSED_COARSE");
+    return e && e[0] == '1';
+  }();
+  if (!fused_coarse || disabled) return;
+  const int L = (int)levels_.size();
+  for (int l = std::max(0, k_levels); l < L; ++l)
+    if (levels_[l].n <= kFusedMaxRows) {
+      coop_start_ = l;
+      break;
+    }
+  if (coop_start_ < 0) return;
+  std::vector<CoopLevel<T>> h;
+  for (int l = coop_start_; l < L; ++l) {
+    AMGLevel<T>& V = levels_[l];
+    CoopLevel<T> c;
+    c.n = V.n;
+    c.lanes = V.lanes;
+    c.rp = V.row_ptr;
+    c.ci = V.col;
+    c.val = V.val.get();
+    c.dinv = V.dinv.get();
+    c.lmax = V.lmax.get();
+    c.x = V.x.get();
+    c.b = V.b.get();
+    c.d = V.r.get();
+    c.t = V.t.get();
+    c.cptr = V.cptr.get();
+    c.cmem = V.cmem.get();
+    c.agg = V.agg.get();
+    h.push_back(c);
+  }
+  coop_levels_.resize(sizeof(CoopLevel<T>) * h.size());
+  PMB_CUDA(cudaMemcpyAsync(coop_levels_.get(), h.data(), sizeof(CoopLevel<T>) * h.size(), cudaMemcpyHostToDevice, s));
+  coop_bar_.resize(2);
+  coop_bar_.zero(s);
+  int dev = 0, sms = 0, per_sm = 0;
+  PMB_CUDA(cudaGetDevice(&dev));
+  PMB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  PMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, amg_fused_cycle_kernel<T>, 256, 0));
+  coop_grid_ = std::min(per_sm, 4) * sms;
+  if (coop_grid_ < 1) coop_start_ = -1;
+}
+
+template <class T>
+void AMG<T>::launch_fused(const T* b, T* x, cudaStream_t s) {
+  PMB_REQUIRE(coop_status_ != nullptr, "AMG refresh must run before a cycle");
+  PMB_CUDA(cudaMemsetAsync(coop_bar_.get(), 0, 2 * sizeof(unsigned int), s));
+  const CoopLevel<T>* lv = reinterpret_cast<const CoopLevel<T>*>(coop_levels_.get());
+  int nlev = (int)levels_.size() - coop_start_;
+  int deg = degree;
+  int nco = nco_;
+  const double* inv = co_inv_.get();
+  T* cob = co_b_.get();
+  T* cox = co_x_.get();
+  unsigned int* bar = coop_bar_.get();
+  int* st = coop_status_;
+  // cooperative: every block resident at once, which the grid barrier needs
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(coop_grid_);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  PMB_CUDA(cudaLaunchKernelEx(&cfg, amg_fused_cycle_kernel<T>, lv, nlev, deg, nco, inv, cob, cox, b, x, bar, st));
+  PMB_CHECK_LAUNCH();
+}
+
 template <class T>
 void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
+  if (coop_start_ >= 0 && l == coop_start_) {
+    launch_fused(b, x, s);
+    return;
+  }
   if (l == (int)levels_.size()) {
     dense_apply_kernel<T><<<grid_for(32LL * nco_, 256), 256, 0, s>>>(nco_, co_inv_.get(), b, x);
     PMB_CHECK_LAUNCH();

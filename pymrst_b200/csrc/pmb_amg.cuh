@@ -43,6 +43,24 @@ struct AMGLevel {
   DArray<double> lmax;  // Chebyshev upper bound (device scalar)
 };
 
+// One level as seen by the fused coarse-cycle kernel.
+template <class T>
+struct CoopLevel {
+  int n, lanes;
+  const int* rp;
+  const int* ci;
+  const T* val;
+  const T* dinv;
+  const double* lmax;
+  T* x;
+  T* b;
+  T* d;  // Chebyshev direction
+  T* t;  // ping-pong partner of x
+  const int* cptr;
+  const int* cmem;
+  const int* agg;
+};
+
 template <class T>
 class AMG {
  public:
@@ -63,8 +81,18 @@ class AMG {
   int num_levels() const { return (int)levels_.size() + (nco_ > 0 ? 1 : 0); }
   int level_size(int l) const { return l < (int)levels_.size() ? levels_[l].n : nco_; }
   int degree = 2;
+  // Run the levels below the K-cycle levels, down to the dense coarsest
+  // solve, as one cooperative kernel when they are small (set before build).
+  bool fused_coarse = true;
+  int fused_first_level() const { return coop_start_; }
 
  private:
+  int coop_start_ = -1, coop_grid_ = 0;
+  DArray<unsigned char> coop_levels_;
+  DArray<unsigned int> coop_bar_;  // grid barrier: arrivals, generation
+  int* coop_status_ = nullptr;
+  void build_fused(cudaStream_t s);
+  void launch_fused(const T* b, T* x, cudaStream_t s);
   void cycle(int l, const T* b, T* x, cudaStream_t s);
   void coarse_correction(int l, const T* rc, T* ec, cudaStream_t s);
   void smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start);
