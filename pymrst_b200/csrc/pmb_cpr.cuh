@@ -14,8 +14,8 @@ class CPRSolver {
   // Returns true when converged; info = [iterations, relres, ok, setups].
   bool solve(const double* b, double* x, double* info);
   const pmb_cpr_opts& opts() const { return o_; }
-  int num_levels() const { return amg_.num_levels(); }
-  int level_size(int l) const { return amg_.level_size(l); }
+  int num_levels() const { return f32_ ? amg32_.num_levels() : amg_.num_levels(); }
+  int level_size(int l) const { return f32_ ? amg32_.level_size(l) : amg_.level_size(l); }
   long long setups() const { return setups_; }
   long long total_iterations() const { return total_its_; }
   // Mean milliseconds of one application of a preconditioner stage (0: the
