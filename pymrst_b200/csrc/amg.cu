@@ -413,15 +413,15 @@ __global__ void dense_apply_kernel(int n, const double* __restrict__ Inv, const 
   if (lane == 0) x[row] = (T)s;
 }
 
-// Fused coarse cycle ---------------------------------------------------------
+// Fused coarse cycle (opt-in) ----------------------------------------------
 //
 // The V-cycle from level `first` down to the dense coarsest solve in one
 // cooperative launch, the steps separated by a grid barrier: the same
 // arithmetic, row grouping and buffer order as the per-step kernels, so the
-// result is identical; what goes is one launch per step on levels of a few
-// thousand rows, where launch latency is the whole cost.
+// result is the same; what goes is one launch per step on levels of a few
+// thousand rows.
 
-constexpr long long kBarrierSpins = 1LL << 24;  // with 64 ns sleeps: about a second
+constexpr long long kBarrierSpins = 1LL << 25;  // polls of an L2 line: a second or so
 
 // Grid barrier for a cooperative launch.  Bounded: a block that waits too
 // long records PMB_ERR_INTERNAL in *status and goes on; once the status is
@@ -446,7 +446,6 @@ __device__ __forceinline__ void grid_barrier(unsigned int* bar, int* status) {
             atomicExch(status, PMB_ERR_INTERNAL);
             break;
           }
-          __nanosleep(64);
         }
       }
       __threadfence();
@@ -785,11 +784,15 @@ constexpr int kFusedMaxRows = 65536;
 template <class T>
 void AMG<T>::build_fused(cudaStream_t s) {
   coop_start_ = -1;
-  static const bool disabled = [] {
-    const char* e = std::getenv("PMB_NO_FUSED_COARSE");
+  // Off unless PMB_FUSED_COARSE=1: measured on the channelised model (528,000
+  // cells, mixed precision) the fused cycle made a step 26% slower than the
+  // per-step kernels replayed from the preconditioner's CUDA graph, with 1, 2
+  // or 4 blocks per SM, although it launched 2.4x fewer kernels.
+  static const bool enabled = [] {
+    const char* e = std::getenv("PMB_FUSED_COARSE");
     return e && e[0] == '1';
   }();
-  if (!fused_coarse || disabled) return;
+  if (!fused_coarse || !enabled) return;
   const int L = (int)levels_.size();
   for (int l = std::max(0, k_levels); l < L; ++l)
     if (levels_[l].n <= kFusedMaxRows) {
@@ -825,7 +828,12 @@ void AMG<T>::build_fused(cudaStream_t s) {
   PMB_CUDA(cudaGetDevice(&dev));
   PMB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   PMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, amg_fused_cycle_kernel<T>, 256, 0));
-  coop_grid_ = std::min(per_sm, 4) * sms;
+  static const int blocks_per_sm = [] {
+    const char* e = std::getenv("PMB_FUSED_BLOCKS_PER_SM");
+    const int v = e ? std::atoi(e) : 1;
+    return v < 1 ? 1 : v;
+  }();
+  coop_grid_ = std::min(per_sm, blocks_per_sm) * sms;
   if (coop_grid_ < 1) coop_start_ = -1;
 }
 

@@ -453,12 +453,46 @@ __global__ void __launch_bounds__(32 * kLineWarps) line_gs_kernel(OWView v, int 
 // line's length; shared memory 144 B per thread.
 constexpr int kPcrMaxLen = 256;
 
-__device__ __forceinline__ double4 add4(double4 a, double4 b) {
-  return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+// 2x2 block (row-major) and 2-vector in the arithmetic type of the line solve.
+template <class CT>
+struct alignas(4 * sizeof(CT)) Blk2 {
+  CT x, y, z, w;
+};
+template <class CT>
+struct alignas(2 * sizeof(CT)) Vec2 {
+  CT x, y;
+};
+template <class CT>
+__device__ __forceinline__ Blk2<CT> blk_of(double4 a) {
+  return Blk2<CT>{(CT)a.x, (CT)a.y, (CT)a.z, (CT)a.w};
 }
-__device__ __forceinline__ double4 neg4(double4 a) { return make_double4(-a.x, -a.y, -a.z, -a.w); }
+template <class CT>
+__device__ __forceinline__ Blk2<CT> bmul(Blk2<CT> a, Blk2<CT> b) {
+  return Blk2<CT>{a.x * b.x + a.y * b.z, a.x * b.y + a.y * b.w, a.z * b.x + a.w * b.z, a.z * b.y + a.w * b.w};
+}
+template <class CT>
+__device__ __forceinline__ Vec2<CT> bmv(Blk2<CT> a, Vec2<CT> v) {
+  return Vec2<CT>{a.x * v.x + a.y * v.y, a.z * v.x + a.w * v.y};
+}
+template <class CT>
+__device__ __forceinline__ Blk2<CT> badd(Blk2<CT> a, Blk2<CT> b) {
+  return Blk2<CT>{a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w};
+}
+template <class CT>
+__device__ __forceinline__ Blk2<CT> bneg(Blk2<CT> a) {
+  return Blk2<CT>{-a.x, -a.y, -a.z, -a.w};
+}
+template <class CT>
+__device__ __forceinline__ Blk2<CT> binv(Blk2<CT> D, bool& ok) {
+  const CT det = D.x * D.w - D.y * D.z;
+  ok = det != CT(0) && isfinite(det);
+  const CT id = ok ? CT(1) / det : CT(0);
+  return Blk2<CT>{id * D.w, -id * D.y, -id * D.z, id * D.x};
+}
 
-template <class BT>
+// CT is the arithmetic of the cyclic reduction: double, or float when the
+// smoother blocks are FP32 (mixed precision); the residual is formed in FP64.
+template <class BT, class CT>
 __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lstart, const int* __restrict__ clines,
                                                               const int* __restrict__ lptr,
                                                               const int* __restrict__ lcells,
@@ -468,13 +502,12 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
                                                               const double* __restrict__ wj,
                                                               const double* __restrict__ r, double* __restrict__ z,
                                                               int* status) {
-  extern __shared__ double4 pcr_sm[];
+  extern __shared__ __align__(16) unsigned char pcr_raw[];
   const int nb = blockDim.x;
-  double4* sD = pcr_sm;
-  double4* sL = pcr_sm + nb;
-  double4* sU = pcr_sm + 2 * nb;
-  double4* sI = pcr_sm + 3 * nb;
-  double2* sY = reinterpret_cast<double2*>(pcr_sm + 4 * nb);
+  Blk2<CT>* sL = reinterpret_cast<Blk2<CT>*>(pcr_raw);
+  Blk2<CT>* sU = sL + nb;
+  Blk2<CT>* sI = sL + 2 * nb;
+  Vec2<CT>* sY = reinterpret_cast<Vec2<CT>*>(sL + 3 * nb);
   __shared__ int sBad;
   const int line = clines[lstart + blockIdx.x];
   const int t0 = lptr[line];
@@ -482,10 +515,10 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
   const int u = threadIdx.x;
   const bool act = u < len;
   if (u == 0) sBad = 0;
-  const double4 zero4 = make_double4(0, 0, 0, 0);
+  const Blk2<CT> zero = {CT(0), CT(0), CT(0), CT(0)};
   const double2* z2 = reinterpret_cast<const double2*>(z);
-  double4 D = make_double4(1, 0, 0, 1), Lb = zero4, Ub = zero4;
-  double2 y = make_double2(0, 0);
+  Blk2<CT> D = {CT(1), CT(0), CT(0), CT(1)}, Lb = zero, Ub = zero;
+  Vec2<CT> y = {CT(0), CT(0)};
   int c = 0;
   if (act) {
     const int t = t0 + u;
@@ -494,9 +527,9 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
     // the line blocks first, so that their loads overlap the row gather
     const int kl = u > 0 ? llo[t] : -1;
     const int ku = u + 1 < len ? lup[t] : -1;
-    D = ld4(A[v.diag_pos[c]]);
-    if (kl >= 0) Lb = ld4(A[kl]);
-    if (ku >= 0) Ub = ld4(A[ku]);
+    D = blk_of<CT>(ld4(A[v.diag_pos[c]]));
+    if (kl >= 0) Lb = blk_of<CT>(ld4(A[kl]));
+    if (ku >= 0) Ub = blk_of<CT>(ld4(A[ku]));
     sub_row(v.col, A, z2, v.row_ptr[c], v.row_ptr[c + 1], rc);
     const int q = v.cell_pc[c];
     if (q >= 0) {
@@ -509,14 +542,13 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
         rc.y -= B[3] * zw[3 * kw] + B[4] * zw[3 * kw + 1] + B[5] * zw[3 * kw + 2];
       }
     }
-    y = rc;
+    y = Vec2<CT>{(CT)rc.x, (CT)rc.y};
   }
   for (int s = 1; s < len; s <<= 1) {
     bool ok = true;
-    const double4 I = inv2(D, ok);
+    const Blk2<CT> I = binv(D, ok);
     if (act && !ok) sBad = 1;
     if (act) {
-      sD[u] = D;
       sL[u] = Lb;
       sU[u] = Ub;
       sI[u] = I;
@@ -525,21 +557,21 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
     __syncthreads();
     if (sBad) break;  // uniform: read after the barrier by every thread
     if (act) {
-      double4 nD = D, nL = zero4, nU = zero4;
-      double2 ny = y;
+      Blk2<CT> nD = D, nL = zero, nU = zero;
+      Vec2<CT> ny = y;
       if (u - s >= 0) {
-        const double4 a = neg4(mul2(Lb, sI[u - s]));
-        nD = add4(nD, mul2(a, sU[u - s]));
-        nL = mul2(a, sL[u - s]);
-        const double2 q = mv2(a, sY[u - s]);
+        const Blk2<CT> a = bneg(bmul(Lb, sI[u - s]));
+        nD = badd(nD, bmul(a, sU[u - s]));
+        nL = bmul(a, sL[u - s]);
+        const Vec2<CT> q = bmv(a, sY[u - s]);
         ny.x += q.x;
         ny.y += q.y;
       }
       if (u + s < len) {
-        const double4 g = neg4(mul2(Ub, sI[u + s]));
-        nD = add4(nD, mul2(g, sL[u + s]));
-        nU = mul2(g, sU[u + s]);
-        const double2 q = mv2(g, sY[u + s]);
+        const Blk2<CT> g = bneg(bmul(Ub, sI[u + s]));
+        nD = badd(nD, bmul(g, sL[u + s]));
+        nU = bmul(g, sU[u + s]);
+        const Vec2<CT> q = bmv(g, sY[u + s]);
         ny.x += q.x;
         ny.y += q.y;
       }
@@ -556,15 +588,15 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
   }
   if (!act) return;
   bool ok = true;
-  const double4 I = inv2(D, ok);
+  const Blk2<CT> I = binv(D, ok);
   if (!ok) {
     atomicExch(status, PMB_ERR_PIVOT);
     return;
   }
-  const double2 x = mv2(I, y);
+  const Vec2<CT> x = bmv(I, y);
   double2 zc = z2[c];
-  zc.x += x.x;
-  zc.y += x.y;
+  zc.x += (double)x.x;
+  zc.y += (double)x.y;
   reinterpret_cast<double2*>(z)[c] = zc;
 }
 
@@ -792,16 +824,17 @@ void CPRSolver::local_stage(const double* r, double* z) {
         if (cnt <= 0) continue;
         if (Ls.max_len <= kPcrMaxLen) {
           const int nb = std::max(32, (Ls.max_len + 31) / 32 * 32);
-          const size_t smem = (size_t)nb * (4 * sizeof(double4) + sizeof(double2));
           if (f32_)
-            line_pcr_kernel<<<cnt, nb, smem, s_>>>(v, Ls.h_color_ptr[q], Ls.color_lines.get(), Ls.line_ptr.get(),
+            line_pcr_kernel<float4, float><<<cnt, nb, (size_t)nb * (3 * sizeof(Blk2<float>) + sizeof(Vec2<float>)),
+                                             s_>>>(v, Ls.h_color_ptr[q], Ls.color_lines.get(), Ls.line_ptr.get(),
                                                    Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(),
                                                    reinterpret_cast<const float4*>(jac32_.get()), well_, r, z,
                                                    status_.get());
           else
-            line_pcr_kernel<<<cnt, nb, smem, s_>>>(v, Ls.h_color_ptr[q], Ls.color_lines.get(), Ls.line_ptr.get(),
-                                                   Ls.line_cells.get(), Ls.line_lo.get(), Ls.line_up.get(), A, well_,
-                                                   r, z, status_.get());
+            line_pcr_kernel<double4, double>
+                <<<cnt, nb, (size_t)nb * (3 * sizeof(Blk2<double>) + sizeof(Vec2<double>)), s_>>>(
+                    v, Ls.h_color_ptr[q], Ls.color_lines.get(), Ls.line_ptr.get(), Ls.line_cells.get(),
+                    Ls.line_lo.get(), Ls.line_up.get(), A, well_, r, z, status_.get());
           PMB_CHECK_LAUNCH();
           continue;
         }

@@ -82,7 +82,8 @@ class AMG {
   int level_size(int l) const { return l < (int)levels_.size() ? levels_[l].n : nco_; }
   int degree = 2;
   // Run the levels below the K-cycle levels, down to the dense coarsest
-  // solve, as one cooperative kernel when they are small (set before build).
+  // solve, as one cooperative kernel when they are small (set before build;
+  // also needs PMB_FUSED_COARSE=1 in the environment).
   bool fused_coarse = true;
   int fused_first_level() const { return coop_start_; }
 

@@ -1,6 +1,6 @@
-"""The fused coarse AMG cycle (one cooperative launch for the levels below
-the K-cycle levels) against the per-step kernels: the same Newton step run in
-two processes, with PMB_NO_FUSED_COARSE=1 in one, gives the same iteration
+"""The opt-in fused coarse AMG cycle (one cooperative launch for the levels
+below the K-cycle levels, PMB_FUSED_COARSE=1) against the default per-step
+kernels: the same Newton step run in two processes gives the same iteration
 counts and states to roundoff, with far fewer kernel launches."""
 
 import json
@@ -26,7 +26,7 @@ import numpy as np
 sys.path.insert(0, sys.argv[1])
 from pymrst_b200 import cases, _native as N
 from pymrst_b200.ow_model import GpuOilWaterModel
-case = cases.five_spot(dims=(48, 48, 6), nsteps=2)
+case = cases.five_spot(dims=(48, 48, 6))
 m = GpuOilWaterModel(case.grid, case.rock, case.fluid, case.wells, gravity=case.gravity,
                      cpr_options=dict(amg_cycle=1, rtol=1e-10, maxiter=400))
 st = m.initial_state(case.p0, case.sw0)
@@ -39,12 +39,12 @@ print(json.dumps({"ok": bool(ok), "its": int(its), "krylov": float(m.last_stats[
 """
 
 
-def _run(tmp_path, disable):
+def _run(tmp_path, fused):
     env = dict(os.environ)
-    env.pop("PMB_NO_FUSED_COARSE", None)
-    if disable:
-        env["PMB_NO_FUSED_COARSE"] = "1"
-    out = tmp_path / f"state_{int(disable)}.npy"
+    env.pop("PMB_FUSED_COARSE", None)
+    if fused:
+        env["PMB_FUSED_COARSE"] = "1"
+    out = tmp_path / f"state_{int(fused)}.npy"
     r = subprocess.run([sys.executable, "-c", SNIPPET, str(ROOT), str(out)], env=env, capture_output=True,
                        text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
@@ -52,8 +52,8 @@ def _run(tmp_path, disable):
 
 
 def test_fused_coarse_cycle_matches_the_per_step_kernels(tmp_path):
-    fused, xf = _run(tmp_path, False)
-    plain, xp = _run(tmp_path, True)
+    fused, xf = _run(tmp_path, True)
+    plain, xp = _run(tmp_path, False)
     assert fused["ok"] and plain["ok"]
     assert len(fused["levels"]) >= 3  # levels below the K-cycle level exist, so the fused path ran
     assert fused["its"] == plain["its"] and fused["krylov"] == plain["krylov"]
