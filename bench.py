@@ -42,6 +42,9 @@ WORKLOAD = dict(name="channelised oil-water 60x220x85 (1,122,000 cells), 10-day 
 # reference's default linear solver.  A smaller sample favours the CPU
 # (direct-solve cost grows faster than linearly).
 CPU_SAMPLE = dict(dims=(18, 66, 25), cell_size=(6.1 * 60 / 18, 3.05 * 220 / 66, 0.61 * 85 / 25))
+# DRAM bytes per swept cell of one line_pcr_kernel launch, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the 60x220x60 model.
+PCR_DRAM_BYTES_PER_CELL = {"fp64": (190039296 + 8392448) / 396000.0}
 
 
 def parse():
@@ -388,6 +391,11 @@ def run_ours(args):
     peak, peak_kind = peaks()
     dom = kr["line_gs_sweep"]
     ach = dom["bytes"] / dom["seconds"] / 1e9
+    # DRAM traffic of one line_pcr_kernel launch (one colour, half the cells),
+    # scaled from the ncu capture of dram__bytes_read.sum + dram__bytes_write.sum
+    # on the 60x220x60 model (396,000 cells per colour)
+    traffic = PCR_DRAM_BYTES_PER_CELL.get(args.precision)
+    traffic = traffic * model.nc / 2 if traffic else None
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -407,9 +415,10 @@ def run_ours(args):
                     "d2h_bytes_per_step": nvec_bytes},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm",
-                         "kernel": "line_gs_kernel (one sweep = two colour launches; per-launch figures are half)",
+                         "kernel": "line_pcr_kernel (vertical-line block Gauss-Seidel, one colour per launch)",
                          "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                         "peak_kind": peak_kind, "traffic": None,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes": dom["bytes"] / 2,
                          "kernels": {k: {"ms": v["seconds"] * 1e3, "bytes": v["bytes"],
                                          "GBps": (v["bytes"] / v["seconds"] / 1e9) if v["bytes"] else None}
                                      for k, v in kr.items()}},
