@@ -44,7 +44,8 @@ WORKLOAD = dict(name="channelised oil-water 60x220x85 (1,122,000 cells), 10-day 
 CPU_SAMPLE = dict(dims=(18, 66, 25), cell_size=(6.1 * 60 / 18, 3.05 * 220 / 66, 0.61 * 85 / 25))
 # DRAM bytes per swept cell of one line_pcr_kernel launch, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the 60x220x60 model.
-PCR_DRAM_BYTES_PER_CELL = {"fp64": (190039296 + 8392448) / 396000.0}
+PCR_DRAM_BYTES_PER_CELL = {"fp64": (190039296 + 8392448) / 396000.0,
+                           "mixed": (150901760 + 7420416) / 396000.0}
 
 
 def parse():

@@ -278,6 +278,7 @@ __global__ void __launch_bounds__(256) cheb_step_kernel(int n, const int* __rest
                                                         const T* __restrict__ b, const T* __restrict__ xin,
                                                         T* __restrict__ xout, T* __restrict__ d, const double* lmax,
                                                         int step) {
+  pdl_enter();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long i = t / LANES;
   const int sub = (int)(t % LANES);
@@ -304,6 +305,7 @@ __global__ void __launch_bounds__(256) restrict_residual_kernel(int nc, const in
                                                                 const int* __restrict__ rp, const int* __restrict__ ci,
                                                                 const T* __restrict__ a, const T* __restrict__ b,
                                                                 const T* __restrict__ x, T* __restrict__ bc) {
+  pdl_enter();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long I = t / LANES;
   const int sub = (int)(t % LANES);
@@ -321,6 +323,7 @@ __global__ void __launch_bounds__(256) restrict_residual_kernel(int nc, const in
 template <class T>
 __global__ void prolong_add_kernel(int n, const int* __restrict__ agg, const T* __restrict__ xc,
                                    T* __restrict__ x) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   x[i] = (T)((double)x[i] + (double)xc[agg[i]]);
@@ -328,6 +331,7 @@ __global__ void prolong_add_kernel(int n, const int* __restrict__ agg, const T* 
 
 template <class T>
 __global__ void copy_kernel(int n, const T* __restrict__ a, T* __restrict__ b) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = a[i];
 }
@@ -404,6 +408,7 @@ __global__ void __launch_bounds__(512) gauss_jordan_kernel(int n, double* __rest
 template <class T>
 __global__ void dense_apply_kernel(int n, const double* __restrict__ Inv, const T* __restrict__ b,
                                    T* __restrict__ x) {
+  pdl_enter();
   const int lane = threadIdx.x & 31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= n) return;
@@ -569,6 +574,7 @@ template <class T, int LANES>
 __global__ void __launch_bounds__(256) csr_spmv_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                                                        const T* __restrict__ a, const T* __restrict__ x,
                                                        T* __restrict__ y) {
+  pdl_enter();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long i = t / LANES;
   const int sub = (int)(t % LANES);
@@ -583,6 +589,7 @@ __global__ void __launch_bounds__(256) csr_spmv_kernel(int n, const int* __restr
 template <class T, int NDOT>
 __global__ void __launch_bounds__(256) kdots_kernel(int n, const T* __restrict__ v1, const T* __restrict__ v2,
                                                     const T* __restrict__ rc, double* __restrict__ part) {
+  pdl_enter();
   __shared__ double sh[32];
   double d[NDOT];
   for (int q = 0; q < NDOT; ++q) d[q] = 0.0;
@@ -610,6 +617,7 @@ __global__ void __launch_bounds__(256) kdots_kernel(int n, const T* __restrict__
 // [coef[1], coef[2]] minimising |rc - y0 v1 - y1 v2|.  One warp sums each
 // dot's G block partials; launched with 5 warps.
 __global__ void kcoef_kernel(int G, int mode, const double* __restrict__ part, double* __restrict__ coef) {
+  pdl_enter();
   __shared__ double d[5];
   const int nd = mode == 0 ? 2 : 5;
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
@@ -640,6 +648,7 @@ __global__ void kcoef_kernel(int G, int mode, const double* __restrict__ part, d
 template <class T>
 __global__ void kaxpy_kernel(int n, const T* __restrict__ a, const T* __restrict__ b, const double* __restrict__ coef,
                              T* __restrict__ out) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (T)((double)a[i] - coef[0] * (double)b[i]);
 }
@@ -648,6 +657,7 @@ __global__ void kaxpy_kernel(int n, const T* __restrict__ a, const T* __restrict
 template <class T>
 __global__ void kcombine_kernel(int n, const T* __restrict__ c1, const T* __restrict__ c2,
                                 const double* __restrict__ coef, T* __restrict__ out) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (T)(coef[1] * (double)c1[i] + coef[2] * (double)c2[i]);
 }
@@ -759,23 +769,20 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
     const int g = grid_for((long long)L.n * LN, 256);
     if (zero_start) {
       T* out = (steps % 2 == 1) ? x : t;
-      cheb_step_kernel<T, true, LN><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, nullptr,
-                                                      out, L.r.get(), L.lmax.get(), 0);
-      PMB_CHECK_LAUNCH();
+      launch_pdl(cheb_step_kernel<T, true, LN>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
+                 (const T*)L.dinv.get(), b, (const T*)nullptr, out, L.r.get(), (const double*)L.lmax.get(), 0);
       cur = out;
       step = 1;
     }
     for (; step < steps; ++step) {
       T* out = (cur == x) ? t : x;
-      cheb_step_kernel<T, false, LN><<<g, 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(), b, cur,
-                                                       out, L.r.get(), L.lmax.get(), step);
-      PMB_CHECK_LAUNCH();
+      launch_pdl(cheb_step_kernel<T, false, LN>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
+                 (const T*)L.dinv.get(), b, (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step);
       cur = out;
     }
   });
   if (cur != x) {
-    copy_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, cur, x);
-    PMB_CHECK_LAUNCH();
+    launch_pdl(copy_kernel<T>, grid_for(L.n, 256), 256, 0, s, L.n, (const T*)cur, x);
   }
 }
 
@@ -872,8 +879,8 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
     return;
   }
   if (l == (int)levels_.size()) {
-    dense_apply_kernel<T><<<grid_for(32LL * nco_, 256), 256, 0, s>>>(nco_, co_inv_.get(), b, x);
-    PMB_CHECK_LAUNCH();
+    launch_pdl(dense_apply_kernel<T>, grid_for(32LL * nco_, 256), 256, 0, s, nco_, (const double*)co_inv_.get(), b,
+               x);
     return;
   }
   AMGLevel<T>& L = levels_[l];
@@ -884,13 +891,12 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
   smooth(L, b, x, s, true);
   with_lanes(L.lanes, [&](auto ln) {
     constexpr int LN = decltype(ln)::value;
-    restrict_residual_kernel<T, LN><<<grid_for((long long)nc * LN, 256), 256, 0, s>>>(
-        nc, L.cptr.get(), L.cmem.get(), L.row_ptr, L.col, L.val.get(), b, x, bc);
-    PMB_CHECK_LAUNCH();
+    launch_pdl(restrict_residual_kernel<T, LN>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
+               (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
+               (const T*)x, bc);
   });
   coarse_correction(l, bc, xc, s);
-  prolong_add_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.agg.get(), xc, x);
-  PMB_CHECK_LAUNCH();
+  launch_pdl(prolong_add_kernel<T>, grid_for(L.n, 256), 256, 0, s, L.n, (const int*)L.agg.get(), (const T*)xc, x);
   smooth(L, b, x, s, false);
 }
 
@@ -911,29 +917,24 @@ void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
   cycle(l + 1, rc, C.kc1.get(), s);
   with_lanes(C.lanes, [&](auto ln) {
     constexpr int LN = decltype(ln)::value;
-    csr_spmv_kernel<T, LN><<<grid_for((long long)n * LN, 256), 256, 0, s>>>(n, C.row_ptr, C.col, C.val.get(),
-                                                                            C.kc1.get(), C.kv1.get());
-    PMB_CHECK_LAUNCH();
+    launch_pdl(csr_spmv_kernel<T, LN>, grid_for((long long)n * LN, 256), 256, 0, s, n, C.row_ptr, C.col,
+               (const T*)C.val.get(), (const T*)C.kc1.get(), C.kv1.get());
   });
-  kdots_kernel<T, 2><<<G, 256, 0, s>>>(n, C.kv1.get(), nullptr, rc, C.kpart.get());
-  PMB_CHECK_LAUNCH();
-  kcoef_kernel<<<1, 160, 0, s>>>(G, 0, C.kpart.get(), C.kcoef.get());
-  PMB_CHECK_LAUNCH();
-  kaxpy_kernel<T><<<g, 256, 0, s>>>(n, rc, C.kv1.get(), C.kcoef.get(), C.kr2.get());
-  PMB_CHECK_LAUNCH();
+  launch_pdl(kdots_kernel<T, 2>, G, 256, 0, s, n, (const T*)C.kv1.get(), (const T*)nullptr, rc, C.kpart.get());
+  launch_pdl(kcoef_kernel, 1, 160, 0, s, G, 0, (const double*)C.kpart.get(), C.kcoef.get());
+  launch_pdl(kaxpy_kernel<T>, g, 256, 0, s, n, rc, (const T*)C.kv1.get(), (const double*)C.kcoef.get(),
+             C.kr2.get());
   cycle(l + 1, C.kr2.get(), C.kc2.get(), s);
   with_lanes(C.lanes, [&](auto ln) {
     constexpr int LN = decltype(ln)::value;
-    csr_spmv_kernel<T, LN><<<grid_for((long long)n * LN, 256), 256, 0, s>>>(n, C.row_ptr, C.col, C.val.get(),
-                                                                            C.kc2.get(), C.kv2.get());
-    PMB_CHECK_LAUNCH();
+    launch_pdl(csr_spmv_kernel<T, LN>, grid_for((long long)n * LN, 256), 256, 0, s, n, C.row_ptr, C.col,
+               (const T*)C.val.get(), (const T*)C.kc2.get(), C.kv2.get());
   });
-  kdots_kernel<T, 5><<<G, 256, 0, s>>>(n, C.kv1.get(), C.kv2.get(), rc, C.kpart.get());
-  PMB_CHECK_LAUNCH();
-  kcoef_kernel<<<1, 160, 0, s>>>(G, 1, C.kpart.get(), C.kcoef.get());
-  PMB_CHECK_LAUNCH();
-  kcombine_kernel<T><<<g, 256, 0, s>>>(n, C.kc1.get(), C.kc2.get(), C.kcoef.get(), ec);
-  PMB_CHECK_LAUNCH();
+  launch_pdl(kdots_kernel<T, 5>, G, 256, 0, s, n, (const T*)C.kv1.get(), (const T*)C.kv2.get(), rc,
+             C.kpart.get());
+  launch_pdl(kcoef_kernel, 1, 160, 0, s, G, 1, (const double*)C.kpart.get(), C.kcoef.get());
+  launch_pdl(kcombine_kernel<T>, g, 256, 0, s, n, (const T*)C.kc1.get(), (const T*)C.kc2.get(),
+             (const double*)C.kcoef.get(), ec);
 }
 
 template <class T>

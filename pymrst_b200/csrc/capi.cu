@@ -14,6 +14,14 @@ namespace pmb {
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("PMB_NO_PDL");
+    return !(e && e[0] == '1');
+  }();
+  return on;
+}
+
 static std::atomic<long long> g_launches{0};
 void count_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(); }

@@ -147,6 +147,35 @@ class PinnedArray {
 
 constexpr int kNumSM = 148;
 
+// Programmatic dependent launch (sm_90+).  A kernel launched by launch_pdl
+// may be scheduled while its predecessor on the stream is still draining;
+// pdl_enter(), its first statement, waits until the predecessor grid has
+// completed and its memory is visible, then lets the successor be scheduled.
+// So only the launch latency overlaps, never the data.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+bool pdl_enabled();  // false when the environment has PMB_NO_PDL=1
+
+template <class... KArgs, class... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  PMB_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+  count_launch();
+  PMB_CUDA(cudaGetLastError());
+}
+
 inline int grid_for(long long n, int block) {
   long long g = (n + block - 1) / block;
   if (g < 1) g = 1;
