@@ -131,7 +131,7 @@ static void galerkin_values(const std::vector<int>& gptr, const std::vector<int>
 
 std::vector<AMGHostLevel> amg_build_hierarchy(int n, const int* row_ptr, const int* col,
                                               const double* val, double theta, int passes,
-                                              int coarse_size, int max_levels) {
+                                              int coarse_size, int max_levels, int aggressive_below) {
   std::vector<AMGHostLevel> out;
   HostCSR cur;
   cur.n = n;
@@ -143,14 +143,15 @@ std::vector<AMGHostLevel> amg_build_hierarchy(int n, const int* row_ptr, const i
     std::iota(agg.begin(), agg.end(), 0);
     int na = cur.n;
     HostCSR work = cur;
-    for (int p = 0; p < passes; ++p) {
+    const int level_passes = cur.n < aggressive_below ? passes + 1 : passes;
+    for (int p = 0; p < level_passes; ++p) {
       std::vector<int> a2;
       int na2 = pairwise_match(work.n, work.rp.data(), work.ci.data(), work.v.data(), theta, a2, false);
       if (na2 > 0.7 * work.n)
         na2 = pairwise_match(work.n, work.rp.data(), work.ci.data(), work.v.data(), 0.0, a2, true);
       for (int i = 0; i < cur.n; ++i) agg[i] = a2[agg[i]];
       na = na2;
-      if (p + 1 < passes) {
+      if (p + 1 < level_passes) {
         HostCSR next;
         std::vector<int> gp, gi, cp, cm;
         galerkin_structure(work.n, work.rp.data(), work.ci.data(), a2, na2, next.rp, next.ci, gp, gi, cp, cm);
@@ -670,7 +671,12 @@ template <class T>
 void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<int>& h_col,
                    const int* d_row_ptr, const int* d_col, const std::vector<double>& h_val,
                    double theta, int coarse_size, cudaStream_t s) {
-  auto H = amg_build_hierarchy(n, h_row_ptr.data(), h_col.data(), h_val.data(), theta, 2, coarse_size, 40);
+  static const int aggressive = [] {
+    const char* e = std::getenv("PMB_AMG_AGGRESSIVE_BELOW");
+    return e ? std::atoi(e) : 0;
+  }();
+  auto H = amg_build_hierarchy(n, h_row_ptr.data(), h_col.data(), h_val.data(), theta, 2, coarse_size, 40,
+                               aggressive);
   levels_.clear();
   levels_.resize(H.size() - 1);
   for (size_t l = 0; l + 1 < H.size(); ++l) {

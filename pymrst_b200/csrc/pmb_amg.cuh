@@ -24,10 +24,11 @@ struct AMGHostLevel {
 // Pairwise aggregation hierarchy from a CSR matrix (host).  `passes`
 // successive pairwise matchings form one level (aggregates of up to
 // 2^passes); a matching whose coarsening ratio is poor at threshold `theta`
-// is redone with theta = 0.  The last entry is the coarsest level (no agg).
+// is redone with theta = 0; levels with fewer than aggressive_below unknowns
+// take one pass more.  The last entry is the coarsest level (no agg).
 std::vector<AMGHostLevel> amg_build_hierarchy(int n, const int* row_ptr, const int* col,
                                               const double* val, double theta, int passes,
-                                              int coarse_size, int max_levels);
+                                              int coarse_size, int max_levels, int aggressive_below = 0);
 
 template <class T>
 struct AMGLevel {
