@@ -273,29 +273,43 @@ __device__ __forceinline__ void cheb_coeffs(double lm, int step, double& c1, dou
 // Chebyshev on D^{-1} A over [lmax/10, lmax]: step `step` of the
 // three-term recurrence; x_out = x_in + d, d = c1 d + c2 D^{-1}(b - A x_in).
 // LANES threads share a row.
-template <class T, bool ZERO, int LANES>
+// With PRO, x_in is first corrected by the coarse-level correction, read as
+// x_in[j] + xc[agg[j]] rounded to T exactly as prolong_add_kernel would store
+// it: the prolongation and the first post-smoothing step in one launch.
+template <class T, bool PRO>
+__device__ __forceinline__ double cheb_x(const T* __restrict__ xin, const int* __restrict__ agg,
+                                         const T* __restrict__ xc, int j) {
+  if (!PRO) return (double)xin[j];
+  return (double)(T)((double)xin[j] + (double)xc[agg[j]]);
+}
+
+template <class T, bool ZERO, int LANES, bool PRO = false>
 __global__ void __launch_bounds__(256) cheb_step_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                                                         const T* __restrict__ a, const T* __restrict__ dinv,
                                                         const T* __restrict__ b, const T* __restrict__ xin,
                                                         T* __restrict__ xout, T* __restrict__ d, const double* lmax,
-                                                        int step) {
+                                                        int step, const int* __restrict__ agg = nullptr,
+                                                        const T* __restrict__ xc = nullptr) {
   pdl_enter();
+  __shared__ double s_c[2];
+  if (threadIdx.x == 0) cheb_coeffs(lmax[0], step, s_c[0], s_c[1]);  // once per block
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long i = t / LANES;
   const int sub = (int)(t % LANES);
   double ax = 0.0;
   if (!ZERO) {
     if (i < n)
-      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) ax += (double)a[k] * (double)xin[ci[k]];
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES)
+        ax += (double)a[k] * cheb_x<T, PRO>(xin, agg, xc, ci[k]);
     ax = group_sum<LANES>(ax);
   }
+  __syncthreads();
   if (i >= n || sub != 0) return;
-  double c1, c2;
-  cheb_coeffs(lmax[0], step, c1, c2);
+  const double c1 = s_c[0], c2 = s_c[1];
   const double r = ((double)b[i] - ax) * (double)dinv[i];
   const double dn = (step == 0 ? 0.0 : c1 * (double)d[i]) + c2 * r;
   d[i] = (T)dn;
-  xout[i] = (T)((ZERO ? 0.0 : (double)xin[i]) + dn);
+  xout[i] = (T)((ZERO ? 0.0 : cheb_x<T, PRO>(xin, agg, xc, (int)i)) + dn);
 }
 
 // b_c[I] = sum over members i of (b_i - (A x)_i); LANES threads per aggregate
@@ -763,7 +777,7 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
 }
 
 template <class T>
-void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start) {
+void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start, const T* xc) {
   // degree steps ping-pong between x and L.t, ordered so that the last one
   // writes x; only an odd step count from a non-zero start needs a copy
   const int steps = std::max(1, degree);
@@ -776,14 +790,21 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
     if (zero_start) {
       T* out = (steps % 2 == 1) ? x : t;
       launch_pdl(cheb_step_kernel<T, true, LN>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
-                 (const T*)L.dinv.get(), b, (const T*)nullptr, out, L.r.get(), (const double*)L.lmax.get(), 0);
+                 (const T*)L.dinv.get(), b, (const T*)nullptr, out, L.r.get(), (const double*)L.lmax.get(), 0,
+                 (const int*)nullptr, (const T*)nullptr);
       cur = out;
       step = 1;
     }
     for (; step < steps; ++step) {
       T* out = (cur == x) ? t : x;
-      launch_pdl(cheb_step_kernel<T, false, LN>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
-                 (const T*)L.dinv.get(), b, (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step);
+      if (xc && step == 0)  // x + P xc, folded into the first step
+        launch_pdl(cheb_step_kernel<T, false, LN, true>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
+                   (const T*)L.dinv.get(), b, (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step,
+                   (const int*)L.agg.get(), xc);
+      else
+        launch_pdl(cheb_step_kernel<T, false, LN>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
+                   (const T*)L.dinv.get(), b, (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step,
+                   (const int*)nullptr, (const T*)nullptr);
       cur = out;
     }
   });
@@ -793,6 +814,10 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
 }
 
 constexpr int kFusedMaxRows = 65536;
+// Levels below this size fold the prolongation into the first post-smoothing
+// step (one launch less per visit); on larger levels the extra gathers of agg
+// and the correction cost more than the launch.
+constexpr int kFoldProlongRows = 200000;
 
 template <class T>
 void AMG<T>::build_fused(cudaStream_t s) {
@@ -902,8 +927,13 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
                (const T*)x, bc);
   });
   coarse_correction(l, bc, xc, s);
-  launch_pdl(prolong_add_kernel<T>, grid_for(L.n, 256), 256, 0, s, L.n, (const int*)L.agg.get(), (const T*)xc, x);
-  smooth(L, b, x, s, false);
+  if (L.n < kFoldProlongRows && degree >= 1) {
+    smooth(L, b, x, s, false, xc);  // prolongation folded into the first smoothing step
+  } else {
+    launch_pdl(prolong_add_kernel<T>, grid_for(L.n, 256), 256, 0, s, L.n, (const int*)L.agg.get(), (const T*)xc,
+               x);
+    smooth(L, b, x, s, false);
+  }
 }
 
 // Coarse correction of level l: a plain recursive cycle, or on the first

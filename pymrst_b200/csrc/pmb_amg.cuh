@@ -97,7 +97,8 @@ class AMG {
   void launch_fused(const T* b, T* x, cudaStream_t s);
   void cycle(int l, const T* b, T* x, cudaStream_t s);
   void coarse_correction(int l, const T* rc, T* ec, cudaStream_t s);
-  void smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start);
+  // xc (non-zero start only): fold x += P xc into the first step
+  void smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start, const T* xc = nullptr);
   std::vector<AMGLevel<T>> levels_;
   // coarsest level: dense inverse in FP64
   int nco_ = 0, co_nnz_ = 0;
