@@ -248,11 +248,18 @@ void with_lanes(int lanes, F&& f) {
 // Row-group width for a level: enough lanes that a row is read in one or two
 // coalesced passes (coarse aggregation levels have long rows).
 inline int lanes_for(long long n, long long nnz) {
+  static const int div = [] {
+    const char* e = std::getenv("PMB_AMG_LANES_DIV");
+    const int v = e ? std::atoi(e) : 1;
+    return v == 2 || v == 4 ? v : 1;
+  }();
   const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
-  if (avg > 24.0) return 32;
-  if (avg > 12.0) return 16;
-  if (avg > 5.0) return 8;
-  return 4;
+  int lanes = 4;
+  if (avg > 24.0) lanes = 32;
+  else if (avg > 12.0) lanes = 16;
+  else if (avg > 5.0) lanes = 8;
+  lanes /= div;
+  return lanes < 1 ? 1 : lanes;
 }
 
 // Coefficients of step `step` of the Chebyshev recurrence on [lm/10, lm].

@@ -258,3 +258,34 @@ class GpuOilWaterEnsemble(GpuOilWaterModel):
             for k, s in enumerate(self.split(self.from_device(x))):
                 out[k].append(s)
         return out, its_all
+
+
+def simulate_members_concurrently(members: Sequence, fluid, states0: Sequence[OWState], timesteps: Sequence[float],
+                                  gravity: float = 0.0, workers: int = 16, max_cuts: int = 6,
+                                  model_options: Optional[dict] = None):
+    """Every member on its own device model and CUDA stream, `workers` host
+    threads stepping members concurrently; each member follows exactly the
+    single-run path (simulate_schedule_ad), so its results are those of a
+    single run.  `members` are (grid, rock, wells).  Returns
+    (states[member][step], iterations[member, step])."""
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+    from .schedule import simulate_schedule_ad
+    torch = _torch()
+    opts = dict(model_options or {})
+    local = threading.local()
+
+    def run(k):
+        if not hasattr(local, "stream"):
+            local.stream = torch.cuda.Stream()
+        g, rock, wells = members[k]
+        with torch.cuda.stream(local.stream):
+            m = GpuOilWaterModel(g, rock, fluid, wells, gravity=gravity, **opts)
+            states, its = simulate_schedule_ad(states0[k], m, timesteps, max_cuts=max_cuts, verbose=False)
+            local.stream.synchronize()
+            del m
+        return states, its
+
+    with ThreadPoolExecutor(max_workers=max(1, int(workers))) as pool:
+        results = list(pool.map(run, range(len(members))))
+    return [r[0] for r in results], np.array([r[1] for r in results])
