@@ -241,25 +241,22 @@ void with_lanes(int lanes, F&& f) {
     case 16: f(std::integral_constant<int, 16>{}); break;
     case 8: f(std::integral_constant<int, 8>{}); break;
     case 4: f(std::integral_constant<int, 4>{}); break;
+    case 2: f(std::integral_constant<int, 2>{}); break;
     default: f(std::integral_constant<int, 1>{}); break;
   }
 }
 
-// Row-group width for a level: enough lanes that a row is read in one or two
-// coalesced passes (coarse aggregation levels have long rows).
+// Row-group width for a level: about two entries of the row per lane.
+// Measured on the channelised model: one entry per lane left the finest
+// level latency-bound (20 of 32 threads active, scoreboard stalls); two per
+// lane made the AMG cycle 11% faster, four per lane 9% slower.
 inline int lanes_for(long long n, long long nnz) {
-  static const int div = [] {
-    const char* e = std::getenv("PMB_AMG_LANES_DIV");
-    const int v = e ? std::atoi(e) : 1;
-    return v == 2 || v == 4 ? v : 1;
-  }();
   const double avg = n > 0 ? (double)nnz / (double)n : 0.0;
-  int lanes = 4;
-  if (avg > 24.0) lanes = 32;
-  else if (avg > 12.0) lanes = 16;
-  else if (avg > 5.0) lanes = 8;
-  lanes /= div;
-  return lanes < 1 ? 1 : lanes;
+  if (avg > 48.0) return 32;
+  if (avg > 24.0) return 16;
+  if (avg > 12.0) return 8;
+  if (avg > 5.0) return 4;
+  return 2;
 }
 
 // Coefficients of step `step` of the Chebyshev recurrence on [lm/10, lm].
