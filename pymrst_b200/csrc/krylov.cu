@@ -331,6 +331,10 @@ void GraphedApply::run(long long n, const double* r, double* z, cudaStream_t& s,
     out_.resize(n);
   }
   if (!exec_) {
+    if (failures_ >= kMaxCaptureFailures) {
+      body(r, z);
+      return;
+    }
     // capture on a private stream (the legacy default stream cannot be
     // captured); the graph is then launched on the owner's stream
     if (!cap_) PMB_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
@@ -338,25 +342,46 @@ void GraphedApply::run(long long n, const double* r, double* z, cudaStream_t& s,
     const long long before = launch_count();
     const cudaStream_t saved = s;
     s = cap_;
-    PMB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    PMB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
     cudaGraph_t g = nullptr;
+    bool captured = true;
     try {
       body(in_.get(), out_.get());
-    } catch (...) {
-      cudaStreamEndCapture(s, &g);
-      if (g) cudaGraphDestroy(g);
-      s = saved;
-      count_launch(-(launch_count() - before));
-      throw;
+    } catch (const Error& e) {
+      // only a CUDA-level failure can come from the capture being disturbed
+      // (by other threads' device work); anything else is a real error
+      if (e.code != PMB_ERR_CUDA) {
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        s = saved;
+        count_launch(-(launch_count() - before));
+        throw;
+      }
+      captured = false;
     }
     const cudaError_t ce = cudaStreamEndCapture(s, &g);
     s = saved;
-    PMB_CUDA(ce);
-    nodes_ = launch_count() - before;
-    count_launch(-nodes_);  // captured, not launched
+    count_launch(-(launch_count() - before));  // captured (or abandoned), not launched
+    if (!captured || ce != cudaSuccess || !g) {
+      // the capture was invalidated: clear the non-sticky capture error and
+      // run this application directly; later calls try to capture again
+      if (g) cudaGraphDestroy(g);
+      (void)cudaGetLastError();
+      ++failures_;
+      body(r, z);
+      return;
+    }
+    nodes_ = 0;
+    PMB_CUDA(cudaGraphGetNodes(g, nullptr, reinterpret_cast<size_t*>(&nodes_)));
     const cudaError_t e = cudaGraphInstantiate(&exec_, g, 0);
     cudaGraphDestroy(g);
-    PMB_CUDA(e);
+    if (e != cudaSuccess) {
+      exec_ = nullptr;
+      (void)cudaGetLastError();
+      ++failures_;
+      body(r, z);
+      return;
+    }
   }
   PMB_CUDA(cudaMemcpyAsync(in_.get(), r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   PMB_CUDA(cudaGraphLaunch(exec_, s));

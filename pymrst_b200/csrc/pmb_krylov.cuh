@@ -44,7 +44,9 @@ class Fgmres {
 // The body enqueues on the stream variable it is given (`s`), which is
 // pointed at a private capture stream while the body is recorded; the graph
 // then runs on the owner's stream.  PMB_NO_GRAPH=1 or PMB_PROFILE=1 run the
-// body directly.
+// body directly, and so does a call whose capture was invalidated (device
+// work of other threads can do that); after three such failures the graph is
+// no longer attempted.
 class GraphedApply {
  public:
   ~GraphedApply();
@@ -54,9 +56,11 @@ class GraphedApply {
   long long nodes() const { return nodes_; }
 
  private:
+  static constexpr int kMaxCaptureFailures = 3;
   cudaGraphExec_t exec_ = nullptr;
   cudaStream_t cap_ = nullptr;
   long long nodes_ = 0;
+  int failures_ = 0;  // invalidated captures; after kMaxCaptureFailures the body always runs directly
   DArray<double> in_, out_;
 };
 
