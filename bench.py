@@ -42,10 +42,11 @@ WORKLOAD = dict(name="channelised oil-water 60x220x85 (1,122,000 cells), 10-day 
 # reference's default linear solver.  A smaller sample favours the CPU
 # (direct-solve cost grows faster than linearly).
 CPU_SAMPLE = dict(dims=(18, 66, 25), cell_size=(6.1 * 60 / 18, 3.05 * 220 / 66, 0.61 * 85 / 25))
-# DRAM bytes per swept cell of one line_pcr_kernel launch, from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum) on the 60x220x60 model.
-PCR_DRAM_BYTES_PER_CELL = {"fp64": (190039296 + 8392448) / 396000.0,
-                           "mixed": (150901760 + 7420416) / 396000.0}
+# DRAM bytes per swept cell of one line_pcr_ell_kernel launch, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the 60x220x60 model
+# (396,000 cells per colour); None where no capture was taken.
+PCR_DRAM_BYTES_PER_CELL = {"fp64": None,
+                           "mixed": (78393600 + 3079936) / 396000.0}
 
 
 def parse():
@@ -238,12 +239,14 @@ def kernel_roofline(model, x, x0, dt, torch, N, reps=20):
     ms = N.C.c_double()
     sweeps = max(1, int(model.cpr_options.get("local_sweeps", 2)))
     N.check(N.lib().pmb_cpr_time_stage(s, 0, N.ptr(res), N.ptr(z), reps, N.C.byref(ms)))
-    # one line Gauss-Seidel sweep (two colour launches of line_gs_kernel and the
-    # well update): every block (FP64 32 B or FP32 16 B) and its column index
-    # once, row_ptr, and per cell r (16 B), z read and written (32 B), and the
-    # diagonal / line-neighbour / line-cell / perforation indices (20 B)
+    # one line Gauss-Seidel sweep (two colour launches of line_pcr_ell_kernel
+    # and the well update) on the line-ordered operator copy: every block (FP64
+    # 32 B or FP32 16 B) once, the column index of every block off the line
+    # (4 B; the diagonal and the two line couplings need none), and per cell r
+    # (16 B), z read and written (32 B) and its perforation index (4 B).  The
+    # zero padding of short rows is not counted.
     blk = 16 if int(model.cpr_options.get("precision", 0)) == 1 else 32
-    sweep_bytes = nnzb * (blk + 4) + (nc + 1) * 4 + nc * (16 + 32 + 20)
+    sweep_bytes = nnzb * blk + max(nnzb - 3 * nc, 0) * 4 + nc * (16 + 32 + 4)
     out["line_gs_sweep"] = dict(seconds=ms.value * 1e-3 / sweeps, bytes=sweep_bytes)
     N.check(N.lib().pmb_cpr_time_stage(s, 1, N.ptr(res), N.ptr(z), reps, N.C.byref(ms)))
     out["amg_cycle"] = dict(seconds=ms.value * 1e-3, bytes=None)
@@ -392,7 +395,7 @@ def run_ours(args):
     peak, peak_kind = peaks()
     dom = kr["line_gs_sweep"]
     ach = dom["bytes"] / dom["seconds"] / 1e9
-    # DRAM traffic of one line_pcr_kernel launch (one colour, half the cells),
+    # DRAM traffic of one line_pcr_ell_kernel launch (one colour, half the cells),
     # scaled from the ncu capture of dram__bytes_read.sum + dram__bytes_write.sum
     # on the 60x220x60 model (396,000 cells per colour)
     traffic = PCR_DRAM_BYTES_PER_CELL.get(args.precision)
@@ -416,7 +419,7 @@ def run_ours(args):
                     "d2h_bytes_per_step": nvec_bytes},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm",
-                         "kernel": "line_pcr_kernel (vertical-line block Gauss-Seidel, one colour per launch)",
+                         "kernel": "line_pcr_ell_kernel (vertical-line block Gauss-Seidel, one colour per launch)",
                          "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes": dom["bytes"] / 2,

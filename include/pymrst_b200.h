@@ -186,11 +186,15 @@ typedef struct pmb_cpr_opts {
   int32_t amg_coarse_size;  /* stop coarsening at this many unknowns */
   int32_t amg_rebuild_interval; /* re-aggregate after this many setups */
   double inner_rtol;        /* mixed precision: FP32 inner solve target */
+  int32_t replay_graph;     /* 1: the preconditioner is captured once and replayed as a CUDA
+                               graph; 0: its kernels are launched directly (for callers
+                               that drive several solvers from concurrent host threads) */
 } pmb_cpr_opts;
 
 /* Defaults: rtol 1e-8, maxiter 200, restart 50 (CPRSolver's,
  * linear_solvers.py:113-116); local_sweeps 4, Chebyshev degree 2, K-cycle on
- * 3 levels, theta 0.1, coarse size 200, re-aggregation every 8 setups. */
+ * 3 levels, theta 0.1, coarse size 200, re-aggregation every 8 setups,
+ * graph replay on. */
 int pmb_cpr_default_opts(pmb_cpr_opts* out);
 int pmb_cpr_create(pmb_ow* model, const pmb_cpr_opts* opts, pmb_cpr** out);
 int pmb_cpr_destroy(pmb_cpr* s);

@@ -45,7 +45,7 @@ class CPROpts(C.Structure):
         ("rtol", c_dbl), ("maxiter", c_int), ("restart", c_int), ("precision", c_int),
         ("use_pressure_stage", c_int), ("local_sweeps", c_int), ("amg_smoother_degree", c_int),
         ("amg_cycle", c_int), ("amg_theta", c_dbl), ("amg_coarse_size", c_int),
-        ("amg_rebuild_interval", c_int), ("inner_rtol", c_dbl),
+        ("amg_rebuild_interval", c_int), ("inner_rtol", c_dbl), ("replay_graph", c_int),
     ]
 
 

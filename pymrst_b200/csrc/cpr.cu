@@ -490,64 +490,26 @@ __device__ __forceinline__ Blk2<CT> binv(Blk2<CT> D, bool& ok) {
   return Blk2<CT>{id * D.w, -id * D.y, -id * D.z, id * D.x};
 }
 
-// CT is the arithmetic of the cyclic reduction: double, or float when the
-// smoother blocks are FP32 (mixed precision); the residual is formed in FP64.
-template <class BT, class CT>
-__global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lstart, const int* __restrict__ clines,
-                                                              const int* __restrict__ lptr,
-                                                              const int* __restrict__ lcells,
-                                                              const int* __restrict__ llo,
-                                                              const int* __restrict__ lup,
-                                                              const BT* __restrict__ A,
-                                                              const double* __restrict__ wj,
-                                                              const double* __restrict__ r, double* __restrict__ z,
-                                                              int* status) {
-  extern __shared__ __align__(16) unsigned char pcr_raw[];
+// The cyclic reduction of one line: thread u holds row u of the line's
+// block-tridiagonal system (D, Lb, Ub, y; Lb of the first row and Ub of the
+// last are zero); on a true return x is its solution.  Every thread of the CTA
+// takes part (act false for threads past the line's end); a singular pivot
+// sets *status and returns false.  `raw` is the CTA's shared memory,
+// 3 blocks and one vector per thread; `bad` a shared flag zeroed by thread 0
+// before the first barrier.
+template <class CT>
+__device__ __forceinline__ bool pcr_line(unsigned char* raw, int u, int len, bool act, Blk2<CT> D, Blk2<CT> Lb,
+                                         Blk2<CT> Ub, Vec2<CT> y, int* bad, int* status, Vec2<CT>& x) {
   const int nb = blockDim.x;
-  Blk2<CT>* sL = reinterpret_cast<Blk2<CT>*>(pcr_raw);
+  Blk2<CT>* sL = reinterpret_cast<Blk2<CT>*>(raw);
   Blk2<CT>* sU = sL + nb;
   Blk2<CT>* sI = sL + 2 * nb;
   Vec2<CT>* sY = reinterpret_cast<Vec2<CT>*>(sL + 3 * nb);
-  __shared__ int sBad;
-  const int line = clines[lstart + blockIdx.x];
-  const int t0 = lptr[line];
-  const int len = lptr[line + 1] - t0;
-  const int u = threadIdx.x;
-  const bool act = u < len;
-  if (u == 0) sBad = 0;
   const Blk2<CT> zero = {CT(0), CT(0), CT(0), CT(0)};
-  const double2* z2 = reinterpret_cast<const double2*>(z);
-  Blk2<CT> D = {CT(1), CT(0), CT(0), CT(1)}, Lb = zero, Ub = zero;
-  Vec2<CT> y = {CT(0), CT(0)};
-  int c = 0;
-  if (act) {
-    const int t = t0 + u;
-    c = lcells[t];
-    double2 rc = reinterpret_cast<const double2*>(r)[c];
-    // the line blocks first, so that their loads overlap the row gather
-    const int kl = u > 0 ? llo[t] : -1;
-    const int ku = u + 1 < len ? lup[t] : -1;
-    D = blk_of<CT>(ld4(A[v.diag_pos[c]]));
-    if (kl >= 0) Lb = blk_of<CT>(ld4(A[kl]));
-    if (ku >= 0) Ub = blk_of<CT>(ld4(A[ku]));
-    sub_row(v.col, A, z2, v.row_ptr[c], v.row_ptr[c + 1], rc);
-    const int q = v.cell_pc[c];
-    if (q >= 0) {
-      const double* zw = z + 2LL * v.nc;
-      for (int jj = v.pc_ptr[q]; jj < v.pc_ptr[q + 1]; ++jj) {
-        const int i = v.pc_perf[jj];
-        const int kw = v.perf_well[i];
-        const double* B = wj + v.wl.B + 6LL * i;
-        rc.x -= B[0] * zw[3 * kw] + B[1] * zw[3 * kw + 1] + B[2] * zw[3 * kw + 2];
-        rc.y -= B[3] * zw[3 * kw] + B[4] * zw[3 * kw + 1] + B[5] * zw[3 * kw + 2];
-      }
-    }
-    y = Vec2<CT>{(CT)rc.x, (CT)rc.y};
-  }
   for (int s = 1; s < len; s <<= 1) {
     bool ok = true;
     const Blk2<CT> I = binv(D, ok);
-    if (act && !ok) sBad = 1;
+    if (act && !ok) *bad = 1;
     if (act) {
       sL[u] = Lb;
       sU[u] = Ub;
@@ -555,7 +517,7 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
       sY[u] = y;
     }
     __syncthreads();
-    if (sBad) break;  // uniform: read after the barrier by every thread
+    if (*bad) break;  // uniform: read after the barrier by every thread
     if (act) {
       Blk2<CT> nD = D, nL = zero, nU = zero;
       Vec2<CT> ny = y;
@@ -582,35 +544,243 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lsta
     }
     __syncthreads();
   }
-  if (sBad) {
+  if (*bad) {
     if (u == 0) atomicExch(status, PMB_ERR_PIVOT);
-    return;
+    return false;
   }
-  if (!act) return;
+  if (!act) return false;
   bool ok = true;
   const Blk2<CT> I = binv(D, ok);
   if (!ok) {
     atomicExch(status, PMB_ERR_PIVOT);
-    return;
+    return false;
   }
-  const Vec2<CT> x = bmv(I, y);
+  x = bmv(I, y);
+  return true;
+}
+
+// rc -= the well columns of a cell's row: B blocks of its perforations (pc
+// its index among the perforated cells, -1 for none) times the well unknowns.
+__device__ __forceinline__ void sub_wells(const OWView& v, const double* __restrict__ wj,
+                                          const double* __restrict__ z, int pc, double2& rc) {
+  if (pc < 0) return;
+  const double* zw = z + 2LL * v.nc;
+  for (int jj = v.pc_ptr[pc]; jj < v.pc_ptr[pc + 1]; ++jj) {
+    const int i = v.pc_perf[jj];
+    const int kw = v.perf_well[i];
+    const double* B = wj + v.wl.B + 6LL * i;
+    rc.x -= B[0] * zw[3 * kw] + B[1] * zw[3 * kw + 1] + B[2] * zw[3 * kw + 2];
+    rc.y -= B[3] * zw[3 * kw] + B[4] * zw[3 * kw + 1] + B[5] * zw[3 * kw + 2];
+  }
+}
+
+// CT is the arithmetic of the cyclic reduction: double, or float when the
+// smoother blocks are FP32 (mixed precision); the residual is formed in FP64.
+template <class BT, class CT>
+__global__ void __launch_bounds__(kPcrMaxLen) line_pcr_kernel(OWView v, int lstart, const int* __restrict__ clines,
+                                                              const int* __restrict__ lptr,
+                                                              const int* __restrict__ lcells,
+                                                              const int* __restrict__ llo,
+                                                              const int* __restrict__ lup,
+                                                              const BT* __restrict__ A,
+                                                              const double* __restrict__ wj,
+                                                              const double* __restrict__ r, double* __restrict__ z,
+                                                              int* status) {
+  extern __shared__ __align__(16) unsigned char pcr_raw[];
+  __shared__ int sBad;
+  const int line = clines[lstart + blockIdx.x];
+  const int t0 = lptr[line];
+  const int len = lptr[line + 1] - t0;
+  const int u = threadIdx.x;
+  const bool act = u < len;
+  if (u == 0) sBad = 0;
+  const Blk2<CT> zero = {CT(0), CT(0), CT(0), CT(0)};
+  const double2* z2 = reinterpret_cast<const double2*>(z);
+  Blk2<CT> D = {CT(1), CT(0), CT(0), CT(1)}, Lb = zero, Ub = zero;
+  Vec2<CT> y = {CT(0), CT(0)};
+  int c = 0;
+  if (act) {
+    const int t = t0 + u;
+    c = lcells[t];
+    double2 rc = reinterpret_cast<const double2*>(r)[c];
+    // the line blocks first, so that their loads overlap the row gather
+    const int kl = u > 0 ? llo[t] : -1;
+    const int ku = u + 1 < len ? lup[t] : -1;
+    D = blk_of<CT>(ld4(A[v.diag_pos[c]]));
+    if (kl >= 0) Lb = blk_of<CT>(ld4(A[kl]));
+    if (ku >= 0) Ub = blk_of<CT>(ld4(A[ku]));
+    sub_row(v.col, A, z2, v.row_ptr[c], v.row_ptr[c + 1], rc);
+    sub_wells(v, wj, z, v.cell_pc[c], rc);
+    y = Vec2<CT>{(CT)rc.x, (CT)rc.y};
+  }
+  Vec2<CT> x;
+  if (!pcr_line<CT>(pcr_raw, u, len, act, D, Lb, Ub, y, &sBad, status, x)) return;
   double2 zc = z2[c];
   zc.x += (double)x.x;
   zc.y += (double)x.y;
   reinterpret_cast<double2*>(z)[c] = zc;
 }
 
+// ---- the line smoother on a line-ordered copy of its operator ----------------
+//
+// Position t of the line order is the t-th cell of the concatenated lines, so
+// the cells of one line are consecutive.  Blocks are stored slot-major,
+// blk[slot * nc + t]: slot 0 the diagonal, 1 and 2 the couplings to the
+// previous and next cell of the line (zero at a line end or where the cells
+// do not couple), 3.. the row's other blocks (zero-padded, their column the
+// position t itself).  Thread u of a line's CTA then reads blk[slot * nc +
+// t0 + u], rl / zl at t0 + u and, in a grid whose neighbouring lines have the
+// same cells, zl of the lateral neighbours at t0' + u: every load of a warp is
+// one contiguous run.
+constexpr int kEllMaxSlots = 12;  // diagonal, two line couplings, up to nine others
+constexpr int kEllPrefetch = 4;   // lateral entries loaded before the first is used
+
+template <class BT>
+__device__ __forceinline__ BT blk_store(double4 a);
+template <>
+__device__ __forceinline__ double4 blk_store<double4>(double4 a) {
+  return a;
+}
+template <>
+__device__ __forceinline__ float4 blk_store<float4>(double4 a) {
+  return make_float4((float)a.x, (float)a.y, (float)a.z, (float)a.w);
+}
+
+// blk[i] = A[src[i]] (zero where src is -1), in the smoother's storage type.
+template <class BT>
+__global__ void ell_gather_kernel(long long n, const int* __restrict__ src, const double4* __restrict__ A,
+                                  BT* __restrict__ blk) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = src[i];
+  blk[i] = blk_store<BT>(k >= 0 ? A[k] : make_double4(0.0, 0.0, 0.0, 0.0));
+}
+
+// Into line order: rl[t] = r of the t-th cell, zl[t] = its z (from_z) or the
+// prolonged pressure correction (xp_c, 0) (xp null: zero).  Without from_z
+// the well part of z is prolonged as well: (0, 0, xp[nc + k]) when the
+// pressure system has bhp unknowns (pw), else zero.
+template <class T>
+__global__ void line_enter_kernel(int nc, int nw, bool from_z, bool pw, const int* __restrict__ lcells,
+                                  const T* __restrict__ xp, const double* __restrict__ r, double* __restrict__ z,
+                                  double* __restrict__ rl, double* __restrict__ zl) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nc) {
+    const int c = lcells[t];
+    reinterpret_cast<double2*>(rl)[t] = reinterpret_cast<const double2*>(r)[c];
+    reinterpret_cast<double2*>(zl)[t] =
+        from_z ? reinterpret_cast<const double2*>(z)[c] : make_double2(xp ? (double)xp[c] : 0.0, 0.0);
+  }
+  if (from_z) return;
+  if (t < nw) {
+    z[2LL * nc + 3LL * t] = 0.0;
+    z[2LL * nc + 3LL * t + 1] = 0.0;
+    z[2LL * nc + 3LL * t + 2] = pw && xp ? (double)xp[nc + t] : 0.0;
+  }
+}
+
+// line_pcr_kernel on the line-ordered copy: one CTA per line of the colour,
+// thread u on position t0 + u.  zl is updated in place; with OUT (the last
+// sweep) the cell's new z is also written to z in cell order.  The well
+// unknowns are read from z (they stay in cell order).
+template <class BT, class CT, bool OUT>
+__global__ void __launch_bounds__(kPcrMaxLen) line_pcr_ell_kernel(OWView v, int lstart, const int* __restrict__ clines,
+                                                                  const int* __restrict__ lptr,
+                                                                  const int* __restrict__ lcells, int nslots,
+                                                                  const BT* __restrict__ blk,
+                                                                  const int* __restrict__ ecol,
+                                                                  const int* __restrict__ epc,
+                                                                  const double* __restrict__ wj,
+                                                                  const double* __restrict__ rl,
+                                                                  double* __restrict__ zl, double* __restrict__ z,
+                                                                  int* status) {
+  extern __shared__ __align__(16) unsigned char pcr_raw[];
+  __shared__ int sBad;
+  const int line = clines[lstart + blockIdx.x];
+  const int t0 = lptr[line];
+  const int len = lptr[line + 1] - t0;
+  const int u = threadIdx.x;
+  const bool act = u < len;
+  if (u == 0) sBad = 0;
+  const long long n = v.nc;
+  const int t = t0 + u;
+  const Blk2<CT> zero = {CT(0), CT(0), CT(0), CT(0)};
+  const double2 z0 = make_double2(0.0, 0.0);
+  const double2* zl2 = reinterpret_cast<const double2*>(zl);
+  Blk2<CT> D = {CT(1), CT(0), CT(0), CT(1)}, Lb = zero, Ub = zero;
+  Vec2<CT> y = {CT(0), CT(0)};
+  double2 zs = z0;
+  if (act) {
+    const int nlat = nslots - 3;
+    int cj[kEllPrefetch];
+#pragma unroll
+    for (int q = 0; q < kEllPrefetch; ++q) cj[q] = q < nlat ? ecol[q * n + t] : t;
+    const double4 Dd = ld4(blk[t]);
+    const double4 Ld = u > 0 ? ld4(blk[n + t]) : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double4 Ud = u + 1 < len ? ld4(blk[2 * n + t]) : make_double4(0.0, 0.0, 0.0, 0.0);
+    zs = zl2[t];
+    const double2 zlo = u > 0 ? zl2[t - 1] : z0;
+    const double2 zup = u + 1 < len ? zl2[t + 1] : z0;
+    double2 zq[kEllPrefetch];
+    double4 aq[kEllPrefetch];
+#pragma unroll
+    for (int q = 0; q < kEllPrefetch; ++q) {
+      zq[q] = z0;
+      aq[q] = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (q < nlat) {
+        zq[q] = zl2[cj[q]];
+        aq[q] = ld4(blk[(3 + q) * n + t]);
+      }
+    }
+    double2 rc = reinterpret_cast<const double2*>(rl)[t];
+    double2 m = mv2(Dd, zs);
+    rc.x -= m.x;
+    rc.y -= m.y;
+    m = mv2(Ld, zlo);
+    rc.x -= m.x;
+    rc.y -= m.y;
+    m = mv2(Ud, zup);
+    rc.x -= m.x;
+    rc.y -= m.y;
+#pragma unroll
+    for (int q = 0; q < kEllPrefetch; ++q) {
+      m = mv2(aq[q], zq[q]);
+      rc.x -= m.x;
+      rc.y -= m.y;
+    }
+    for (int q = kEllPrefetch; q < nlat; ++q) {
+      m = mv2(ld4(blk[(3 + q) * n + t]), zl2[ecol[q * n + t]]);
+      rc.x -= m.x;
+      rc.y -= m.y;
+    }
+    sub_wells(v, wj, z, epc[t], rc);
+    D = blk_of<CT>(Dd);
+    Lb = blk_of<CT>(Ld);
+    Ub = blk_of<CT>(Ud);
+    y = Vec2<CT>{(CT)rc.x, (CT)rc.y};
+  }
+  Vec2<CT> x;
+  if (!pcr_line<CT>(pcr_raw, u, len, act, D, Lb, Ub, y, &sBad, status, x)) return;
+  zs.x += (double)x.x;
+  zs.y += (double)x.y;
+  reinterpret_cast<double2*>(zl)[t] = zs;
+  if (OUT) reinterpret_cast<double2*>(z)[lcells[t]] = zs;
+}
+
 // Well unknowns: z_w += inv(D_k) (r_w - C z_cells - D_k z_w); one warp per
-// well, the lanes over its perforations.
+// well, the lanes over its perforations.  The cells' z is read from zc at the
+// perforated cell (ppos null) or at its line position ppos[i]; the wells' z
+// and r are in z and r.
 __global__ void __launch_bounds__(256) gs_well_kernel(OWView v, const double* __restrict__ wj,
-                                                      const double* __restrict__ r, double* __restrict__ z) {
+                                                      const double* __restrict__ r, double* __restrict__ z,
+                                                      const double* __restrict__ zc, const int* __restrict__ ppos) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int k = warp; k < v.nw; k += nwarp) {
     double s0 = 0.0, s1 = 0.0;
     for (int i = v.perf_ptr[k] + lane; i < v.perf_ptr[k + 1]; i += 32) {
-      const int c = v.perf_cell[i];
+      const int c = ppos ? ppos[i] : v.perf_cell[i];
       const double* C = wj + v.wl.C + 4LL * i;
-      const double zp = z[2LL * c], zs = z[2LL * c + 1];
+      const double zp = zc[2LL * c], zs = zc[2LL * c + 1];
       s0 += C[0] * zp + C[1] * zs;
       s1 += C[2] * zp + C[3] * zs;
     }
@@ -646,6 +816,7 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   PMB_REQUIRE(o_.rtol > 0.0, "rtol must be positive");
   PMB_REQUIRE(o_.precision == 0 || o_.precision == 1, "precision must be 0 (FP64) or 1 (FP32 preconditioner)");
   f32_ = o_.precision == 1;
+  graph_.enabled = o_.replay_graph != 0;
   kry_.init(m.nvec(), o_.restart, s_);
   w_.resize(2);
   part_.resize((size_t)kRedBlocks);
@@ -655,7 +826,8 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   if (m.nw() > 0) build_pressure_pattern();
   bp_.resize(np_);
   xp_.resize(np_);
-  if (m.has_lines()) {
+  if (m.has_lines()) build_line_ell();
+  if (m.has_lines() && !use_ell_) {
     line_y_.resize(2LL * m.nc());
     line_g_.resize(4LL * m.nc());
   }
@@ -665,7 +837,7 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   amg_.degree = amg32_.degree = std::max(1, o_.amg_smoother_degree);
   amg_.k_levels = amg32_.k_levels = std::max(0, o_.amg_cycle);
   if (f32_) {
-    jac32_.resize(4LL * m.nnzb());
+    if (m.has_lines() && !use_ell_) jac32_.resize(4LL * m.nnzb());
     bp32_.resize(np_);
     xp32_.resize(np_);
   }
@@ -732,6 +904,94 @@ void CPRSolver::build_pressure_pattern() {
   a_well_.resize(2LL * nw);
 }
 
+// The line-ordered copy of the smoother's operator (the layout is described
+// above line_pcr_ell_kernel).  Left unbuilt, so that the block-CSR kernels
+// run, when a line is longer than one CTA, a row has too many blocks, or
+// PMB_LINE_ELL=0.
+void CPRSolver::build_line_ell() {
+  static const bool off = [] {
+    const char* e = std::getenv("PMB_LINE_ELL");
+    return e && e[0] == '0';
+  }();
+  const auto& Ls = m_.lines();
+  const int nc = m_.nc();
+  if (off || Ls.max_len > kPcrMaxLen) return;
+  const auto& rp = m_.h_row_ptr();
+  const auto& col = m_.h_col();
+  const OWView v = m_.view();
+  std::vector<int> cells(nc), lo(nc), up(nc), cell_pc(nc), perf_cell(v.nperf);
+  PMB_CUDA(cudaMemcpy(cells.data(), Ls.line_cells.get(), sizeof(int) * nc, cudaMemcpyDeviceToHost));
+  PMB_CUDA(cudaMemcpy(lo.data(), Ls.line_lo.get(), sizeof(int) * nc, cudaMemcpyDeviceToHost));
+  PMB_CUDA(cudaMemcpy(up.data(), Ls.line_up.get(), sizeof(int) * nc, cudaMemcpyDeviceToHost));
+  PMB_CUDA(cudaMemcpy(cell_pc.data(), v.cell_pc, sizeof(int) * nc, cudaMemcpyDeviceToHost));
+  if (v.nperf)
+    PMB_CUDA(cudaMemcpy(perf_cell.data(), v.perf_cell, sizeof(int) * v.nperf, cudaMemcpyDeviceToHost));
+  std::vector<int> pos(nc);
+  for (int t = 0; t < nc; ++t) pos[cells[t]] = t;
+  int slots = 3;
+  for (int t = 0; t < nc; ++t) {
+    const int c = cells[t];
+    const int others = (rp[c + 1] - rp[c]) - 1 - (lo[t] >= 0) - (up[t] >= 0);
+    slots = std::max(slots, 3 + others);
+  }
+  if (slots > kEllMaxSlots) return;
+  const long long n = nc;
+  std::vector<int> src((size_t)slots * n, -1), ecol((size_t)std::max(slots - 3, 1) * n, 0), pc(nc);
+  for (int t = 0; t < nc; ++t) {
+    const int c = cells[t];
+    int q = 0;
+    for (int k = rp[c]; k < rp[c + 1]; ++k) {
+      if (col[k] == c) {
+        src[t] = k;
+      } else if (k == lo[t]) {
+        src[n + t] = k;
+      } else if (k == up[t]) {
+        src[2 * n + t] = k;
+      } else {
+        src[(3 + q) * n + t] = k;
+        ecol[q * n + t] = pos[col[k]];
+        ++q;
+      }
+    }
+    PMB_REQUIRE(src[t] >= 0, "a cell's block row has no diagonal block");
+    for (; q < slots - 3; ++q) ecol[q * n + t] = t;
+    pc[t] = cell_pc[c];
+  }
+  std::vector<int> perf_pos(std::max(v.nperf, 1), 0);
+  for (int i = 0; i < v.nperf; ++i) perf_pos[i] = pos[perf_cell[i]];
+  ell_.slots = slots;
+  ell_.src.upload(src, s_);
+  ell_.col.upload(ecol, s_);
+  ell_.pc.upload(pc, s_);
+  ell_.perf_pos.upload(perf_pos, s_);
+  if (f32_)
+    ell_.blk32.resize(4LL * slots * n);
+  else
+    ell_.blk64.resize(4LL * slots * n);
+  ell_.rl.resize(2 * n);
+  ell_.zl.resize(2 * n);
+  use_ell_ = true;
+}
+
+// The second stage's copy of the Jacobian: the line-ordered blocks, or the
+// FP32 block-CSR for the line kernels of mixed precision.
+void CPRSolver::prepare_local(const double* jac) {
+  const long long nnzb = m_.nnzb();
+  if (use_ell_) {
+    const long long n = (long long)ell_.slots * m_.nc();
+    if (f32_)
+      ell_gather_kernel<<<grid_for(n, 256), 256, 0, s_>>>(n, ell_.src.get(), reinterpret_cast<const double4*>(jac),
+                                                          reinterpret_cast<float4*>(ell_.blk32.get()));
+    else
+      ell_gather_kernel<<<grid_for(n, 256), 256, 0, s_>>>(n, ell_.src.get(), reinterpret_cast<const double4*>(jac),
+                                                          reinterpret_cast<double4*>(ell_.blk64.get()));
+    PMB_CHECK_LAUNCH();
+  } else if (f32_ && m_.has_lines()) {
+    to_f32_kernel<<<grid_for(4 * nnzb, 256), 256, 0, s_>>>(4 * nnzb, jac, jac32_.get());
+    PMB_CHECK_LAUNCH();
+  }
+}
+
 void CPRSolver::pressure_values(double* ext) {
   const OWView v = m_.view();
   const long long nnzb = m_.nnzb();
@@ -760,6 +1020,7 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
   well_ = well;
   const OWView v = m_.view();
   ++setups_;
+  prepare_local(jac);
   if (!o_.use_pressure_stage) return;
   psum_kernel<<<kRedBlocks, 256, 0, s_>>>(v.nc, reinterpret_cast<const double2*>(x), part_.get());
   PMB_CHECK_LAUNCH();
@@ -802,8 +1063,6 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
     const long long nnz = (long long)ap_.size();
     to_f32_kernel<<<grid_for(nnz, 256), 256, 0, s_>>>(nnz, ap_.get(), amg32_.level0_val());
     PMB_CHECK_LAUNCH();
-    to_f32_kernel<<<grid_for(4 * nnzb, 256), 256, 0, s_>>>(4 * nnzb, jac, jac32_.get());
-    PMB_CHECK_LAUNCH();
     amg32_.refresh(s_, status_.get());
   } else {
     values(amg_.level0_val());
@@ -812,10 +1071,49 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
   ++since_build_;
 }
 
-void CPRSolver::local_stage(const double* r, double* z) {
+void CPRSolver::local_stage(const double* r, double* z, bool entered) {
   const OWView v = m_.view();
   const auto& cp = m_.h_color_ptr();
   const double4* A = reinterpret_cast<const double4*>(jac_);
+  if (use_ell_) {
+    const auto& Ls = m_.lines();
+    if (!entered) {
+      line_enter_kernel<double><<<grid_for(v.nc, 256), 256, 0, s_>>>(
+          v.nc, v.nw, true, false, Ls.line_cells.get(), nullptr, r, z, ell_.rl.get(), ell_.zl.get());
+      PMB_CHECK_LAUNCH();
+    }
+    const int nb = std::max(32, (Ls.max_len + 31) / 32 * 32);
+    const int sweeps = std::max(1, o_.local_sweeps);
+    for (int sweep = 0; sweep < sweeps; ++sweep) {
+      const bool out = sweep + 1 == sweeps;
+      for (int q = 0; q + 1 < (int)Ls.h_color_ptr.size(); ++q) {
+        const int cnt = Ls.h_color_ptr[q + 1] - Ls.h_color_ptr[q];
+        if (cnt <= 0) continue;
+        auto go = [&](auto kernel, auto* blk, size_t smem) {
+          kernel<<<cnt, nb, (size_t)nb * smem, s_>>>(v, Ls.h_color_ptr[q], Ls.color_lines.get(), Ls.line_ptr.get(),
+                                                     Ls.line_cells.get(), ell_.slots, blk, ell_.col.get(),
+                                                     ell_.pc.get(), well_, ell_.rl.get(), ell_.zl.get(), z,
+                                                     status_.get());
+          PMB_CHECK_LAUNCH();
+        };
+        const size_t smem32 = 3 * sizeof(Blk2<float>) + sizeof(Vec2<float>);
+        const size_t smem64 = 3 * sizeof(Blk2<double>) + sizeof(Vec2<double>);
+        const float4* b32 = reinterpret_cast<const float4*>(ell_.blk32.get());
+        const double4* b64 = reinterpret_cast<const double4*>(ell_.blk64.get());
+        if (f32_)
+          out ? go(line_pcr_ell_kernel<float4, float, true>, b32, smem32)
+              : go(line_pcr_ell_kernel<float4, float, false>, b32, smem32);
+        else
+          out ? go(line_pcr_ell_kernel<double4, double, true>, b64, smem64)
+              : go(line_pcr_ell_kernel<double4, double, false>, b64, smem64);
+      }
+      if (v.nw) {
+        gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z, ell_.zl.get(), ell_.perf_pos.get());
+        PMB_CHECK_LAUNCH();
+      }
+    }
+    return;
+  }
   if (m_.has_lines()) {
     const auto& Ls = m_.lines();
     for (int sweep = 0; sweep < std::max(1, o_.local_sweeps); ++sweep) {
@@ -852,7 +1150,7 @@ void CPRSolver::local_stage(const double* r, double* z) {
         PMB_CHECK_LAUNCH();
       }
       if (v.nw) {
-        gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z);
+        gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z, z, nullptr);
         PMB_CHECK_LAUNCH();
       }
     }
@@ -867,7 +1165,7 @@ void CPRSolver::local_stage(const double* r, double* z) {
       PMB_CHECK_LAUNCH();
     }
     if (v.nw) {
-      gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z);
+      gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z, z, nullptr);
       PMB_CHECK_LAUNCH();
     }
   }
@@ -898,7 +1196,11 @@ void CPRSolver::precond_body(const double* r, double* z) {
       PhaseTimer pt("cpr.amg_cycle", s_);
       amg.apply(bp, xp, s_);
     }
-    if (np_ > v.nc) {
+    if (use_ell_) {
+      // prolongation straight into line order, with r
+      line_enter_kernel<<<gpro, 256, 0, s_>>>(v.nc, v.nw, false, np_ > v.nc, m_.lines().line_cells.get(), xp, r, z,
+                                              ell_.rl.get(), ell_.zl.get());
+    } else if (np_ > v.nc) {
       prolong_pw_kernel<<<gpro, 256, 0, s_>>>(v.nc, v.nw, xp, z);
     } else {
       prolong_p_kernel<<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, xp, z);
@@ -910,12 +1212,16 @@ void CPRSolver::precond_body(const double* r, double* z) {
       pressure_stage(bp32_.get(), xp32_.get(), amg32_);
     else
       pressure_stage(bp_.get(), xp_.get(), amg_);
+  } else if (use_ell_) {
+    line_enter_kernel<double><<<gpro, 256, 0, s_>>>(v.nc, v.nw, false, false, m_.lines().line_cells.get(), nullptr,
+                                                    r, z, ell_.rl.get(), ell_.zl.get());
+    PMB_CHECK_LAUNCH();
   } else {
     prolong_p_kernel<double><<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, nullptr, z);
     PMB_CHECK_LAUNCH();
   }
   PhaseTimer pt("cpr.local_stage", s_);
-  local_stage(r, z);
+  local_stage(r, z, use_ell_);
 }
 
 double CPRSolver::time_stage(int stage, const double* r, double* z, int reps) {

@@ -368,6 +368,7 @@ CsrCPR::CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, bool t
   PMB_REQUIRE(o_.rtol > 0.0, "rtol must be positive");
   PMB_REQUIRE(o_.precision == 0 || o_.precision == 1, "precision must be 0 (FP64) or 1 (FP32 preconditioner)");
   f32_ = o_.precision == 1;
+  graph_.enabled = o_.replay_graph != 0;
   PMB_REQUIRE(h_rp[0] == 0, "row_ptr[0] must be 0");
   for (int i = 0; i < n; ++i) {
     PMB_REQUIRE(h_rp[i + 1] >= h_rp[i], "row_ptr must be non-decreasing");

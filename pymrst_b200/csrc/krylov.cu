@@ -321,7 +321,7 @@ void GraphedApply::run(long long n, const double* r, double* z, cudaStream_t& s,
     const char* e = std::getenv("PMB_NO_GRAPH");
     return !(e && e[0] == '1');
   }();
-  if (!use_graph || PhaseTimer::enabled()) {
+  if (!use_graph || !enabled || PhaseTimer::enabled()) {
     body(r, z);
     return;
   }

@@ -27,7 +27,10 @@ class CPRSolver {
  private:
   void precond(const double* r, double* z);
   void precond_body(const double* r, double* z);
-  void local_stage(const double* r, double* z);
+  // entered: rl / zl already hold r and z in line order (ell_ path only)
+  void local_stage(const double* r, double* z, bool entered = false);
+  void prepare_local(const double* jac);
+  void build_line_ell();
   void check_status();
 
   OWModel& m_;
@@ -54,6 +57,18 @@ class CPRSolver {
   DArray<int> status_;
   DArray<double> bp_, xp_, ap_;  // pressure system rhs / solution / values for aggregation
   DArray<double> line_y_, line_g_;  // line Gauss-Seidel scratch (per line position)
+  // Line-ordered copy of the line smoother's operator (vertical lines of at
+  // most 256 cells, at most 12 blocks per row): `slots` blocks per position,
+  // slot-major, refreshed from the Jacobian at every setup; the lateral
+  // columns as line positions; per position the cell's perforated-cell index;
+  // per perforation its cell's position; r and z of the cells in line order.
+  struct LineEll {
+    int slots = 0;
+    DArray<int> src, col, pc, perf_pos;
+    DArray<double> blk64, rl, zl;
+    DArray<float> blk32;
+  } ell_;
+  bool use_ell_ = false;
   // Pressure system with one bhp unknown per well (np_ = nc + nw): CSR
   // pattern, the position of every cell block in it (bsr2ext), of each
   // perforation's (cell, well) and (well, cell) entries, and of each well's

@@ -43,10 +43,10 @@ class Fgmres {
 // z = body(r) replayed from one captured CUDA graph on fixed staging vectors.
 // The body enqueues on the stream variable it is given (`s`), which is
 // pointed at a private capture stream while the body is recorded; the graph
-// then runs on the owner's stream.  PMB_NO_GRAPH=1 or PMB_PROFILE=1 run the
-// body directly, and so does a call whose capture was invalidated (device
-// work of other threads can do that); after three such failures the graph is
-// no longer attempted.
+// then runs on the owner's stream.  PMB_NO_GRAPH=1, PMB_PROFILE=1 or
+// `enabled` false run the body directly, and so does a call whose capture was
+// invalidated (device work of other threads can do that); after three such
+// failures the graph is no longer attempted.
 class GraphedApply {
  public:
   ~GraphedApply();
@@ -54,6 +54,7 @@ class GraphedApply {
   void run(long long n, const double* r, double* z, cudaStream_t& s,
            const std::function<void(const double*, double*)>& body);
   long long nodes() const { return nodes_; }
+  bool enabled = true;  // false: run() always launches the body directly
 
  private:
   static constexpr int kMaxCaptureFailures = 3;

@@ -266,13 +266,19 @@ def simulate_members_concurrently(members: Sequence, fluid, states0: Sequence[OW
     """Every member on its own device model and CUDA stream, `workers` host
     threads stepping members concurrently; each member follows exactly the
     single-run path (simulate_schedule_ad), so its results are those of a
-    single run.  `members` are (grid, rock, wells).  Returns
+    single run (the preconditioner is launched kernel by kernel rather than
+    replayed from a CUDA graph; the kernels are the same).  `members` are
+    (grid, rock, wells).  Returns
     (states[member][step], iterations[member, step])."""
     import threading
     from concurrent.futures import ThreadPoolExecutor
     from .schedule import simulate_schedule_ad
     torch = _torch()
     opts = dict(model_options or {})
+    # A graph capture in one thread and device-wide work in another (a free,
+    # a device synchronisation) do not mix: the members launch directly,
+    # and the concurrency of the streams hides the launch latency instead.
+    opts["cpr_options"] = dict(opts.get("cpr_options") or {}, replay_graph=0)
     local = threading.local()
 
     def run(k):

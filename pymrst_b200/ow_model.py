@@ -114,7 +114,7 @@ def face_transmissibility_device(g, rock) -> np.ndarray:
     d_idx = t(order, np.int32)
     tf = torch.empty(g.faces.num, dtype=torch.float64, device=dev)
     N.check(N.lib().pmb_face_trans(g.faces.num, N.ptr(d_ptr), N.ptr(d_idx), N.ptr(th), N.ptr(tf), stream))
-    torch.cuda.synchronize()
+    torch.cuda.current_stream().synchronize()
     return tf.cpu().numpy(), th.cpu().numpy()
 
 
