@@ -1,6 +1,7 @@
 // Aggregation AMG: host aggregation, device Galerkin refresh, Chebyshev
 // smoothing, V-cycle, dense coarsest solve.
 #include <algorithm>
+#include <string>
 #include <cmath>
 #include <cstdlib>
 #include <numeric>
@@ -773,6 +774,7 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
     galerkin_kernel<T><<<grid_for(nnzc, 256), 256, 0, s>>>(nnzc, L.gptr.get(), L.gidx.get(), L.val.get(), cval);
     PMB_CHECK_LAUNCH();
   }
+  PhaseTimer pt("amg.refresh.coarse_inverse", s);
   dense_assemble_kernel<T><<<grid_for(nco_, 128), 128, 0, s>>>(nco_, co_row_ptr_.get(), co_col_.get(),
                                                                 co_val_.get(), co_dense_.get());
   PMB_CHECK_LAUNCH();
@@ -907,6 +909,20 @@ void AMG<T>::launch_fused(const T* b, T* x, cudaStream_t s) {
   PMB_CHECK_LAUNCH();
 }
 
+// Names of the per-level phase timers (active under PMB_PROFILE=1 only):
+// kind 0 pre-smoothing, 1 residual restriction, 2 prolongation and
+// post-smoothing, 3 the K-cycle's own kernels on that level.
+static const char* level_phase(int l, int kind) {
+  static const std::vector<std::string> names = [] {
+    static const char* kinds[] = {"pre", "restrict", "post", "kcycle"};
+    std::vector<std::string> v;
+    for (int i = 0; i < 32; ++i)
+      for (const char* k : kinds) v.push_back("amg.L" + std::string(i < 10 ? "0" : "") + std::to_string(i) + "." + k);
+    return v;
+  }();
+  return names[(size_t)std::min(l, 31) * 4 + kind].c_str();
+}
+
 template <class T>
 void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
   if (coop_start_ >= 0 && l == coop_start_) {
@@ -914,6 +930,7 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
     return;
   }
   if (l == (int)levels_.size()) {
+    PhaseTimer pt("amg.coarsest", s);
     launch_pdl(dense_apply_kernel<T>, grid_for(32LL * nco_, 256), 256, 0, s, nco_, (const double*)co_inv_.get(), b,
                x);
     return;
@@ -923,14 +940,21 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
   const int nc = next_is_coarsest ? nco_ : levels_[l + 1].n;
   T* bc = next_is_coarsest ? co_b_.get() : levels_[l + 1].b.get();
   T* xc = next_is_coarsest ? co_x_.get() : levels_[l + 1].x.get();
-  smooth(L, b, x, s, true);
-  with_lanes(L.lanes, [&](auto ln) {
-    constexpr int LN = decltype(ln)::value;
-    launch_pdl(restrict_residual_kernel<T, LN>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
-               (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
-               (const T*)x, bc);
-  });
+  {
+    PhaseTimer pt(level_phase(l, 0), s);
+    smooth(L, b, x, s, true);
+  }
+  {
+    PhaseTimer pt(level_phase(l, 1), s);
+    with_lanes(L.lanes, [&](auto ln) {
+      constexpr int LN = decltype(ln)::value;
+      launch_pdl(restrict_residual_kernel<T, LN>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
+                 (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
+                 (const T*)x, bc);
+    });
+  }
   coarse_correction(l, bc, xc, s);
+  PhaseTimer pt(level_phase(l, 2), s);
   if (L.n < kFoldProlongRows && degree >= 1) {
     smooth(L, b, x, s, false, xc);  // prolongation folded into the first smoothing step
   } else {
@@ -955,16 +979,20 @@ void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
   const int n = C.n, g = grid_for(n, 256);
   const int G = std::min(2 * kNumSM, g);
   cycle(l + 1, rc, C.kc1.get(), s);
-  with_lanes(C.lanes, [&](auto ln) {
-    constexpr int LN = decltype(ln)::value;
-    launch_pdl(csr_spmv_kernel<T, LN>, grid_for((long long)n * LN, 256), 256, 0, s, n, C.row_ptr, C.col,
-               (const T*)C.val.get(), (const T*)C.kc1.get(), C.kv1.get());
-  });
-  launch_pdl(kdots_kernel<T, 2>, G, 256, 0, s, n, (const T*)C.kv1.get(), (const T*)nullptr, rc, C.kpart.get());
-  launch_pdl(kcoef_kernel, 1, 160, 0, s, G, 0, (const double*)C.kpart.get(), C.kcoef.get());
-  launch_pdl(kaxpy_kernel<T>, g, 256, 0, s, n, rc, (const T*)C.kv1.get(), (const double*)C.kcoef.get(),
-             C.kr2.get());
+  {
+    PhaseTimer pt(level_phase(l + 1, 3), s);
+    with_lanes(C.lanes, [&](auto ln) {
+      constexpr int LN = decltype(ln)::value;
+      launch_pdl(csr_spmv_kernel<T, LN>, grid_for((long long)n * LN, 256), 256, 0, s, n, C.row_ptr, C.col,
+                 (const T*)C.val.get(), (const T*)C.kc1.get(), C.kv1.get());
+    });
+    launch_pdl(kdots_kernel<T, 2>, G, 256, 0, s, n, (const T*)C.kv1.get(), (const T*)nullptr, rc, C.kpart.get());
+    launch_pdl(kcoef_kernel, 1, 160, 0, s, G, 0, (const double*)C.kpart.get(), C.kcoef.get());
+    launch_pdl(kaxpy_kernel<T>, g, 256, 0, s, n, rc, (const T*)C.kv1.get(), (const double*)C.kcoef.get(),
+               C.kr2.get());
+  }
   cycle(l + 1, C.kr2.get(), C.kc2.get(), s);
+  PhaseTimer pt(level_phase(l + 1, 3), s);
   with_lanes(C.lanes, [&](auto ln) {
     constexpr int LN = decltype(ln)::value;
     launch_pdl(csr_spmv_kernel<T, LN>, grid_for((long long)n * LN, 256), 256, 0, s, n, C.row_ptr, C.col,

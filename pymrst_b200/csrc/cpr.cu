@@ -684,7 +684,7 @@ __global__ void line_enter_kernel(int nc, int nw, bool from_z, bool pw, const in
 // sweep) the cell's new z is also written to z in cell order.  The well
 // unknowns are read from z (they stay in cell order).
 template <class BT, class CT, bool OUT>
-__global__ void __launch_bounds__(kPcrMaxLen) line_pcr_ell_kernel(OWView v, int lstart, const int* __restrict__ clines,
+__global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3) line_pcr_ell_kernel(OWView v, int lstart, const int* __restrict__ clines,
                                                                   const int* __restrict__ lptr,
                                                                   const int* __restrict__ lcells, int nslots,
                                                                   const BT* __restrict__ blk,
@@ -715,36 +715,38 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_ell_kernel(OWView v, int 
     int cj[kEllPrefetch];
 #pragma unroll
     for (int q = 0; q < kEllPrefetch; ++q) cj[q] = q < nlat ? ecol[q * n + t] : t;
-    const double4 Dd = ld4(blk[t]);
-    const double4 Ld = u > 0 ? ld4(blk[n + t]) : make_double4(0.0, 0.0, 0.0, 0.0);
-    const double4 Ud = u + 1 < len ? ld4(blk[2 * n + t]) : make_double4(0.0, 0.0, 0.0, 0.0);
+    // blocks stay in their storage type until used (fewer registers in FP32)
+    const BT bz = blk_store<BT>(make_double4(0.0, 0.0, 0.0, 0.0));
+    const BT Dr = blk[t];
+    const BT Lr = u > 0 ? blk[n + t] : bz;
+    const BT Ur = u + 1 < len ? blk[2 * n + t] : bz;
     zs = zl2[t];
     const double2 zlo = u > 0 ? zl2[t - 1] : z0;
     const double2 zup = u + 1 < len ? zl2[t + 1] : z0;
     double2 zq[kEllPrefetch];
-    double4 aq[kEllPrefetch];
+    BT aq[kEllPrefetch];
 #pragma unroll
     for (int q = 0; q < kEllPrefetch; ++q) {
       zq[q] = z0;
-      aq[q] = make_double4(0.0, 0.0, 0.0, 0.0);
+      aq[q] = bz;
       if (q < nlat) {
         zq[q] = zl2[cj[q]];
-        aq[q] = ld4(blk[(3 + q) * n + t]);
+        aq[q] = blk[(3 + q) * n + t];
       }
     }
     double2 rc = reinterpret_cast<const double2*>(rl)[t];
-    double2 m = mv2(Dd, zs);
+    double2 m = mv2(ld4(Dr), zs);
     rc.x -= m.x;
     rc.y -= m.y;
-    m = mv2(Ld, zlo);
+    m = mv2(ld4(Lr), zlo);
     rc.x -= m.x;
     rc.y -= m.y;
-    m = mv2(Ud, zup);
+    m = mv2(ld4(Ur), zup);
     rc.x -= m.x;
     rc.y -= m.y;
 #pragma unroll
     for (int q = 0; q < kEllPrefetch; ++q) {
-      m = mv2(aq[q], zq[q]);
+      m = mv2(ld4(aq[q]), zq[q]);
       rc.x -= m.x;
       rc.y -= m.y;
     }
@@ -754,9 +756,9 @@ __global__ void __launch_bounds__(kPcrMaxLen) line_pcr_ell_kernel(OWView v, int 
       rc.y -= m.y;
     }
     sub_wells(v, wj, z, epc[t], rc);
-    D = blk_of<CT>(Dd);
-    Lb = blk_of<CT>(Ld);
-    Ub = blk_of<CT>(Ud);
+    D = blk_of<CT>(ld4(Dr));
+    Lb = blk_of<CT>(ld4(Lr));
+    Ub = blk_of<CT>(ld4(Ur));
     y = Vec2<CT>{(CT)rc.x, (CT)rc.y};
   }
   Vec2<CT> x;
@@ -1020,8 +1022,12 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
   well_ = well;
   const OWView v = m_.view();
   ++setups_;
-  prepare_local(jac);
+  {
+    PhaseTimer pt("cpr.setup.local", s_);
+    prepare_local(jac);
+  }
   if (!o_.use_pressure_stage) return;
+  PhaseTimer pt_values("cpr.setup.weights_values", s_);
   psum_kernel<<<kRedBlocks, 256, 0, s_>>>(v.nc, reinterpret_cast<const double2*>(x), part_.get());
   PMB_CHECK_LAUNCH();
   weights_kernel<<<1, 32, 0, s_>>>(v, kRedBlocks, part_.get(), w_.get());
@@ -1048,6 +1054,7 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
   };
   if (rebuild || f32_) values(ap_.get());
   if (rebuild) {
+    PhaseTimer pt("cpr.setup.aggregate", s_);
     const size_t nnz = ap_.size();
     h_ap_.resize(nnz);
     PMB_CUDA(cudaMemcpyAsync(h_ap_.data(), ap_.get(), sizeof(double) * nnz, cudaMemcpyDeviceToHost, s_));
@@ -1059,6 +1066,7 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
     since_build_ = 0;
     graph_.invalidate();  // the hierarchy's buffers are new
   }
+  PhaseTimer pt("cpr.setup.refresh", s_);
   if (f32_) {
     const long long nnz = (long long)ap_.size();
     to_f32_kernel<<<grid_for(nnz, 256), 256, 0, s_>>>(nnz, ap_.get(), amg32_.level0_val());
