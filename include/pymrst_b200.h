@@ -259,6 +259,13 @@ int pmb_csr_cpr_solve(pmb_csr_cpr* h, const double* d_b, double* d_x, double* h_
 int pmb_csr_spmv(pmb_csr_cpr* h, const double* d_values, const double* d_x, double* d_y);
 int pmb_csr_cpr_levels(const pmb_csr_cpr* h, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
 
+/* d_inv = d_a^-1 for a dense row-major n x n FP64 matrix (1 <= n <= 4096),
+ * the AMG coarsest-level solver: Gauss-Jordan with row pivoting.  Returns
+ * PMB_ERR_PIVOT for a singular matrix.  Synchronises the stream.  An
+ * internal of the device AMG, exported for testing; no reference
+ * counterpart. */
+int pmb_dense_inverse(int32_t n, const double* d_a, double* d_inv, void* stream);
+
 /* ------------------------------------------------------------------------
  * One backward-Euler step solved by Newton on the device (step,
  * two_phase_oil_water_model.py:605-657): d_x holds the state at the start

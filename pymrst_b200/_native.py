@@ -57,6 +57,7 @@ SIGNATURES = {
     "pmb_profile_report": (c_int, [C.c_char_p, c_int, c_int]),
     "pmb_compute_trans": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_vp, c_vp]),
     "pmb_face_trans": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "pmb_dense_inverse": (c_int, [c_int, c_vp, c_vp, c_vp]),
     "pmb_ow_create": (c_int, [C.POINTER(OWDesc), c_vp, C.POINTER(c_vp)]),
     "pmb_ow_destroy": (c_int, [c_vp]),
     "pmb_ow_sizes": (c_int, [c_vp, P_i64]),

@@ -340,6 +340,45 @@ __global__ void __launch_bounds__(256) restrict_residual_kernel(int nc, const in
   if (I < nc && sub == 0) bc[I] = (T)s;
 }
 
+// The same restricted residual, parallel over member rows: CTA b takes the
+// aggregates [blk[b], blk[b+1]) of the restriction plan; each lane group
+// forms the residual b_i - (A x)_i of one member row (looping over the
+// members only when one aggregate has more rows than the CTA has groups),
+// keeps it in shared memory, and one thread per aggregate then sums its
+// members in member order.  The member loop of restrict_residual_kernel
+// waits on a chain of dependent loads (member, row start, column, x) per
+// member; here the chains of all members overlap.
+template <class T, int LANES>
+__global__ void __launch_bounds__(256) restrict_rows_kernel(const int* __restrict__ blk, const int* __restrict__ cptr,
+                                                            const int* __restrict__ cmem,
+                                                            const int* __restrict__ rp, const int* __restrict__ ci,
+                                                            const T* __restrict__ a, const T* __restrict__ b,
+                                                            const T* __restrict__ x, T* __restrict__ bc) {
+  pdl_enter();
+  extern __shared__ double rr_smem[];
+  const int I0 = blk[blockIdx.x], I1 = blk[blockIdx.x + 1];
+  const int m0 = cptr[I0], m1 = cptr[I1];
+  const int groups = blockDim.x / LANES;
+  const int g = threadIdx.x / LANES, sub = threadIdx.x % LANES;
+  for (int mb = m0; mb < m1; mb += groups) {  // the same trip count for every thread
+    const int m = mb + g;
+    int i = 0;
+    double s = 0.0;
+    if (m < m1) {
+      i = cmem[m];
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s -= (double)a[k] * (double)x[ci[k]];
+    }
+    s = group_sum<LANES>(s);
+    if (m < m1 && sub == 0) rr_smem[m - m0] = (double)b[i] + s;
+  }
+  __syncthreads();
+  for (int I = I0 + threadIdx.x; I < I1; I += blockDim.x) {
+    double v = 0.0;
+    for (int m = cptr[I]; m < cptr[I + 1]; ++m) v += rr_smem[m - m0];
+    bc[I] = (T)v;
+  }
+}
+
 template <class T>
 __global__ void prolong_add_kernel(int n, const int* __restrict__ agg, const T* __restrict__ xc,
                                    T* __restrict__ x) {
@@ -367,62 +406,152 @@ __global__ void dense_assemble_kernel(int n, const int* __restrict__ rp, const i
   for (int k = rp[i]; k < rp[i + 1]; ++k) M[(size_t)i * n + ci[k]] = (double)a[k];
 }
 
-__global__ void __launch_bounds__(512) gauss_jordan_kernel(int n, double* __restrict__ M, double* __restrict__ Inv,
-                                    int* __restrict__ status) {
-  __shared__ int piv;
-  __shared__ double pval;
-  const int t = threadIdx.x, nt = blockDim.x;
-  for (int idx = t; idx < n * n; idx += nt) Inv[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
+// Dense coarsest inverse: in-place Gauss-Jordan elimination with row
+// pivoting in one CTA.  Step k takes the largest |A[i][k]|, i >= k, as pivot
+// (ties to the lowest row), swaps it into row k, scales row k by 1/pivot
+// (A[k][k] becomes 1/pivot) and subtracts A[i][k] times the new row k from
+// every other row i (A[i][k] becomes -A[i][k]/pivot).  The row interchanges
+// are undone at the end by the same column interchanges in reverse order.
+// The first m rows of the working matrix live in shared memory, the others
+// in Inv itself (L2-resident at these sizes); the pivot row and the
+// multipliers of each step are staged in shared memory, so every step is
+// four barriers and one parallel pass over the matrix.  Dynamic shared
+// memory: (2n + m n) doubles and n ints.  A zero or non-finite pivot sets
+// PMB_ERR_PIVOT in *status (the elimination goes on with pivot 1).
+constexpr int kGJThreads = 1024;
+
+__global__ void __launch_bounds__(kGJThreads) gauss_jordan_kernel(int n, int m, const double* __restrict__ M,
+                                                                  double* __restrict__ Inv,
+                                                                  int* __restrict__ status) {
+  extern __shared__ __align__(16) double gj_smem[];
+  double* prow = gj_smem;
+  double* fcol = prow + n;
+  double* srows = fcol + n;
+  int* piv = reinterpret_cast<int*>(srows + (size_t)m * n);
+  __shared__ double w_best[kGJThreads / 32];
+  __shared__ int w_idx[kGJThreads / 32];
+  __shared__ int s_p;
+  const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, warp = t >> 5;
+  auto row = [&](int r) -> double* { return r < m ? srows + (size_t)r * n : Inv + (size_t)r * n; };
+  const int nwarps = nt >> 5;
+  for (int i = warp; i < n; i += nwarps) {
+    double* ri = row(i);
+    for (int j = lane; j < n; j += 32) ri[j] = M[(size_t)i * n + j];
+  }
   __syncthreads();
-  for (int c = 0; c < n; ++c) {
-    if (t == 0) {
-      int p = c;
-      double best = fabs(M[(size_t)c * n + c]);
-      for (int r = c + 1; r < n; ++r) {
-        const double v = fabs(M[(size_t)r * n + c]);
-        if (v > best) { best = v; p = r; }
+  for (int k = 0; k < n; ++k) {
+    // pivot: the largest |A[i][k]| over i >= k, lowest row on ties
+    double best = -1.0;
+    int bi = n;
+    for (int i = k + t; i < n; i += nt) {
+      const double v = fabs(row(i)[k]);
+      if (v > best) {  // rows are visited in increasing order: ties keep the lower
+        best = v;
+        bi = i;
       }
-      piv = p;
-      pval = M[(size_t)p * n + c];
-      if (!(best > 0.0) || !isfinite(best)) atomicExch(status, PMB_ERR_PIVOT);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_down_sync(0xffffffffu, best, o);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      w_best[warp] = best;
+      w_idx[warp] = bi;
     }
     __syncthreads();
-    const int p = piv;
-    const double pv = (pval == 0.0 || !isfinite(pval)) ? 1.0 : pval;
-    if (p != c) {
+    if (warp == 0) {
+      const int nw = nt >> 5;
+      best = lane < nw ? w_best[lane] : -1.0;
+      bi = lane < nw ? w_idx[lane] : n;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (lane == 0) {
+        if (!(best > 0.0) || !isfinite(best) || bi >= n) {
+          atomicExch(status, PMB_ERR_PIVOT);
+          bi = k;
+        }
+        s_p = bi;
+        piv[k] = bi;
+      }
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p != k) {
+      double* rk = row(k);
+      double* rp = row(p);
       for (int j = t; j < n; j += nt) {
-        const double a = M[(size_t)c * n + j];
-        M[(size_t)c * n + j] = M[(size_t)p * n + j];
-        M[(size_t)p * n + j] = a;
-        const double b = Inv[(size_t)c * n + j];
-        Inv[(size_t)c * n + j] = Inv[(size_t)p * n + j];
-        Inv[(size_t)p * n + j] = b;
+        const double a = rk[j];
+        rk[j] = rp[j];
+        rp[j] = a;
       }
     }
     __syncthreads();
-    for (int j = t; j < n; j += nt) {
-      M[(size_t)c * n + j] /= pv;
-      Inv[(size_t)c * n + j] /= pv;
+    {
+      const double d = row(k)[k];
+      const double inv_d = (d != 0.0 && isfinite(d)) ? 1.0 / d : 1.0;
+      const double* rk = row(k);
+      for (int j = t; j < n; j += nt) prow[j] = j == k ? inv_d : rk[j] * inv_d;
+      for (int i = t; i < n; i += nt) fcol[i] = i == k ? 0.0 : row(i)[k];
     }
     __syncthreads();
-    // eliminate column c from every other row; M[r][c] is read, not written,
-    // in this pass, and updated with the Inv column afterwards
-    for (int idx = t; idx < n * n; idx += nt) {
-      const int r = idx / n, j = idx % n;
-      if (r == c || j == c) continue;
-      const double f = M[(size_t)r * n + c];
-      M[(size_t)r * n + j] -= f * M[(size_t)c * n + j];
-      Inv[(size_t)r * n + j] -= f * Inv[(size_t)c * n + j];
-    }
-    __syncthreads();
-    for (int r = t; r < n; r += nt) {
-      if (r == c) continue;
-      const double f = M[(size_t)r * n + c];
-      Inv[(size_t)r * n + c] -= f * Inv[(size_t)c * n + c];
-      M[(size_t)r * n + c] = 0.0;
+    for (int i = warp; i < n; i += nwarps) {
+      double* ri = row(i);
+      if (i == k) {
+        for (int j = lane; j < n; j += 32) ri[j] = prow[j];
+      } else {
+        const double f = fcol[i];
+        for (int j = lane; j < n; j += 32) ri[j] = (j == k ? 0.0 : ri[j]) - f * prow[j];
+      }
     }
     __syncthreads();
   }
+  for (int k = n - 1; k >= 0; --k) {
+    const int p = piv[k];
+    if (p != k)
+      for (int r = t; r < n; r += nt) {
+        double* rr = row(r);
+        const double a = rr[k];
+        rr[k] = rr[p];
+        rr[p] = a;
+      }
+    __syncthreads();
+  }
+  for (int i = warp; i < m; i += nwarps)
+    for (int j = lane; j < n; j += 32) Inv[(size_t)i * n + j] = srows[(size_t)i * n + j];
+}
+
+// Rows of an n x n Gauss-Jordan working matrix that fit in shared memory, and
+// the kernel's dynamic shared memory for them.  The kernel's limit is raised
+// once to the whole opt-in budget (the same value for every caller), so that
+// hierarchies with different coarsest sizes never lower it for one another.
+static void gj_layout(int n, int& rows, size_t& smem) {
+  int dev = 0, optin = 0;
+  PMB_CUDA(cudaGetDevice(&dev));
+  PMB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const long long budget = (long long)optin - 1024;  // the kernel's static shared memory
+  const long long fixed = 2LL * n * sizeof(double) + (long long)n * sizeof(int);
+  PMB_REQUIRE(n >= 1 && fixed <= budget, "dense matrix too large for the one-CTA inverse");
+  rows = (int)std::min<long long>(n, (budget - fixed) / ((long long)n * sizeof(double)));
+  smem = (size_t)(fixed + (long long)rows * n * sizeof(double));
+  PMB_CUDA(cudaFuncSetAttribute(gauss_jordan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
+}
+
+void dense_inverse(int n, const double* a, double* inv, int* d_status, cudaStream_t s) {
+  int rows = 0;
+  size_t smem = 0;
+  gj_layout(n, rows, smem);
+  gauss_jordan_kernel<<<1, kGJThreads, smem, s>>>(n, rows, a, inv, d_status);
+  PMB_CHECK_LAUNCH();
 }
 
 template <class T>
@@ -713,6 +842,26 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
       L.col = L.own_col.get();
     }
     L.lanes = lanes_for(L.n, L.nnz);
+    {
+      // restriction plan: consecutive aggregates while their members fit
+      // one per lane group
+      const int groups = 256 / L.lanes;
+      std::vector<int> blk(1, 0);
+      size_t most = 0;
+      const int nag = (int)h.cptr.size() - 1;
+      PMB_REQUIRE(nag >= 1, "an AMG level without aggregates");
+      for (int I = 0; I < nag;) {
+        int J = I + 1;
+        while (J < nag && h.cptr[J + 1] - h.cptr[I] <= groups) ++J;
+        most = std::max<size_t>(most, (size_t)(h.cptr[J] - h.cptr[I]));
+        blk.push_back(J);
+        I = J;
+      }
+      L.rblocks = (int)blk.size() - 1;
+      L.rsmem = std::max<size_t>(most, 1) * sizeof(double);
+      PMB_REQUIRE(L.rsmem <= 48 * 1024, "an AMG aggregate has too many members for the restriction kernel");
+      L.rblk.upload(blk, s);
+    }
     L.val.resize(L.nnz);
     L.dinv.resize(L.n);
     L.x.resize(L.n);
@@ -752,6 +901,7 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
   co_inv_.resize((size_t)nco_ * nco_);
   co_x_.resize(nco_);
   co_b_.resize(nco_);
+  gj_layout(nco_, gj_rows_, gj_smem_);
   bits_.resize(std::max<size_t>(levels_.size(), 1));
   build_fused(s);
   PMB_CUDA(cudaStreamSynchronize(s));
@@ -778,7 +928,7 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
   dense_assemble_kernel<T><<<grid_for(nco_, 128), 128, 0, s>>>(nco_, co_row_ptr_.get(), co_col_.get(),
                                                                 co_val_.get(), co_dense_.get());
   PMB_CHECK_LAUNCH();
-  gauss_jordan_kernel<<<1, 512, 0, s>>>(nco_, co_dense_.get(), co_inv_.get(), d_status);
+  gauss_jordan_kernel<<<1, kGJThreads, gj_smem_, s>>>(nco_, gj_rows_, co_dense_.get(), co_inv_.get(), d_status);
   PMB_CHECK_LAUNCH();
 }
 
@@ -946,11 +1096,20 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
   }
   {
     PhaseTimer pt(level_phase(l, 1), s);
+    static const bool by_rows = [] {
+      const char* e = std::getenv("PMB_RESTRICT_ROWS");
+      return !(e && e[0] == '0');
+    }();
     with_lanes(L.lanes, [&](auto ln) {
       constexpr int LN = decltype(ln)::value;
-      launch_pdl(restrict_residual_kernel<T, LN>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
-                 (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
-                 (const T*)x, bc);
+      if (by_rows)
+        launch_pdl(restrict_rows_kernel<T, LN>, L.rblocks, 256, L.rsmem, s, (const int*)L.rblk.get(),
+                   (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
+                   (const T*)x, bc);
+      else
+        launch_pdl(restrict_residual_kernel<T, LN>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
+                   (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
+                   (const T*)x, bc);
     });
   }
   coarse_correction(l, bc, xc, s);

@@ -164,6 +164,22 @@ int pmb_face_trans(int64_t nf, const int32_t* d_hf_ptr, const int32_t* d_hf_idx,
   });
 }
 
+int pmb_dense_inverse(int32_t n, const double* d_a, double* d_inv, void* stream) {
+  return guarded([&] {
+    PMB_REQUIRE(n >= 1 && n <= 4096, "n must be in 1..4096");
+    PMB_REQUIRE(d_a && d_inv && d_a != d_inv, "NULL or aliased argument");
+    const cudaStream_t s = (cudaStream_t)stream;
+    DArray<int> st;
+    st.resize(1);
+    st.zero(s);
+    dense_inverse(n, d_a, d_inv, st.get(), s);
+    int h = 0;
+    PMB_CUDA(cudaMemcpyAsync(&h, st.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    PMB_CUDA(cudaStreamSynchronize(s));
+    if (h != 0) throw Error(h, "zero pivot: the matrix is singular");
+  });
+}
+
 int pmb_ow_create(const pmb_ow_desc* desc, void* stream, pmb_ow** out) {
   return guarded([&] {
     PMB_REQUIRE(desc && out, "NULL argument");

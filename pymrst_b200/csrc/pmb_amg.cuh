@@ -13,6 +13,11 @@
 
 namespace pmb {
 
+// inv = A^-1 for a dense row-major n x n FP64 matrix on the device: in-place
+// Gauss-Jordan with row pivoting in one CTA (n up to about 11,000).  A zero or
+// non-finite pivot sets PMB_ERR_PIVOT in *d_status.
+void dense_inverse(int n, const double* a, double* inv, int* d_status, cudaStream_t s);
+
 struct AMGHostLevel {
   int n = 0;
   std::vector<int> row_ptr, col;      // pattern of this level's matrix
@@ -42,6 +47,13 @@ struct AMGLevel {
   DArray<double> kpart, kcoef;        // K-cycle reduction partials and coefficients
   DArray<int> agg, cptr, cmem, gptr, gidx;
   DArray<double> lmax;  // Chebyshev upper bound (device scalar)
+  // Restriction plan: CTA b of restrict_rows_kernel takes the aggregates
+  // [rblk[b], rblk[b+1]), at most one member row per lane group unless a
+  // single aggregate is larger; rsmem bytes of shared memory hold the member
+  // residuals of the largest CTA.
+  DArray<int> rblk;
+  int rblocks = 0;
+  size_t rsmem = 0;
 };
 
 // One level as seen by the fused coarse-cycle kernel.
@@ -102,6 +114,8 @@ class AMG {
   std::vector<AMGLevel<T>> levels_;
   // coarsest level: dense inverse in FP64
   int nco_ = 0, co_nnz_ = 0;
+  int gj_rows_ = 0;     // rows of the coarse inverse's working matrix held in shared memory
+  size_t gj_smem_ = 0;  // its dynamic shared memory
   DArray<int> co_row_ptr_, co_col_;
   DArray<T> co_val_;
   DArray<double> co_dense_, co_inv_;
