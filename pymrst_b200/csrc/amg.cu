@@ -868,6 +868,7 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
     L.b.resize(L.n);
     L.r.resize(L.n);
     L.t.resize(L.n);
+    L.u.resize(L.n);
     L.agg.upload(h.agg, s);
     L.cptr.upload(h.cptr, s);
     L.cmem.upload(h.cmem, s);
@@ -935,9 +936,13 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
 template <class T>
 void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start, const T* xc) {
   // degree steps ping-pong between x and L.t, ordered so that the last one
-  // writes x; only an odd step count from a non-zero start needs a copy
+  // writes x; the first step of an odd count from a non-zero start, which
+  // would overwrite its own input, writes L.u instead.  Only a single step
+  // from a non-zero start needs a copy.
   const int steps = std::max(1, degree);
   T* t = L.t.get();
+  T* u = L.u.get();
+  auto out_for = [&](int k) -> T* { return ((steps - 1 - k) % 2 == 0) ? x : t; };
   T* cur = x;
   int step = 0;
   with_lanes(L.lanes, [&](auto ln) {
@@ -952,7 +957,8 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
       step = 1;
     }
     for (; step < steps; ++step) {
-      T* out = (cur == x) ? t : x;
+      T* out = out_for(step);
+      if (out == cur) out = u;
       if (xc && step == 0)  // x + P xc, folded into the first step
         launch_pdl(cheb_step_kernel<T, false, LN, true>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
                    (const T*)L.dinv.get(), b, (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step,

@@ -542,6 +542,12 @@ int pmb_ow_step_members(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t m
       double info[4];
       const bool ok = cpr.solve(m.res(), m.dx(), info);
       krylov += info[0];
+      static const bool trace = [] {
+        const char* e = std::getenv("PMB_NEWTON_TRACE");
+        return e && e[0] == '1';
+      }();
+      if (trace) std::fprintf(stderr, "# members it=%d active=%d krylov=%g relres=%.2e ok=%d\n", it, active, info[0],
+                              info[1], (int)ok);
       if (!ok) {
         for (int k = 0; k < nmem; ++k)
           if (state[k] == 1) {

@@ -42,7 +42,7 @@ struct AMGLevel {
   const int* row_ptr = nullptr;  // device (level 0 borrows the operator pattern)
   const int* col = nullptr;
   DArray<int> own_row_ptr, own_col;
-  DArray<T> val, dinv, x, b, r, t;
+  DArray<T> val, dinv, x, b, r, t, u;  // u: first output of an odd smoothing count
   DArray<T> kc1, kc2, kv1, kv2, kr2;  // K-cycle vectors of this level (as a coarse level)
   DArray<double> kpart, kcoef;        // K-cycle reduction partials and coefficients
   DArray<int> agg, cptr, cmem, gptr, gidx;
