@@ -100,8 +100,8 @@ struct pmb_ow {
   PinnedArray<double> conv;
   // batch-of-members stepping: member ranges, flags and per-member values
   DArray<int> mem_cell, mem_well, mem_flag;
-  DArray<double> mem_conv;
-  PinnedArray<double> mem_conv_h;
+  DArray<double> mem_conv, mem_lin, mem_linres;
+  PinnedArray<double> mem_conv_h, mem_linres_h;
   PinnedArray<int> mem_flag_h;
 };
 
@@ -549,13 +549,38 @@ int pmb_ow_step_members(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t m
       if (trace) std::fprintf(stderr, "# members it=%d active=%d krylov=%g relres=%.2e ok=%d\n", it, active, info[0],
                               info[1], (int)ok);
       if (!ok) {
-        for (int k = 0; k < nmem; ++k)
-          if (state[k] == 1) {
+        // The shared solve missed its tolerance.  A member whose own block of
+        // the linear residual meets it has the update a solve of its system
+        // alone would accept: it goes on; the others fail this step.
+        if (h->mem_lin.size() != (size_t)m.nvec()) h->mem_lin.resize(m.nvec());
+        if (h->mem_linres.size() != 2 * (size_t)nmem) {
+          h->mem_linres.resize(2LL * nmem);
+          h->mem_linres_h.resize(2LL * nmem);
+        }
+        m.member_linear_residuals_async(nmem, h->mem_cell.get(), h->mem_well.get(), m.res(), m.dx(),
+                                        h->mem_lin.get(), h->mem_linres.get());
+        PMB_CUDA(cudaMemcpyAsync(h->mem_linres_h.get(), h->mem_linres.get(), sizeof(double) * 2 * nmem,
+                                 cudaMemcpyDeviceToHost, st));
+        PMB_CUDA(cudaStreamSynchronize(st));
+        const double tol2 = cpr.opts().rtol * cpr.opts().rtol;
+        int kept = 0;
+        for (int k = 0; k < nmem; ++k) {
+          if (state[k] != 1) continue;
+          const double rr = h->mem_linres_h[2 * k], bb = h->mem_linres_h[2 * k + 1];
+          if (std::isfinite(rr) && rr <= tol2 * bb) {
+            ++kept;
+          } else {
             state[k] = 3;
             h_its[k] = it;
           }
-        active = 0;
-        break;
+        }
+        if (trace) std::fprintf(stderr, "# members it=%d kept %d of %d after the shared solve failed\n", it, kept,
+                                active);
+        active = kept;
+        if (kept == 0) break;
+        for (int k = 0; k < nmem; ++k) h->mem_flag_h[k] = state[k] == 1 ? 1 : 0;
+        PMB_CUDA(cudaMemcpyAsync(h->mem_flag.get(), h->mem_flag_h.get(), sizeof(int) * nmem,
+                                 cudaMemcpyHostToDevice, st));
       }
       m.mask_members(nmem, h->mem_cell.get(), h->mem_well.get(), h->mem_flag.get(), m.dx());
       m.update(d_x, m.dx(), -1.0);

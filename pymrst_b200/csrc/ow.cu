@@ -698,6 +698,35 @@ __global__ void __launch_bounds__(256) ow_member_conv_kernel(OWView v, const int
   o[7] = 0.0;
 }
 
+// Per member m, out[2m] = ||b_m - y_m||^2 and out[2m+1] = ||b_m||^2 over its
+// cells and wells (y = J dx of the shared solve); one CTA per member.
+__global__ void __launch_bounds__(256) ow_member_linres_kernel(OWView v, const int* __restrict__ cell_ptr,
+                                                               const int* __restrict__ well_ptr,
+                                                               const double* __restrict__ b,
+                                                               const double* __restrict__ y,
+                                                               double* __restrict__ out) {
+  __shared__ double sh[32];
+  const int m = blockIdx.x;
+  double rr = 0.0, bb = 0.0;
+  for (long long i = 2LL * cell_ptr[m] + threadIdx.x; i < 2LL * cell_ptr[m + 1]; i += blockDim.x) {
+    const double d = b[i] - y[i];
+    rr += d * d;
+    bb += b[i] * b[i];
+  }
+  for (long long i = 2LL * v.nc + 3LL * well_ptr[m] + threadIdx.x; i < 2LL * v.nc + 3LL * well_ptr[m + 1];
+       i += blockDim.x) {
+    const double d = b[i] - y[i];
+    rr += d * d;
+    bb += b[i] * b[i];
+  }
+  rr = block_sum(rr, sh);
+  bb = block_sum(bb, sh);
+  if (threadIdx.x == 0) {
+    out[2 * m] = rr;
+    out[2 * m + 1] = bb;
+  }
+}
+
 // Zero the entries (cells and wells) of every member whose flag is 0.
 __global__ void __launch_bounds__(256) ow_member_mask_kernel(OWView v, const int* __restrict__ cell_ptr,
                                                              const int* __restrict__ well_ptr,
@@ -1011,6 +1040,13 @@ void OWModel::spmv(const double* jac, const double* well, const double* x, doubl
 void OWModel::member_convergence_async(int nmem, const int* cell_ptr, const int* well_ptr, const double* res,
                                        const double* x, double dt, double* d_out) {
   ow_member_conv_kernel<<<nmem, 256, 0, stream_>>>(v_, cell_ptr, well_ptr, res, x, dt, d_out);
+  PMB_CHECK_LAUNCH();
+}
+
+void OWModel::member_linear_residuals_async(int nmem, const int* cell_ptr, const int* well_ptr, const double* b,
+                                            const double* dx, double* tmp, double* d_out) {
+  spmv(jac(), well(), dx, tmp);
+  ow_member_linres_kernel<<<nmem, 256, 0, stream_>>>(v_, cell_ptr, well_ptr, b, tmp, d_out);
   PMB_CHECK_LAUNCH();
 }
 

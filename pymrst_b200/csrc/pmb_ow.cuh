@@ -106,6 +106,10 @@ class OWModel {
   void member_convergence_async(int nmem, const int* cell_ptr, const int* well_ptr, const double* res,
                                 const double* x, double dt, double* d_out);
   void mask_members(int nmem, const int* cell_ptr, const int* well_ptr, const int* flag, double* vec);
+  // Per member squared norms [||b - J dx||^2, ||b||^2] of a shared linear
+  // solve (J the current Jacobian; tmp an nvec scratch vector).
+  void member_linear_residuals_async(int nmem, const int* cell_ptr, const int* well_ptr, const double* b,
+                                     const double* dx, double* tmp, double* d_out);
   // Phase fluxes of every interface (what face f adds to the rows of N[f,0]
   // and subtracts from those of N[f,1]) and every perforation's surface
   // rates (what it subtracts from its cell's rows and its well's rate rows)
