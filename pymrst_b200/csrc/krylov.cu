@@ -8,29 +8,58 @@
 
 namespace pmb {
 
-constexpr int kRedBlocks = 2 * kNumSM;
+constexpr int kRedBlocks = 4 * kNumSM;
 constexpr int kDotChunk = 8;
 
 // Chunked multi-dot: part[i * G + blk] = partial dot(V_i, w) for i < nv and,
 // with with_ww, part[nv * G + blk] = partial dot(w, w).  Eight dots share one
 // read of w and one block reduction; each block owns one contiguous chunk.
+// VEC reads pairs of elements (16-byte loads; V's row stride even, V and w
+// 16-byte aligned); an odd last element is added by the last block.
 // Skipped (returns at once) when `gate` is given and *gate != run_if.
-__global__ void __launch_bounds__(256) mdot8_kernel(long long n, const double* __restrict__ V, long long ld, int nv,
-                                                    const double* __restrict__ w, int with_ww,
-                                                    double* __restrict__ part, const int* __restrict__ gate,
-                                                    int run_if) {
+template <bool VEC>
+__global__ void __launch_bounds__(256, 4) mdot8_kernel(long long n, const double* __restrict__ V, long long ld, int nv,
+                                                       const double* __restrict__ w, int with_ww,
+                                                       double* __restrict__ part, const int* __restrict__ gate,
+                                                       int run_if) {
   if (gate && *gate != run_if) return;
   __shared__ double sh[kDotChunk][8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  const long long chunk = (n + gridDim.x - 1) / gridDim.x;
+  const long long nu = VEC ? n / 2 : n;
+  const long long chunk = (nu + gridDim.x - 1) / gridDim.x;
   const long long e0 = blockIdx.x * chunk;
-  const long long e1 = min(n, e0 + chunk);
+  const long long e1 = min(nu, e0 + chunk);
+  const bool tail = VEC && (n & 1) && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0;
   const int ntot = nv + (with_ww ? 1 : 0);
   for (int i0 = 0; i0 < ntot; i0 += kDotChunk) {
     double acc[kDotChunk];
 #pragma unroll
     for (int q = 0; q < kDotChunk; ++q) acc[q] = 0.0;
     for (long long e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+      if (VEC) {
+        const double2 we = reinterpret_cast<const double2*>(w)[e];
+#pragma unroll
+        for (int q = 0; q < kDotChunk; ++q) {
+          const int i = i0 + q;
+          if (i < nv) {
+            const double2 v = reinterpret_cast<const double2*>(V + i * ld)[e];
+            acc[q] += v.x * we.x + v.y * we.y;
+          } else if (i == nv && with_ww) {
+            acc[q] += we.x * we.x + we.y * we.y;
+          }
+        }
+      } else {
+        const double we = w[e];
+#pragma unroll
+        for (int q = 0; q < kDotChunk; ++q) {
+          const int i = i0 + q;
+          if (i < nv) acc[q] += V[i * ld + e] * we;
+          else if (i == nv && with_ww) acc[q] += we * we;
+        }
+      }
+    }
+    if (tail) {
+      const long long e = n - 1;
       const double we = w[e];
 #pragma unroll
       for (int q = 0; q < kDotChunk; ++q) {
@@ -53,6 +82,17 @@ __global__ void __launch_bounds__(256) mdot8_kernel(long long n, const double* _
     }
     __syncthreads();
   }
+}
+
+// Launches mdot8_kernel, with pair loads where the alignment allows them.
+static void launch_mdot8(cudaStream_t s, long long n, const double* V, long long ld, int nv, const double* w,
+                         int with_ww, double* part, const int* gate, int run_if) {
+  const bool vec = ((uintptr_t)w % 16 == 0) && (nv == 0 || ((uintptr_t)V % 16 == 0 && ld % 2 == 0));
+  if (vec)
+    mdot8_kernel<true><<<kRedBlocks, 256, 0, s>>>(n, V, ld, nv, w, with_ww, part, gate, run_if);
+  else
+    mdot8_kernel<false><<<kRedBlocks, 256, 0, s>>>(n, V, ld, nv, w, with_ww, part, gate, run_if);
+  PMB_CHECK_LAUNCH();
 }
 
 // hs[q] = sum_b part[q*G + b] for q < nq (fixed order: lane-strided sums, then
@@ -108,7 +148,11 @@ __global__ void __launch_bounds__(256) mdot_final_kernel(int nv, int G, const do
   if (acc) acc[i] += s;
 }
 
-// w -= sum_i h[i] V_i
+// w -= sum_i h[i] V_i, subtracting in the order of i.  Each thread takes a
+// pair of elements (16-byte loads: V is the basis, its row stride a multiple
+// of 32, and w the work vector, both allocated by Fgmres) and issues the
+// loads of four vectors before their updates; the thread with global index 0
+// also takes an odd last element.
 __global__ void __launch_bounds__(256) vupdate_kernel(long long n, const double* __restrict__ V, long long ld,
                                                       int nv, const double* __restrict__ h,
                                                       double* __restrict__ w, const int* __restrict__ gate = nullptr,
@@ -117,8 +161,30 @@ __global__ void __launch_bounds__(256) vupdate_kernel(long long n, const double*
   __shared__ double hs[kMaxRestart + 2];
   for (int i = threadIdx.x; i < nv; i += blockDim.x) hs[i] = h[i];
   __syncthreads();
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
+  const long long nu = n / 2;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (long long e = tid; e < nu; e += (long long)gridDim.x * blockDim.x) {
+    double2 s = reinterpret_cast<const double2*>(w)[e];
+    int i = 0;
+    for (; i + 4 <= nv; i += 4) {
+      double2 v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] = reinterpret_cast<const double2*>(V + (i + q) * ld)[e];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        s.x -= hs[i + q] * v[q].x;
+        s.y -= hs[i + q] * v[q].y;
+      }
+    }
+    for (; i < nv; ++i) {
+      const double2 v = reinterpret_cast<const double2*>(V + i * ld)[e];
+      s.x -= hs[i] * v.x;
+      s.y -= hs[i] * v.y;
+    }
+    reinterpret_cast<double2*>(w)[e] = s;
+  }
+  if ((n & 1) && tid == 0) {
+    const long long e = n - 1;
     double s = w[e];
     for (int i = 0; i < nv; ++i) s -= hs[i] * V[i * ld + e];
     w[e] = s;
@@ -183,8 +249,7 @@ void Fgmres::init(long long n, int restart, cudaStream_t s) {
 }
 
 double Fgmres::norm(const double* a) {
-  mdot8_kernel<<<kRedBlocks, 256, 0, s_>>>(n_, a, n_, 0, a, 1, part_.get(), nullptr, 0);
-  PMB_CHECK_LAUNCH();
+  launch_mdot8(s_, n_, a, n_, 0, a, 1, part_.get(), nullptr, 0);
   mdot_final_kernel<<<1, 256, 0, s_>>>(1, kRedBlocks, part_.get(), htmp_.get(), nullptr, 1);
   PMB_CHECK_LAUNCH();
   PMB_CUDA(cudaMemcpyAsync(h_pin_.get(), htmp_.get(), sizeof(double), cudaMemcpyDeviceToHost, s_));
@@ -229,20 +294,17 @@ bool Fgmres::solve(const Apply& op, const Apply& prec, const double* b, double* 
       const int nv = j + 1;
       PhaseTimer pt_orth("gmres.orthogonalise", s_);
       int* flag = flag_.get();
-      mdot8_kernel<<<kRedBlocks, 256, 0, s_>>>(n, V_.get(), ld_, nv, wv_.get(), 1, part_.get(), nullptr, 0);
-      PMB_CHECK_LAUNCH();
+      launch_mdot8(s_, n, V_.get(), ld_, nv, wv_.get(), 1, part_.get(), nullptr, 0);
       orth_decide_kernel<<<1, 256, 0, s_>>>(nv, kRedBlocks, part_.get(), hcol_.get(), flag);
       PMB_CHECK_LAUNCH();
       vupdate_kernel<<<gv, 256, 0, s_>>>(n, V_.get(), ld_, nv, hcol_.get(), wv_.get());
       PMB_CHECK_LAUNCH();
-      mdot8_kernel<<<kRedBlocks, 256, 0, s_>>>(n, V_.get(), ld_, nv, wv_.get(), 0, part_.get(), flag, 1);
-      PMB_CHECK_LAUNCH();
+      launch_mdot8(s_, n, V_.get(), ld_, nv, wv_.get(), 0, part_.get(), flag, 1);
       mdot_final_kernel<<<1, 256, 0, s_>>>(nv, kRedBlocks, part_.get(), htmp_.get(), hcol_.get(), 0, flag, 1);
       PMB_CHECK_LAUNCH();
       vupdate_kernel<<<gv, 256, 0, s_>>>(n, V_.get(), ld_, nv, htmp_.get(), wv_.get(), flag, 1);
       PMB_CHECK_LAUNCH();
-      mdot8_kernel<<<kRedBlocks, 256, 0, s_>>>(n, wv_.get(), n, 0, wv_.get(), 1, part_.get(), flag, 1);
-      PMB_CHECK_LAUNCH();
+      launch_mdot8(s_, n, wv_.get(), n, 0, wv_.get(), 1, part_.get(), flag, 1);
       mdot_final_kernel<<<1, 256, 0, s_>>>(1, kRedBlocks, part_.get(), hcol_.get() + nv, nullptr, 1, flag, 1);
       PMB_CHECK_LAUNCH();
       scale_kernel<<<gv, 256, 0, s_>>>(n, wv_.get(), hcol_.get() + nv, V_.get() + (size_t)(j + 1) * ld_);
