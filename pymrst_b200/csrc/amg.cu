@@ -902,11 +902,13 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
       L.col = L.own_col.get();
     }
     {
-      // padded copy: W covers 99% of the rows, longer rows overflow; kept
-      // when it costs at most three times the CSR entries
-      static const bool padded_on = [] {
+      // padded copy (opt-in, PMB_AMG_PADDED): W covers 99% of the rows,
+      // longer rows overflow.  1: levels whose W is at most 1.25 times the
+      // mean row length plus one; 2: level 0 only.  The lanes per row follow
+      // the mean row length, as for the CSR kernels.
+      static const int padded_mode = [] {
         const char* e = std::getenv("PMB_AMG_PADDED");
-        return !(e && e[0] == '0');
+        return e ? std::atoi(e) : 0;
       }();
       const std::vector<int>& rp = h.row_ptr;
       const std::vector<int>& col = h.col;
@@ -926,7 +928,9 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
       W = std::max(W, 1);
       const long long padded = (long long)L.n * W;
       L.W = 0;
-      if (padded_on && W <= 64 && padded <= 3LL * std::max(L.nnz, 1)) {
+      const double mean_len = (double)L.nnz / std::max(L.n, 1);
+      const bool want = (padded_mode == 1 && W <= 1.25 * mean_len + 1.0) || (padded_mode == 2 && l == 0);
+      if (want && W <= 64) {
         std::vector<int> pc(padded), psrc(padded, -1), optr(1, 0), oc, osrc;
         for (int i = 0; i < L.n; ++i) {
           const int k0 = rp[i], k1 = rp[i + 1], len = k1 - k0;
@@ -957,7 +961,7 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
         }
         L.W = W;
       }
-      L.lanes = lanes_for(L.n, L.W > 0 ? padded : L.nnz);
+      L.lanes = lanes_for(L.n, L.nnz);
     }
     {
       // restriction plan: consecutive aggregates while their members fit
