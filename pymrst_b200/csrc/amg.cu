@@ -234,64 +234,6 @@ __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
-// The rows of a level's matrix as the row-wise kernels read them; dot<LANES>
-// returns lane `sub`'s part of sum_k a_ik f(col_k) (f maps a column to its x
-// value).
-//
-// CsrRows: entries rp[i] .. rp[i+1]; the row start is a load that every
-// entry's load waits on.
-template <class T>
-struct CsrRows {
-  const int* __restrict__ rp;
-  const int* __restrict__ ci;
-  const T* __restrict__ a;
-  template <int LANES, class F>
-  __device__ __forceinline__ double dot(long long i, int sub, F f) const {
-    double s = 0.0;
-    for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s += (double)a[k] * f(ci[k]);
-    return s;
-  }
-};
-
-// PadRows: every row padded to W entries at i * W (padding: value 0, column
-// i), so an entry's position is known without a load.  A row longer than W
-// keeps its first W - 1 entries there; its last slot holds column -(o + 1),
-// and the rest of the row is overflow list o: entries optr[o] .. optr[o+1].
-template <class T>
-struct PadRows {
-  int W;
-  const int* __restrict__ pc;
-  const T* __restrict__ pa;
-  const int* __restrict__ optr;
-  const int* __restrict__ oc;
-  const T* __restrict__ oa;
-  template <int LANES, class F>
-  __device__ __forceinline__ double dot(long long i, int sub, F f) const {
-    double s = 0.0;
-    const long long base = i * W;
-    for (int q = sub; q < W; q += LANES) {
-      const int c = pc[base + q];
-      if (c >= 0) {
-        s += (double)pa[base + q] * f(c);
-      } else {
-        const int o = -c - 1;
-        for (int k = optr[o]; k < optr[o + 1]; ++k) s += (double)oa[k] * f(oc[k]);
-      }
-    }
-    return s;
-  }
-};
-
-// dst[i] = src[idx[i]] (zero where idx is -1): the padded values from CSR.
-template <class T>
-__global__ void pad_gather_kernel(long long n, const int* __restrict__ idx, const T* __restrict__ src,
-                                  T* __restrict__ dst) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int k = idx[i];
-  dst[i] = k >= 0 ? src[k] : T(0);
-}
-
 // Calls f(std::integral_constant<int, L>) with L the row-group width.
 template <class F>
 void with_lanes(int lanes, F&& f) {
@@ -303,16 +245,6 @@ void with_lanes(int lanes, F&& f) {
     case 2: f(std::integral_constant<int, 2>{}); break;
     default: f(std::integral_constant<int, 1>{}); break;
   }
-}
-
-// Calls f(rows) with the level's row accessor: PadRows when it has a padded
-// copy, else CsrRows.
-template <class T, class F>
-void with_rows(const AMGLevel<T>& L, F&& f) {
-  if (L.W > 0)
-    f(PadRows<T>{L.W, L.pc.get(), L.pa.get(), L.optr.get(), L.oc.get(), L.oa.get()});
-  else
-    f(CsrRows<T>{L.row_ptr, L.col, L.val.get()});
 }
 
 // Row-group width for a level: about two entries of the row per lane.
@@ -356,8 +288,9 @@ __device__ __forceinline__ double cheb_x(const T* __restrict__ xin, const int* _
   return (double)(T)((double)xin[j] + (double)xc[agg[j]]);
 }
 
-template <class T, bool ZERO, int LANES, bool PRO = false, class R = CsrRows<T>>
-__global__ void __launch_bounds__(256) cheb_step_kernel(int n, R rows, const T* __restrict__ dinv,
+template <class T, bool ZERO, int LANES, bool PRO = false>
+__global__ void __launch_bounds__(256) cheb_step_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                                        const T* __restrict__ a, const T* __restrict__ dinv,
                                                         const T* __restrict__ b, const T* __restrict__ xin,
                                                         T* __restrict__ xout, T* __restrict__ d, const double* lmax,
                                                         int step, const int* __restrict__ agg = nullptr,
@@ -370,7 +303,9 @@ __global__ void __launch_bounds__(256) cheb_step_kernel(int n, R rows, const T* 
   const int sub = (int)(t % LANES);
   double ax = 0.0;
   if (!ZERO) {
-    if (i < n) ax = rows.template dot<LANES>(i, sub, [&](int c) { return cheb_x<T, PRO>(xin, agg, xc, c); });
+    if (i < n)
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES)
+        ax += (double)a[k] * cheb_x<T, PRO>(xin, agg, xc, ci[k]);
     ax = group_sum<LANES>(ax);
   }
   __syncthreads();
@@ -384,11 +319,12 @@ __global__ void __launch_bounds__(256) cheb_step_kernel(int n, R rows, const T* 
 
 // b_c[I] = sum over members i of (b_i - (A x)_i); LANES threads per aggregate
 // share each member row.
-template <class T, int LANES, class R = CsrRows<T>>
+template <class T, int LANES>
 __global__ void __launch_bounds__(256) restrict_residual_kernel(int nc, const int* __restrict__ cptr,
-                                                                const int* __restrict__ cmem, R rows,
-                                                                const T* __restrict__ b, const T* __restrict__ x,
-                                                                T* __restrict__ bc) {
+                                                                const int* __restrict__ cmem,
+                                                                const int* __restrict__ rp, const int* __restrict__ ci,
+                                                                const T* __restrict__ a, const T* __restrict__ b,
+                                                                const T* __restrict__ x, T* __restrict__ bc) {
   pdl_enter();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long I = t / LANES;
@@ -398,7 +334,7 @@ __global__ void __launch_bounds__(256) restrict_residual_kernel(int nc, const in
     for (int m = cptr[I]; m < cptr[I + 1]; ++m) {
       const int i = cmem[m];
       if (sub == 0) s += (double)b[i];
-      s -= rows.template dot<LANES>(i, sub, [&](int c) { return (double)x[c]; });
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s -= (double)a[k] * (double)x[ci[k]];
     }
   s = group_sum<LANES>(s);
   if (I < nc && sub == 0) bc[I] = (T)s;
@@ -412,11 +348,12 @@ __global__ void __launch_bounds__(256) restrict_residual_kernel(int nc, const in
 // members in member order.  The member loop of restrict_residual_kernel
 // waits on a chain of dependent loads (member, row start, column, x) per
 // member; here the chains of all members overlap.
-template <class T, int LANES, class R = CsrRows<T>>
+template <class T, int LANES>
 __global__ void __launch_bounds__(256) restrict_rows_kernel(const int* __restrict__ blk, const int* __restrict__ cptr,
-                                                            const int* __restrict__ cmem, R rows,
-                                                            const T* __restrict__ b, const T* __restrict__ x,
-                                                            T* __restrict__ bc) {
+                                                            const int* __restrict__ cmem,
+                                                            const int* __restrict__ rp, const int* __restrict__ ci,
+                                                            const T* __restrict__ a, const T* __restrict__ b,
+                                                            const T* __restrict__ x, T* __restrict__ bc) {
   pdl_enter();
   extern __shared__ double rr_smem[];
   const int I0 = blk[blockIdx.x], I1 = blk[blockIdx.x + 1];
@@ -429,7 +366,7 @@ __global__ void __launch_bounds__(256) restrict_rows_kernel(const int* __restric
     double s = 0.0;
     if (m < m1) {
       i = cmem[m];
-      s = -rows.template dot<LANES>(i, sub, [&](int c) { return (double)x[c]; });
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s -= (double)a[k] * (double)x[ci[k]];
     }
     s = group_sum<LANES>(s);
     if (m < m1 && sub == 0) rr_smem[m - m0] = (double)b[i] + s;
@@ -782,14 +719,17 @@ __global__ void __launch_bounds__(256) amg_fused_cycle_kernel(const CoopLevel<T>
 
 // K-cycle pieces ------------------------------------------------------------
 
-template <class T, int LANES, class R = CsrRows<T>>
-__global__ void __launch_bounds__(256) csr_spmv_kernel(int n, R rows, const T* __restrict__ x, T* __restrict__ y) {
+template <class T, int LANES>
+__global__ void __launch_bounds__(256) csr_spmv_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                                       const T* __restrict__ a, const T* __restrict__ x,
+                                                       T* __restrict__ y) {
   pdl_enter();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long i = t / LANES;
   const int sub = (int)(t % LANES);
   double s = 0.0;
-  if (i < n) s = rows.template dot<LANES>(i, sub, [&](int c) { return (double)x[c]; });
+  if (i < n)
+    for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s += (double)a[k] * (double)x[ci[k]];
   s = group_sum<LANES>(s);
   if (i < n && sub == 0) y[i] = (T)s;
 }
@@ -901,68 +841,7 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
       L.row_ptr = L.own_row_ptr.get();
       L.col = L.own_col.get();
     }
-    {
-      // padded copy (opt-in, PMB_AMG_PADDED): W covers 99% of the rows,
-      // longer rows overflow.  1: levels whose W is at most 1.25 times the
-      // mean row length plus one; 2: level 0 only.  The lanes per row follow
-      // the mean row length, as for the CSR kernels.
-      static const int padded_mode = [] {
-        const char* e = std::getenv("PMB_AMG_PADDED");
-        return e ? std::atoi(e) : 0;
-      }();
-      const std::vector<int>& rp = h.row_ptr;
-      const std::vector<int>& col = h.col;
-      int maxlen = 0;
-      for (int i = 0; i < L.n; ++i) maxlen = std::max(maxlen, rp[i + 1] - rp[i]);
-      std::vector<long long> hist(maxlen + 1, 0);
-      for (int i = 0; i < L.n; ++i) ++hist[rp[i + 1] - rp[i]];
-      int W = maxlen;
-      long long covered = 0;
-      for (int w = 0; w <= maxlen; ++w) {
-        covered += hist[w];
-        if (covered * 100 >= 99LL * L.n) {
-          W = w;
-          break;
-        }
-      }
-      W = std::max(W, 1);
-      const long long padded = (long long)L.n * W;
-      L.W = 0;
-      const double mean_len = (double)L.nnz / std::max(L.n, 1);
-      const bool want = (padded_mode == 1 && W <= 1.25 * mean_len + 1.0) || (padded_mode == 2 && l == 0);
-      if (want && W <= 64) {
-        std::vector<int> pc(padded), psrc(padded, -1), optr(1, 0), oc, osrc;
-        for (int i = 0; i < L.n; ++i) {
-          const int k0 = rp[i], k1 = rp[i + 1], len = k1 - k0;
-          const long long base = (long long)i * W;
-          const int kept = len <= W ? len : W - 1;
-          for (int q = 0; q < kept; ++q) {
-            pc[base + q] = col[k0 + q];
-            psrc[base + q] = k0 + q;
-          }
-          for (int q = kept; q < W; ++q) pc[base + q] = i;
-          if (len > W) {
-            pc[base + W - 1] = -(int)optr.size();  // -(o + 1), o = optr.size() - 1
-            for (int k = k0 + W - 1; k < k1; ++k) {
-              oc.push_back(col[k]);
-              osrc.push_back(k);
-            }
-            optr.push_back((int)oc.size());
-          }
-        }
-        L.pc.upload(pc, s);
-        L.psrc.upload(psrc, s);
-        L.pa.resize(padded);
-        if (!oc.empty()) {
-          L.optr.upload(optr, s);
-          L.oc.upload(oc, s);
-          L.osrc.upload(osrc, s);
-          L.oa.resize(oc.size());
-        }
-        L.W = W;
-      }
-      L.lanes = lanes_for(L.n, L.nnz);
-    }
+    L.lanes = lanes_for(L.n, L.nnz);
     {
       // restriction plan: consecutive aggregates while their members fit
       // one per lane group
@@ -1034,16 +913,6 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
   coop_status_ = d_status;
   for (size_t l = 0; l < levels_.size(); ++l) {
     AMGLevel<T>& L = levels_[l];
-    if (L.W > 0) {  // this level's CSR values are final here (level 0 from the caller)
-      const long long np = (long long)L.n * L.W;
-      pad_gather_kernel<T><<<grid_for(np, 256), 256, 0, s>>>(np, L.psrc.get(), L.val.get(), L.pa.get());
-      PMB_CHECK_LAUNCH();
-      if (L.oa.size()) {
-        const long long no = (long long)L.oa.size();
-        pad_gather_kernel<T><<<grid_for(no, 256), 256, 0, s>>>(no, L.osrc.get(), L.val.get(), L.oa.get());
-        PMB_CHECK_LAUNCH();
-      }
-    }
     PMB_CUDA(cudaMemsetAsync(bits_.get() + l, 0, sizeof(unsigned long long), s));
     diag_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(),
                                                        bits_.get() + l, d_status);
@@ -1079,30 +948,27 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
   with_lanes(L.lanes, [&](auto ln) {
     constexpr int LN = decltype(ln)::value;
     const int g = grid_for((long long)L.n * LN, 256);
-    with_rows(L, [&](auto rows) {
-      using R = decltype(rows);
-      if (zero_start) {
-        T* out = (steps % 2 == 1) ? x : t;
-        launch_pdl(cheb_step_kernel<T, true, LN, false, R>, g, 256, 0, s, L.n, rows, (const T*)L.dinv.get(), b,
-                   (const T*)nullptr, out, L.r.get(), (const double*)L.lmax.get(), 0, (const int*)nullptr,
-                   (const T*)nullptr);
-        cur = out;
-        step = 1;
-      }
-      for (; step < steps; ++step) {
-        T* out = out_for(step);
-        if (out == cur) out = u;
-        if (xc && step == 0)  // x + P xc, folded into the first step
-          launch_pdl(cheb_step_kernel<T, false, LN, true, R>, g, 256, 0, s, L.n, rows, (const T*)L.dinv.get(), b,
-                     (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step, (const int*)L.agg.get(),
-                     xc);
-        else
-          launch_pdl(cheb_step_kernel<T, false, LN, false, R>, g, 256, 0, s, L.n, rows, (const T*)L.dinv.get(), b,
-                     (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step, (const int*)nullptr,
-                     (const T*)nullptr);
-        cur = out;
-      }
-    });
+    if (zero_start) {
+      T* out = (steps % 2 == 1) ? x : t;
+      launch_pdl(cheb_step_kernel<T, true, LN>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
+                 (const T*)L.dinv.get(), b, (const T*)nullptr, out, L.r.get(), (const double*)L.lmax.get(), 0,
+                 (const int*)nullptr, (const T*)nullptr);
+      cur = out;
+      step = 1;
+    }
+    for (; step < steps; ++step) {
+      T* out = out_for(step);
+      if (out == cur) out = u;
+      if (xc && step == 0)  // x + P xc, folded into the first step
+        launch_pdl(cheb_step_kernel<T, false, LN, true>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
+                   (const T*)L.dinv.get(), b, (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step,
+                   (const int*)L.agg.get(), xc);
+      else
+        launch_pdl(cheb_step_kernel<T, false, LN>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
+                   (const T*)L.dinv.get(), b, (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step,
+                   (const int*)nullptr, (const T*)nullptr);
+      cur = out;
+    }
   });
   if (cur != x) {
     launch_pdl(copy_kernel<T>, grid_for(L.n, 256), 256, 0, s, L.n, (const T*)cur, x);
@@ -1242,15 +1108,14 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
     }();
     with_lanes(L.lanes, [&](auto ln) {
       constexpr int LN = decltype(ln)::value;
-      with_rows(L, [&](auto rows) {
-        using R = decltype(rows);
-        if (by_rows)
-          launch_pdl(restrict_rows_kernel<T, LN, R>, L.rblocks, 256, L.rsmem, s, (const int*)L.rblk.get(),
-                     (const int*)L.cptr.get(), (const int*)L.cmem.get(), rows, b, (const T*)x, bc);
-        else
-          launch_pdl(restrict_residual_kernel<T, LN, R>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
-                     (const int*)L.cptr.get(), (const int*)L.cmem.get(), rows, b, (const T*)x, bc);
-      });
+      if (by_rows)
+        launch_pdl(restrict_rows_kernel<T, LN>, L.rblocks, 256, L.rsmem, s, (const int*)L.rblk.get(),
+                   (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
+                   (const T*)x, bc);
+      else
+        launch_pdl(restrict_residual_kernel<T, LN>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
+                   (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
+                   (const T*)x, bc);
     });
   }
   coarse_correction(l, bc, xc, s);
@@ -1283,10 +1148,8 @@ void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
     PhaseTimer pt(level_phase(l + 1, 3), s);
     with_lanes(C.lanes, [&](auto ln) {
       constexpr int LN = decltype(ln)::value;
-      with_rows(C, [&](auto rows) {
-        launch_pdl(csr_spmv_kernel<T, LN, decltype(rows)>, grid_for((long long)n * LN, 256), 256, 0, s, n, rows,
-                   (const T*)C.kc1.get(), C.kv1.get());
-      });
+      launch_pdl(csr_spmv_kernel<T, LN>, grid_for((long long)n * LN, 256), 256, 0, s, n, C.row_ptr, C.col,
+                 (const T*)C.val.get(), (const T*)C.kc1.get(), C.kv1.get());
     });
     launch_pdl(kdots_kernel<T, 2>, G, 256, 0, s, n, (const T*)C.kv1.get(), (const T*)nullptr, rc, C.kpart.get());
     launch_pdl(kcoef_kernel, 1, 160, 0, s, G, 0, (const double*)C.kpart.get(), C.kcoef.get());
@@ -1297,10 +1160,8 @@ void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
   PhaseTimer pt(level_phase(l + 1, 3), s);
   with_lanes(C.lanes, [&](auto ln) {
     constexpr int LN = decltype(ln)::value;
-    with_rows(C, [&](auto rows) {
-      launch_pdl(csr_spmv_kernel<T, LN, decltype(rows)>, grid_for((long long)n * LN, 256), 256, 0, s, n, rows,
-                 (const T*)C.kc2.get(), C.kv2.get());
-    });
+    launch_pdl(csr_spmv_kernel<T, LN>, grid_for((long long)n * LN, 256), 256, 0, s, n, C.row_ptr, C.col,
+               (const T*)C.val.get(), (const T*)C.kc2.get(), C.kv2.get());
   });
   launch_pdl(kdots_kernel<T, 5>, G, 256, 0, s, n, (const T*)C.kv1.get(), (const T*)C.kv2.get(), rc,
              C.kpart.get());

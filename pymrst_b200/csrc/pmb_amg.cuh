@@ -54,13 +54,6 @@ struct AMGLevel {
   DArray<int> rblk;
   int rblocks = 0;
   size_t rsmem = 0;
-  // Padded copy of the matrix read by the cycle's row-wise kernels (W > 0):
-  // W entries per row (pc columns, pa values, psrc their CSR positions or -1
-  // for padding) and the overflow lists of longer rows (optr, oc, oa; osrc
-  // CSR positions).  Values are gathered from val at every refresh.
-  int W = 0;
-  DArray<int> pc, psrc, optr, oc, osrc;
-  DArray<T> pa, oa;
 };
 
 // One level as seen by the fused coarse-cycle kernel.
