@@ -843,6 +843,14 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
     }
     L.lanes = lanes_for(L.n, L.nnz);
     {
+      // levels below the K-cycle levels may smooth with a lower degree
+      static const int coarse_degree = [] {
+        const char* e = std::getenv("PMB_AMG_COARSE_DEGREE");
+        return e ? std::atoi(e) : 0;
+      }();
+      L.degree = ((int)l >= k_levels && coarse_degree > 0) ? coarse_degree : 0;
+    }
+    {
       // restriction plan: consecutive aggregates while their members fit
       // one per lane group
       const int groups = 256 / L.lanes;
@@ -939,7 +947,7 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
   // writes x; the first step of an odd count from a non-zero start, which
   // would overwrite its own input, writes L.u instead.  Only a single step
   // from a non-zero start needs a copy.
-  const int steps = std::max(1, degree);
+  const int steps = std::max(1, L.degree > 0 ? L.degree : degree);
   T* t = L.t.get();
   T* u = L.u.get();
   auto out_for = [&](int k) -> T* { return ((steps - 1 - k) % 2 == 0) ? x : t; };

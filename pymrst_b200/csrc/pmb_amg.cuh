@@ -54,6 +54,7 @@ struct AMGLevel {
   DArray<int> rblk;
   int rblocks = 0;
   size_t rsmem = 0;
+  int degree = 0;  // Chebyshev degree of this level; 0: the hierarchy's
 };
 
 // One level as seen by the fused coarse-cycle kernel.
