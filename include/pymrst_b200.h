@@ -189,12 +189,14 @@ typedef struct pmb_cpr_opts {
   int32_t replay_graph;     /* 1: the preconditioner is captured once and replayed as a CUDA
                                graph; 0: its kernels are launched directly (for callers
                                that drive several solvers from concurrent host threads) */
+  int32_t amg_coarse_degree; /* Chebyshev degree on the levels below the K-cycle levels;
+                                0: amg_smoother_degree */
 } pmb_cpr_opts;
 
 /* Defaults: rtol 1e-8, maxiter 200, restart 50 (CPRSolver's,
  * linear_solvers.py:113-116); local_sweeps 4, Chebyshev degree 2, K-cycle on
  * 3 levels, theta 0.1, coarse size 200, re-aggregation every 8 setups,
- * graph replay on. */
+ * graph replay on, coarse degree 0 (the smoother degree on every level). */
 int pmb_cpr_default_opts(pmb_cpr_opts* out);
 int pmb_cpr_create(pmb_ow* model, const pmb_cpr_opts* opts, pmb_cpr** out);
 int pmb_cpr_destroy(pmb_cpr* s);

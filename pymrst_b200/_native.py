@@ -46,6 +46,7 @@ class CPROpts(C.Structure):
         ("use_pressure_stage", c_int), ("local_sweeps", c_int), ("amg_smoother_degree", c_int),
         ("amg_cycle", c_int), ("amg_theta", c_dbl), ("amg_coarse_size", c_int),
         ("amg_rebuild_interval", c_int), ("inner_rtol", c_dbl), ("replay_graph", c_int),
+        ("amg_coarse_degree", c_int),
     ]
 
 

@@ -842,14 +842,7 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
       L.col = L.own_col.get();
     }
     L.lanes = lanes_for(L.n, L.nnz);
-    {
-      // levels below the K-cycle levels may smooth with a lower degree
-      static const int coarse_degree = [] {
-        const char* e = std::getenv("PMB_AMG_COARSE_DEGREE");
-        return e ? std::atoi(e) : 0;
-      }();
-      L.degree = ((int)l >= k_levels && coarse_degree > 0) ? coarse_degree : 0;
-    }
+    L.degree = ((int)l >= k_levels && coarse_degree > 0) ? coarse_degree : 0;
     {
       // restriction plan: consecutive aggregates while their members fit
       // one per lane group

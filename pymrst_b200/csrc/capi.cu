@@ -319,6 +319,7 @@ int pmb_cpr_default_opts(pmb_cpr_opts* o) {
     o->amg_rebuild_interval = 8;
     o->inner_rtol = 1e-4;
     o->replay_graph = 1;
+    o->amg_coarse_degree = 0;
   });
 }
 

@@ -837,6 +837,7 @@ CPRSolver::CPRSolver(OWModel& m, const pmb_cpr_opts& o) : m_(m), o_(o), s_(m.str
   st_pin_.resize(1);
   st_pin_[0] = 0;
   amg_.degree = amg32_.degree = std::max(1, o_.amg_smoother_degree);
+  amg_.coarse_degree = amg32_.coarse_degree = std::max(0, o_.amg_coarse_degree);
   amg_.k_levels = amg32_.k_levels = std::max(0, o_.amg_cycle);
   if (f32_) {
     if (m.has_lines() && !use_ell_) jac32_.resize(4LL * m.nnzb());

@@ -466,6 +466,7 @@ CsrCPR::CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, bool t
   st_pin_.resize(1);
   st_pin_[0] = 0;
   amg_.degree = amg32_.degree = std::max(1, o_.amg_smoother_degree);
+  amg_.coarse_degree = amg32_.coarse_degree = std::max(0, o_.amg_coarse_degree);
   amg_.k_levels = amg32_.k_levels = std::max(0, o_.amg_cycle);
   kry_.init(n, o_.restart, s_);
   PMB_CUDA(cudaStreamSynchronize(s_));

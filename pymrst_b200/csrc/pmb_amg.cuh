@@ -95,6 +95,7 @@ class AMG {
   int num_levels() const { return (int)levels_.size() + (nco_ > 0 ? 1 : 0); }
   int level_size(int l) const { return l < (int)levels_.size() ? levels_[l].n : nco_; }
   int degree = 2;
+  int coarse_degree = 0;  // degree below the K-cycle levels (0: degree)
   // Run the levels below the K-cycle levels, down to the dense coarsest
   // solve, as one cooperative kernel when they are small (set before build;
   // also needs PMB_FUSED_COARSE=1 in the environment).
