@@ -762,11 +762,12 @@ __global__ void __launch_bounds__(256) kdots_kernel(int n, const T* __restrict__
   }
 }
 
-// mode 0: coef[0] = (v1.rc)/(v1.v1); mode 1: least-squares pair
-// [coef[1], coef[2]] minimising |rc - y0 v1 - y1 v2|.  One warp sums each
-// dot's G block partials; launched with 5 warps.
-__global__ void kcoef_kernel(int G, int mode, const double* __restrict__ part, double* __restrict__ coef) {
-  pdl_enter();
+// The coefficients of one K-cycle step from the kdots partials, into c
+// (shared memory): mode 0: c[0] = (v1.rc)/(v1.v1); mode 1: the least-squares
+// pair [c[1], c[2]] minimising |rc - y0 v1 - y1 v2|.  One warp sums each
+// dot's G block partials, in the same order in every CTA, so that every CTA
+// gets the same values.  Needs at least 5 warps.
+__device__ __forceinline__ void kcoef_block(int G, int mode, const double* __restrict__ part, double* c) {
   __shared__ double d[5];
   const int nd = mode == 0 ? 2 : 5;
   const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
@@ -777,38 +778,44 @@ __global__ void kcoef_kernel(int G, int mode, const double* __restrict__ part, d
     if (lane == 0) d[q] = s;
   }
   __syncthreads();
-  if (threadIdx.x != 0) return;
-  if (mode == 0) {
-    coef[0] = d[0] > 0.0 ? d[1] / d[0] : 0.0;
-  } else {
-    const double a11 = d[0], a12 = d[1], a22 = d[2], r1 = d[3], r2 = d[4];
-    const double det = a11 * a22 - a12 * a12;
-    if (det > 1e-14 * a11 * a22 && isfinite(det)) {
-      coef[1] = (a22 * r1 - a12 * r2) / det;
-      coef[2] = (a11 * r2 - a12 * r1) / det;
+  if (threadIdx.x == 0) {
+    if (mode == 0) {
+      c[0] = d[0] > 0.0 ? d[1] / d[0] : 0.0;
     } else {
-      coef[1] = a11 > 0.0 ? r1 / a11 : 0.0;
-      coef[2] = 0.0;
+      const double a11 = d[0], a12 = d[1], a22 = d[2], r1 = d[3], r2 = d[4];
+      const double det = a11 * a22 - a12 * a12;
+      if (det > 1e-14 * a11 * a22 && isfinite(det)) {
+        c[1] = (a22 * r1 - a12 * r2) / det;
+        c[2] = (a11 * r2 - a12 * r1) / det;
+      } else {
+        c[1] = a11 > 0.0 ? r1 / a11 : 0.0;
+        c[2] = 0.0;
+      }
     }
   }
+  __syncthreads();
 }
 
-// out = a - coef[0] * b
+// out = a - c0 b, c0 = (v1.rc)/(v1.v1) from the kdots partials
 template <class T>
-__global__ void kaxpy_kernel(int n, const T* __restrict__ a, const T* __restrict__ b, const double* __restrict__ coef,
-                             T* __restrict__ out) {
+__global__ void __launch_bounds__(256) kaxpy_kernel(int n, const T* __restrict__ a, const T* __restrict__ b, int G,
+                                                    const double* __restrict__ part, T* __restrict__ out) {
   pdl_enter();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = (T)((double)a[i] - coef[0] * (double)b[i]);
+  __shared__ double c[3];
+  kcoef_block(G, 0, part, c);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = (T)((double)a[i] - c[0] * (double)b[i]);
 }
 
-// out = coef[1] c1 + coef[2] c2
+// out = y0 c1 + y1 c2, (y0, y1) the least-squares pair from the kdots partials
 template <class T>
-__global__ void kcombine_kernel(int n, const T* __restrict__ c1, const T* __restrict__ c2,
-                                const double* __restrict__ coef, T* __restrict__ out) {
+__global__ void __launch_bounds__(256) kcombine_kernel(int n, const T* __restrict__ c1, const T* __restrict__ c2,
+                                                       int G, const double* __restrict__ part, T* __restrict__ out) {
   pdl_enter();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = (T)(coef[1] * (double)c1[i] + coef[2] * (double)c2[i]);
+  __shared__ double c[3];
+  kcoef_block(G, 1, part, c);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = (T)(c[1] * (double)c1[i] + c[2] * (double)c2[i]);
 }
 
 // ---------------------------------------------------------------------------
@@ -883,7 +890,6 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
       L.kv2.resize(L.n);
       L.kr2.resize(L.n);
       L.kpart.resize(5 * 2 * kNumSM);
-      L.kcoef.resize(3);
     }
   }
   const AMGHostLevel& c = H.back();
@@ -1153,8 +1159,7 @@ void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
                  (const T*)C.val.get(), (const T*)C.kc1.get(), C.kv1.get());
     });
     launch_pdl(kdots_kernel<T, 2>, G, 256, 0, s, n, (const T*)C.kv1.get(), (const T*)nullptr, rc, C.kpart.get());
-    launch_pdl(kcoef_kernel, 1, 160, 0, s, G, 0, (const double*)C.kpart.get(), C.kcoef.get());
-    launch_pdl(kaxpy_kernel<T>, g, 256, 0, s, n, rc, (const T*)C.kv1.get(), (const double*)C.kcoef.get(),
+    launch_pdl(kaxpy_kernel<T>, G, 256, 0, s, n, rc, (const T*)C.kv1.get(), G, (const double*)C.kpart.get(),
                C.kr2.get());
   }
   cycle(l + 1, C.kr2.get(), C.kc2.get(), s);
@@ -1166,9 +1171,8 @@ void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
   });
   launch_pdl(kdots_kernel<T, 5>, G, 256, 0, s, n, (const T*)C.kv1.get(), (const T*)C.kv2.get(), rc,
              C.kpart.get());
-  launch_pdl(kcoef_kernel, 1, 160, 0, s, G, 1, (const double*)C.kpart.get(), C.kcoef.get());
-  launch_pdl(kcombine_kernel<T>, g, 256, 0, s, n, (const T*)C.kc1.get(), (const T*)C.kc2.get(),
-             (const double*)C.kcoef.get(), ec);
+  launch_pdl(kcombine_kernel<T>, G, 256, 0, s, n, (const T*)C.kc1.get(), (const T*)C.kc2.get(), G,
+             (const double*)C.kpart.get(), ec);
 }
 
 template <class T>

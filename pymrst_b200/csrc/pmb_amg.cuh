@@ -44,7 +44,7 @@ struct AMGLevel {
   DArray<int> own_row_ptr, own_col;
   DArray<T> val, dinv, x, b, r, t, u;  // u: first output of an odd smoothing count
   DArray<T> kc1, kc2, kv1, kv2, kr2;  // K-cycle vectors of this level (as a coarse level)
-  DArray<double> kpart, kcoef;        // K-cycle reduction partials and coefficients
+  DArray<double> kpart;               // K-cycle reduction partials
   DArray<int> agg, cptr, cmem, gptr, gidx;
   DArray<double> lmax;  // Chebyshev upper bound (device scalar)
   // Restriction plan: CTA b of restrict_rows_kernel takes the aggregates
