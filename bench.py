@@ -59,6 +59,7 @@ def parse():
                     help="mixed: FP32 AMG and smoother blocks inside the FP64 FGMRES (the benchmark's method); fp64: all FP64")
     ap.add_argument("--dims", default=None, help="override grid dims, e.g. 30,110,40")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison arm")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--cpr", default="", help="CPR option overrides, e.g. amg_cycle=2,local_sweeps=1")
     ap.add_argument("--probe", type=int, default=0,
@@ -249,7 +250,10 @@ def kernel_roofline(model, x, x0, dt, torch, N, reps=20):
     sweep_bytes = nnzb * blk + max(nnzb - 3 * nc, 0) * 4 + nc * (16 + 32 + 4)
     out["line_gs_sweep"] = dict(seconds=ms.value * 1e-3 / sweeps, bytes=sweep_bytes)
     N.check(N.lib().pmb_cpr_time_stage(s, 1, N.ptr(res), N.ptr(z), reps, N.C.byref(ms)))
-    out["amg_cycle"] = dict(seconds=ms.value * 1e-3, bytes=None)
+    cb = (N.C.c_double * 8)()
+    N.check(N.lib().pmb_cpr_bytes(s, cb))
+    out["amg_cycle"] = dict(seconds=ms.value * 1e-3, bytes=float(cb[0]))
+    out["cpr_bytes"] = [float(v) for v in cb]
     return out
 
 
@@ -261,6 +265,7 @@ def run_ours(args):
     from pymrst_b200.build import build
     from pymrst_b200.ow_model import GpuOilWaterModel
     from pymrst_b200.replicas import reduce_timing
+    from pymrst_b200.schedule import run_report_step
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -301,7 +306,6 @@ def run_ours(args):
                              cpr_options=copts, max_iterations=args.max_newton)
     stream = torch.cuda.current_stream()
     x = model.to_device(model.initial_state(case.p0, case.sw0))
-    backup = x.clone()
     dt = case.dt
     if args.probe:
         model.max_iterations = args.probe
@@ -313,32 +317,46 @@ def run_ours(args):
                               "amg_levels": model.cpr_levels()}), flush=True)
         return
 
-    def one_step(xv):
-        """One report step with the reference's halving cuts; returns
-        (Newton iterations, Krylov iterations, cuts)."""
-        t_local, its, kry, cuts, h = 0.0, 0, 0, 0, dt
-        while t_local < dt - 1e-12 * dt:
-            h = min(h, dt - t_local)
-            backup.copy_(xv)
-            ok, nit, st = model.step_device(xv, h)
-            its += nit
-            kry += int(st[2])
-            if os.environ.get("PMB_VERBOSE") == "1":
-                print(f"# step dt={h / 86400:.3g} d ok={ok} newton={nit} krylov={int(st[2])} "
-                      f"cnv={st[4]:.2e} mb={st[5]:.2e} {getattr(model, 'last_failure', '') if not ok else ''}",
-                      file=sys.stderr, flush=True)
-            if ok:
-                t_local += h
-                h = min(2 * h, dt - t_local) if cuts else h
-            else:
-                xv.copy_(backup)
-                cuts += 1
-                if cuts > 6:
-                    raise RuntimeError("timestep failed after 6 cuts")
-                h /= 2
-        return its, kry, cuts
+    def run_steps(mdl, xv, nsteps, snapshots=None, per_step=None):
+        """Report steps of the schedule with the reference's halving cuts
+        (schedule.run_report_step); returns (Newton its, Krylov its, cuts).
+        With `snapshots`, a device copy of the state after each report step
+        is kept (a device-to-device copy, about 10 us per step)."""
+        tot = [0, 0, 0]
+        saved = xv.clone()
+        for _ in range(nsteps):
+            kry = [0]
 
-    for _ in range(args.warmup):
+            def attempt(h):
+                saved.copy_(xv)
+                ok, nit, st = mdl.step_device(xv, h)
+                kry[0] += int(st[2])
+                if os.environ.get("PMB_VERBOSE") == "1":
+                    print(f"# step dt={h / 86400:.3g} d ok={ok} newton={nit} krylov={int(st[2])} "
+                          f"cnv={st[4]:.2e} mb={st[5]:.2e} {getattr(mdl, 'last_failure', '') if not ok else ''}",
+                          file=sys.stderr, flush=True)
+                if not ok:
+                    xv.copy_(saved)
+                return ok, nit
+
+            its, cuts = run_report_step(attempt, dt, max_cuts=6)
+            tot[0] += its
+            tot[1] += kry[0]
+            tot[2] += cuts
+            if snapshots is not None:
+                snapshots.append(xv.clone())
+            if per_step is not None:
+                per_step.append(its)
+        return tot
+
+    def one_step(xv):
+        i, k, c = run_steps(model, xv, 1)
+        return i, k, c
+
+    x_before_last = None
+    for i in range(args.warmup):
+        if i == args.warmup - 1:
+            x_before_last = x.clone()
         one_step(x)
     torch.cuda.synchronize()
     x_e2e_start = x.clone()
@@ -347,14 +365,10 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    its_total = kry_total = cuts_total = 0
+    snaps, its_steps = [], []
     with ClockSampler(local) as clocks:
         e0.record(stream)
-        for _ in range(args.steps):
-            i, k, c = one_step(x)
-            its_total += i
-            kry_total += k
-            cuts_total += c
+        its_total, kry_total, cuts_total = run_steps(model, x, args.steps, snaps, its_steps)
         e1.record(stream)
         torch.cuda.synchronize()
     if world > 1:
@@ -380,25 +394,77 @@ def run_ours(args):
     its_e2e = 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        # a report step through the public API (cuts handled like the driver)
-        t_local, h, cuts = 0.0, dt, 0
-        while t_local < dt - 1e-12 * dt:
-            h = min(h, dt - t_local)
-            new, ok, nit = model.step(st_host, h)
-            its_e2e += nit
+        # a report step through the public API, cuts as in the driver
+        holder = [st_host]
+
+        def attempt(h):
+            new, ok, nit = model.step(holder[0], h)
             if ok:
-                st_host = new
-                t_local += h
-                h = min(2 * h, dt - t_local) if cuts else h
-            else:
-                cuts += 1
-                h /= 2
+                holder[0] = new
+            return ok, nit
+
+        nit, _ = run_report_step(attempt, dt, max_cuts=6)
+        its_e2e += nit
+        st_host = holder[0]
     torch.cuda.synchronize()
     sec_e2e, cell_its_e2e = reduce_timing(time.perf_counter() - t0, float(its_e2e) * model.nc)
     nvec_bytes = model.sizes["nvec"] * 8
 
+    # The FP64 form of the same solve (every preconditioner array in FP64)
+    # from the same start state, timed the same way, and the difference of
+    # the mixed-precision states from it after every report step.
+    fp64 = None
+    if args.precision == "mixed" and not args.no_fp64:
+        copts64 = dict(copts, precision=0)
+        model64 = GpuOilWaterModel(case.grid, case.rock, case.fluid, case.wells, gravity=case.gravity,
+                                   cpr_options=copts64, max_iterations=args.max_newton)
+        # untimed: aggregation and graph capture on the last warm-up step, which
+        # also leaves the model's previous-step well pressure drops where the
+        # mixed run had them when its timed steps began
+        x64 = (x_before_last if x_before_last is not None else x_e2e_start).clone()
+        if x_before_last is not None:
+            run_steps(model64, x64, 1)
+        x64.copy_(x_e2e_start)
+        snaps64, its64 = [], []
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        n64, k64, c64 = run_steps(model64, x64, args.steps, snaps64, its64)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        sec64, cell_its64 = reduce_timing(f0.elapsed_time(f1) * 1e-3, float(n64) * model.nc)
+        nc2 = 2 * model.nc
+        errs = []
+        for a, b in zip(snaps, snaps64):
+            pa, pb = a[0:nc2:2], b[0:nc2:2]
+            errs.append((float((pa - pb).abs().max() / pb.abs().max()),
+                         float((a[1:nc2:2] - b[1:nc2:2]).abs().max())))
+        fp64 = {"value": cell_its64 / sec64, "ms_per_step": sec64 / args.steps * 1e3, "newton_iterations": n64,
+                "krylov_iterations": k64, "cuts": c64, "speedup_mixed_over_fp64": value / (cell_its64 / sec64)}
+        mixed_vs_fp64 = {"max_rel_pressure": max(e[0] for e in errs), "max_abs_sw": max(e[1] for e in errs),
+                         "per_step_rel_pressure": [e[0] for e in errs], "per_step_abs_sw": [e[1] for e in errs],
+                         "newton_per_step_mixed": its_steps, "newton_per_step_fp64": its64,
+                         "equal_newton_counts": its_steps == its64}
+        del model64, snaps64
+    del snaps
+
     kr = kernel_roofline(model, x, x_e2e_start, dt, torch, N)
     peak, peak_kind = peaks()
+    # whole-step algorithmic bytes from the recorded counts: per Newton
+    # iteration the assembly, the convergence check and update, and one
+    # preconditioner setup; per Krylov iteration the operator product, one
+    # preconditioner application (AMG cycle, restriction and prolongation,
+    # every second-stage sweep) and the Gram-Schmidt traffic at the mean
+    # iteration count per solve
+    cb = kr["cpr_bytes"]
+    nvec = cb[5]
+    m_it = kry_total / max(its_total, 1)
+    orth = its_total * (m_it * (m_it - 1) + 6 * m_it) * nvec * 8
+    sweeps = int(copts.get("local_sweeps", 1))
+    per_newton = kr["assemble"]["bytes"] + cb[4] + cb[6] + model.nc * 40 + nvec * 24
+    per_krylov = cb[2] + cb[0] + cb[3] + sweeps * cb[1]
+    step_bytes = (its_total * per_newton + kry_total * per_krylov + orth) / args.steps
+    step_ach = step_bytes / (sec / args.steps) / 1e9
     dom = kr["line_gs_sweep"]
     ach = dom["bytes"] / dom["seconds"] / 1e9
     # DRAM traffic of one line_pcr_ell_kernel launch (one colour, half the cells),
@@ -429,11 +495,17 @@ def run_ours(args):
                          "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes": dom["bytes"] / 2,
+                         "step": {"bytes_per_step": step_bytes, "achieved": step_ach, "frac": step_ach / peak,
+                                  "per_newton_bytes": per_newton, "per_krylov_bytes": per_krylov,
+                                  "orthogonalisation_bytes_per_step": orth / args.steps},
                          "kernels": {k: {"ms": v["seconds"] * 1e3, "bytes": v["bytes"],
                                          "GBps": (v["bytes"] / v["seconds"] / 1e9) if v["bytes"] else None}
-                                     for k, v in kr.items()}},
+                                     for k, v in kr.items() if k != "cpr_bytes"}},
             "clocks": clocks.summary(),
         }
+        if fp64 is not None:
+            line["fp64"] = fp64
+            line["mixed_vs_fp64"] = mixed_vs_fp64
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)

@@ -153,8 +153,10 @@ int pmb_ow_convergence(pmb_ow* h, const double* d_res, const double* d_x, double
  * h_fluid5 = [c_w, c_o, b0_w, b0_o, p_ref]; d_out4 (device) receives
  * [cnv, mb, non-finite cell count, 0], the cnv and mb of pmb_ow_convergence.
  * The first call on a device looks up the array's device address, so make
- * it before any stream capture.  Calls that overlap on the GPU share the
- * array and race. */
+ * it before any stream capture; the address is kept for the life of the
+ * process, so do not call it on a device after cudaDeviceReset() of that
+ * device.  d_res and d_x must be 16-byte aligned, d_pv and d_out4 8-byte
+ * aligned.  Calls that overlap on the GPU share the array and race. */
 int pmb_ow_cnv_mb_noalloc(int32_t nc, const double* d_res, const double* d_x, const double* d_pv,
                           double pv_total, const double* h_fluid5, double dt, double* d_out4,
                           void* stream);
@@ -213,6 +215,14 @@ int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* h_sizes, int32
  * after one untimed application).  stage 0: the second stage (all local
  * sweeps, updating d_z in place); 1: one AMG cycle on the restricted d_r;
  * 2: the whole preconditioner z = M^{-1} r.  Needs pmb_cpr_setup first. */
+/* Measurement aid, no counterpart in the reference: algorithmic bytes of the
+ * solver's launches on its current hierarchy (every array read or written
+ * once per launch, in its storage type), h_out8 = [one AMG cycle, one
+ * second-stage sweep, one operator product, the pressure restriction and
+ * prolongation of one preconditioner application, one setup without
+ * aggregation, the Krylov vector length, one AMG refresh, 0].  Needs
+ * pmb_cpr_setup first. */
+int pmb_cpr_bytes(const pmb_cpr* s, double* h_out8);
 int pmb_cpr_time_stage(pmb_cpr* s, int32_t stage, const double* d_r, double* d_z, int32_t reps,
                        double* h_ms);
 
@@ -293,6 +303,80 @@ int pmb_pcg_setup(pmb_pcg* p, const double* d_vals);
 int pmb_pcg_solve(pmb_pcg* p, const double* d_b, double* d_x, double rtol, int32_t maxiter,
                   double* h_info3);
 int pmb_pcg_levels(const pmb_pcg* p, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
+
+/* ------------------------------------------------------------------------
+ * Incompressible TPFA pressure system on the device (incomp_tpfa,
+ * pymrst/modules/incomp/incomp_tpfa.py:55-211).  The handle holds the grid
+ * topology and the well perforations; per call the caller gives the
+ * transmissibilities, phase mobilities and driving forces.
+ *
+ * Unknowns: nc cell pressures, then one bottom-hole pressure per well (the
+ * reference's ordering, :104-106).  The matrix is CSR on a pattern fixed at
+ * creation (pmb_tpfa_pattern): per cell row the diagonal, the cell across each
+ * interior interface, and the bhp of each rate well perforating the cell; per
+ * well row the perforated cells of a rate well and the diagonal.
+ */
+typedef struct pmb_tpfa pmb_tpfa;
+
+typedef struct pmb_tpfa_desc {
+  int32_t nc, nf, nhf, dim;
+  const int32_t* h_face_pos;        /* nc+1: half-faces of cell c are face_pos[c] .. face_pos[c+1]-1
+                                       (G.cells.facePos) */
+  const int32_t* h_cell_faces;      /* nhf: the face of each half-face (G.cells.faces[:, 0]) */
+  const int32_t* h_neighbors;       /* nf x 2 (G.faces.neighbors, -1 outside the grid) */
+  const double* h_cell_centroids;   /* nc x dim */
+  const double* h_face_centroids;   /* nf x dim */
+  int32_t nw;
+  const int32_t* h_perf_ptr;        /* nw+1: perforations of well k are perf_ptr[k] .. perf_ptr[k+1]-1 */
+  const int32_t* h_perf_cell;       /* the perforated cells (W[k].cells) */
+  const int32_t* h_well_rate;       /* nw: 1 for a rate well, 0 for a bhp well (W[k].type) */
+  int32_t use_trans;                /* 1: d_T holds one T per face, not per half-face (use_trans) */
+} pmb_tpfa_desc;
+
+typedef struct pmb_tpfa_forces {
+  const double* d_T;      /* nhf one-sided T (or nf face T with use_trans) */
+  const double* d_mob;    /* nc x nph phase mobilities kr / mu, row-major */
+  int32_t nph;            /* 1 .. 4 */
+  const double* h_rho;    /* nph phase densities */
+  double gravity[3];      /* gravity vector of the half-face potentials (zero: off) */
+  double well_gravity;    /* |g| of the wells' hydrostatic drops */
+  int32_t nbc;            /* boundary conditions (the reference's bc struct): */
+  const int32_t* h_bc_face; /*   faces (no face twice) */
+  const int32_t* h_bc_type; /*   1 pressure, 2 flux */
+  const double* h_bc_value; /*   pressure, or flux out of the domain */
+  int32_t nsrc;           /* sources (src.cell, src.rate) */
+  const int32_t* h_src_cell;
+  const double* h_src_rate;
+  const double* h_well_val;  /* nw targets (bhp or total rate) */
+  const double* d_perf_WI;   /* well indices per perforation */
+  const double* d_perf_dZ;   /* depth below the well's reference depth per perforation */
+  int32_t ncompi;            /* phases of the injected composition */
+  const double* h_compi;     /* nw x ncompi */
+  const int32_t* h_injector; /* nw: 1 where the mixture density is the injected composition's */
+} pmb_tpfa_forces;
+
+int pmb_tpfa_create(const pmb_tpfa_desc* desc, void* stream, pmb_tpfa** out);
+int pmb_tpfa_destroy(pmb_tpfa* h);
+/* h_out4 = [n, nnz, perforations, pinned]; pinned = 1 when the last assembly
+ * doubled a diagonal entry to fix the pressure level (no pressure boundary,
+ * no bhp well; incomp_tpfa.py:156-161). */
+int pmb_tpfa_sizes(const pmb_tpfa* h, int64_t* h_out4);
+int pmb_tpfa_pattern(const pmb_tpfa* h, int32_t* h_row_ptr, int32_t* h_col);
+/* Matrix values (nnz, device) and right-hand side (n, device) of the system
+ * (incomp_tpfa.py:91-161); the handle keeps the mobility-weighted
+ * transmissibilities and potentials for pmb_tpfa_reconstruct. */
+int pmb_tpfa_assemble(pmb_tpfa* h, const pmb_tpfa_forces* forces, double* d_vals, double* d_rhs);
+/* Solve the assembled system by AMG-preconditioned CG from p = 0 to
+ * ||rhs - A p|| <= rtol ||rhs|| (the reference calls SuperLU, :172-184).
+ * h_info3 = [iterations, relres, ok]; PMB_ERR_NOCONV when rtol was not met. */
+int pmb_tpfa_solve(pmb_tpfa* h, const double* d_vals, const double* d_rhs, double* d_p, double rtol,
+                   int32_t maxiter, double* h_info3);
+/* Face pressures, face fluxes (nf each) and per-perforation well fluxes and
+ * hydrostatic drops (may be NULL) from the solution d_p (n) of the last
+ * assembly (incomp_tpfa.py:186-211). */
+int pmb_tpfa_reconstruct(pmb_tpfa* h, const double* d_p, double* d_flux, double* d_face_pressure,
+                         double* d_perf_flux, double* d_perf_dp);
+int pmb_tpfa_levels(const pmb_tpfa* h, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
 
 /* Host-side aggregation of the AMG hierarchy for a CSR matrix (no device
  * needed): unknowns per level into h_sizes (up to max_levels), count in

@@ -50,6 +50,27 @@ class CPROpts(C.Structure):
     ]
 
 
+class TpfaDesc(C.Structure):
+    _fields_ = [
+        ("nc", c_int), ("nf", c_int), ("nhf", c_int), ("dim", c_int),
+        ("h_face_pos", P_i32), ("h_cell_faces", P_i32), ("h_neighbors", P_i32),
+        ("h_cell_centroids", P_dbl), ("h_face_centroids", P_dbl),
+        ("nw", c_int), ("h_perf_ptr", P_i32), ("h_perf_cell", P_i32), ("h_well_rate", P_i32),
+        ("use_trans", c_int),
+    ]
+
+
+class TpfaForces(C.Structure):
+    _fields_ = [
+        ("d_T", c_vp), ("d_mob", c_vp), ("nph", c_int), ("h_rho", P_dbl),
+        ("gravity", c_dbl * 3), ("well_gravity", c_dbl),
+        ("nbc", c_int), ("h_bc_face", P_i32), ("h_bc_type", P_i32), ("h_bc_value", P_dbl),
+        ("nsrc", c_int), ("h_src_cell", P_i32), ("h_src_rate", P_dbl),
+        ("h_well_val", P_dbl), ("d_perf_WI", c_vp), ("d_perf_dZ", c_vp),
+        ("ncompi", c_int), ("h_compi", P_dbl), ("h_injector", P_i32),
+    ]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "pmb_last_error": (C.c_char_p, []),
@@ -78,6 +99,7 @@ SIGNATURES = {
     "pmb_cpr_setup": (c_int, [c_vp, c_vp, c_vp, c_vp]),
     "pmb_cpr_solve": (c_int, [c_vp, c_vp, c_vp, P_dbl]),
     "pmb_cpr_levels": (c_int, [c_vp, c_int, P_i64, P_i32]),
+    "pmb_cpr_bytes": (c_int, [c_vp, P_dbl]),
     "pmb_cpr_time_stage": (c_int, [c_vp, c_int, c_vp, c_vp, c_int, P_dbl]),
     "pmb_ow_step": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_int, P_dbl]),
     "pmb_ow_step_members": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_int, c_int, P_i32, P_i32, P_i32, P_i32, P_dbl]),
@@ -93,6 +115,14 @@ SIGNATURES = {
     "pmb_pcg_setup": (c_int, [c_vp, c_vp]),
     "pmb_pcg_solve": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_int, P_dbl]),
     "pmb_pcg_levels": (c_int, [c_vp, c_int, P_i64, P_i32]),
+    "pmb_tpfa_create": (c_int, [C.POINTER(TpfaDesc), c_vp, C.POINTER(c_vp)]),
+    "pmb_tpfa_destroy": (c_int, [c_vp]),
+    "pmb_tpfa_sizes": (c_int, [c_vp, P_i64]),
+    "pmb_tpfa_pattern": (c_int, [c_vp, P_i32, P_i32]),
+    "pmb_tpfa_assemble": (c_int, [c_vp, C.POINTER(TpfaForces), c_vp, c_vp]),
+    "pmb_tpfa_solve": (c_int, [c_vp, c_vp, c_vp, c_vp, c_dbl, c_int, P_dbl]),
+    "pmb_tpfa_reconstruct": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "pmb_tpfa_levels": (c_int, [c_vp, c_int, P_i64, P_i32]),
     "pmb_amg_hierarchy_host": (c_int, [c_int, P_i32, P_i32, P_dbl, c_dbl, c_int, c_int, P_i64, P_i32]),
 }
 

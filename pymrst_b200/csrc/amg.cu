@@ -1180,6 +1180,61 @@ void AMG<T>::apply(const T* b, T* x, cudaStream_t s) {
   cycle(0, b, x, s);
 }
 
+// Byte model of the launches of cycle() and coarse_correction() above.
+template <class T>
+double AMG<T>::cycle_bytes_from(int l) const {
+  const double vb = sizeof(T);
+  if (l == (int)levels_.size()) return (double)nco_ * nco_ * 8.0 + 2.0 * nco_ * vb;  // dense_apply_kernel
+  const AMGLevel<T>& L = levels_[l];
+  const double n = L.n, mat = (double)L.nnz * (vb + 4.0) + (n + 1.0) * 4.0;
+  const int steps = std::max(1, L.degree > 0 ? L.degree : degree);
+  const double nc = (l + 1 == (int)levels_.size()) ? nco_ : levels_[l + 1].n;
+  // pre-smoothing from zero: the first step reads b and D^-1 and writes d, x
+  // (no matrix); each further step reads the matrix, b, D^-1, x, d and writes
+  // x, d
+  const double step = mat + 6.0 * n * vb;
+  double bytes = 4.0 * n * vb + (steps - 1) * step;
+  // restriction: matrix, b and x of every member row, the member lists, the
+  // coarse right-hand side written
+  bytes += mat + 2.0 * n * vb + n * 4.0 + (nc + 1.0) * 4.0 + nc * vb;
+  bytes += coarse_bytes(l);
+  // post-smoothing from the prolonged correction: agg and the coarse
+  // correction once (folded into the first step, or a separate launch that
+  // also reads and writes x)
+  bytes += steps * step + n * 4.0 + nc * vb + (L.n < kFoldProlongRows ? 0.0 : 2.0 * n * vb);
+  return bytes;
+}
+
+template <class T>
+double AMG<T>::coarse_bytes(int l) const {
+  const bool kc = l < k_levels && l + 1 < (int)levels_.size();
+  if (!kc) return cycle_bytes_from(l + 1);
+  const AMGLevel<T>& C = levels_[l + 1];
+  const double vb = sizeof(T), n = C.n;
+  const double spmv = (double)C.nnz * (vb + 4.0) + (n + 1.0) * 4.0 + 2.0 * n * vb;
+  // two cycles, two products, kdots<2> (v1, rc), kaxpy (rc, v1 -> r2),
+  // kdots<5> (v1, v2, rc), kcombine (c1, c2 -> ec)
+  return 2.0 * cycle_bytes_from(l + 1) + 2.0 * spmv + (2.0 + 3.0 + 3.0 + 3.0) * n * vb;
+}
+
+template <class T>
+double AMG<T>::refresh_bytes() const {
+  const double vb = sizeof(T);
+  double bytes = 0.0;
+  for (size_t l = 0; l < levels_.size(); ++l) {
+    const AMGLevel<T>& L = levels_[l];
+    const double nnz_next = (l + 1 < levels_.size()) ? (double)levels_[l + 1].nnz : (double)co_nnz_;
+    // diagonal and Gershgorin bound: matrix read, D^-1 written
+    bytes += (double)L.nnz * (vb + 4.0) + (L.n + 1.0) * 4.0 + L.n * vb;
+    // Galerkin gather: every fine value once through its index, the coarse
+    // values and their index ranges
+    bytes += (double)L.nnz * (vb + 4.0) + nnz_next * (vb + 4.0);
+  }
+  // dense coarsest matrix assembled and inverted in place
+  bytes += (double)co_nnz_ * (vb + 4.0) + 3.0 * (double)nco_ * nco_ * 8.0;
+  return bytes;
+}
+
 template class AMG<double>;
 template class AMG<float>;
 

@@ -371,6 +371,13 @@ int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* sizes, int32_t
   });
 }
 
+int pmb_cpr_bytes(const pmb_cpr* s, double* h_out8) {
+  return guarded([&] {
+    PMB_REQUIRE(s && h_out8, "NULL argument");
+    s->s->bytes(h_out8);
+  });
+}
+
 int pmb_cpr_time_stage(pmb_cpr* s, int32_t stage, const double* d_r, double* d_z, int32_t reps,
                        double* h_ms) {
   return guarded([&] {

@@ -1273,6 +1273,36 @@ double CPRSolver::time_stage(int stage, const double* r, double* z, int reps) {
   return ms / reps;
 }
 
+void CPRSolver::bytes(double* out) const {
+  const double nc = m_.nc(), nnzb = (double)m_.nnzb(), nvec = (double)m_.nvec();
+  const double vb = f32_ ? 4.0 : 8.0, blk = 4.0 * vb;
+  for (int i = 0; i < 8; ++i) out[i] = 0.0;
+  out[0] = o_.use_pressure_stage ? (f32_ ? amg32_.cycle_bytes() : amg_.cycle_bytes()) : 0.0;
+  // one sweep of the second stage (both colours and the well update): every
+  // block once, the index of every block off the line (the line-ordered copy
+  // needs none for the diagonal and the two line couplings; the block-CSR one
+  // per block plus row pointers), r, z read and written, perforation index
+  out[1] = use_ell_ ? nnzb * blk + std::max(nnzb - 3.0 * nc, 0.0) * 4.0 + nc * (16.0 + 32.0 + 4.0)
+                    : nnzb * (blk + 4.0) + (nc + 1.0) * 4.0 + nc * (16.0 + 32.0 + 4.0);
+  // y = J x: blocks, column indices, row pointers, x read, y written
+  out[2] = nnzb * 36.0 + (nc + 1.0) * 4.0 + nvec * 16.0;
+  // restriction (r read, weights, pressure right-hand side written) and the
+  // prolongation into line order (pressure correction, r, the line's cell
+  // index read; r and z in line order written)
+  out[3] = o_.use_pressure_stage ? nc * (16.0 + vb) + nc * (vb + 16.0 + 4.0 + 32.0) : 0.0;
+  // setup: the second stage's copy of the Jacobian (gather index, FP64 block
+  // read, block written), the weights (pressures read), the pressure values
+  // (blocks read, values written), FP32 conversion of level 0
+  double setup = use_ell_ ? (double)ell_.slots * nc * (4.0 + 32.0 + blk) : (f32_ ? nnzb * (32.0 + 16.0) : 0.0);
+  if (o_.use_pressure_stage) {
+    setup += nc * 16.0 + nnzb * (32.0 + 4.0 + 8.0);
+    if (f32_) setup += (double)ap_.size() * (8.0 + 4.0);
+  }
+  out[4] = setup;
+  out[5] = nvec;
+  out[6] = o_.use_pressure_stage ? (f32_ ? amg32_.refresh_bytes() : amg_.refresh_bytes()) : 0.0;
+}
+
 bool CPRSolver::solve(const double* b, double* x, double* info) {
   PMB_REQUIRE(jac_ != nullptr, "pmb_cpr_setup must run before pmb_cpr_solve");
   auto op = [this](const double* in, double* out) {

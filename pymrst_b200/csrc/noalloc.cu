@@ -84,7 +84,9 @@ __global__ void __launch_bounds__(256) na_final_kernel(int nc, int nblocks, cons
 }
 
 // Device address of the scratch array, looked up once per device (the
-// array's name in host code is only a stand-in for the symbol).
+// array's name in host code is only a stand-in for the symbol).  The address
+// is cached for the life of the process, so the entry point must not be used
+// on a device after cudaDeviceReset() of that device in the same process.
 static double* scratch_address(int device) {
   constexpr int kMaxDevices = 64;
   static std::mutex mu;
@@ -114,6 +116,8 @@ extern "C" int pmb_ow_cnv_mb_noalloc(int32_t nc, const double* d_res, const doub
     PMB_REQUIRE(d_res && d_x && d_pv && h_fluid5 && d_out4, "NULL argument");
     PMB_REQUIRE(reinterpret_cast<uintptr_t>(d_res) % 16 == 0 && reinterpret_cast<uintptr_t>(d_x) % 16 == 0,
                 "res and x must be 16-byte aligned");
+    PMB_REQUIRE(reinterpret_cast<uintptr_t>(d_pv) % 8 == 0 && reinterpret_cast<uintptr_t>(d_out4) % 8 == 0,
+                "pv and out must be 8-byte aligned");
     PMB_REQUIRE(dt > 0.0 && pv_total > 0.0, "dt and pv_total must be positive");
     int dev = 0;
     PMB_CUDA(cudaGetDevice(&dev));

@@ -168,6 +168,25 @@ class ScalarPCG {
   AMG<double> amg_;
 };
 
+// Handle used by the incompressible TPFA path (tpfa.cu), which owns one
+// pressure solver per grid and well set.
+struct ScalarPCGHandle {
+  std::unique_ptr<ScalarPCG> s;
+};
+
+ScalarPCGHandle* make_scalar_pcg(int n, const int* h_rp, const int* h_ci, cudaStream_t s, double theta,
+                                 int coarse) {
+  auto h = std::make_unique<ScalarPCGHandle>();
+  h->s = std::make_unique<ScalarPCG>(n, h_rp, h_ci, s, theta, coarse);
+  return h.release();
+}
+void destroy_scalar_pcg(ScalarPCGHandle* p) { delete p; }
+void scalar_pcg_setup(ScalarPCGHandle* p, const double* d_vals) { p->s->setup(d_vals); }
+bool scalar_pcg_solve(ScalarPCGHandle* p, const double* b, double* x, double rtol, int maxiter, double* info) {
+  return p->s->solve(b, x, rtol, maxiter, info);
+}
+int scalar_pcg_levels(const ScalarPCGHandle* p, int64_t* sizes, int maxl) { return p->s->levels(sizes, maxl); }
+
 }  // namespace pmb
 
 using namespace pmb;

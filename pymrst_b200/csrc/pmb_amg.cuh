@@ -101,8 +101,16 @@ class AMG {
   // also needs PMB_FUSED_COARSE=1 in the environment).
   bool fused_coarse = true;
   int fused_first_level() const { return coop_start_; }
+  // Algorithmic bytes of one apply() and of one refresh(): every array a
+  // kernel reads or writes counted once per launch, values in T, indices in
+  // 4 bytes, the dense coarsest inverse in 8 bytes per entry.
+  double cycle_bytes() const { return num_levels() ? cycle_bytes_from(0) : 0.0; }
+  double refresh_bytes() const;
+  long long level_nnz(int l) const { return l < (int)levels_.size() ? levels_[l].nnz : co_nnz_; }
 
  private:
+  double cycle_bytes_from(int l) const;
+  double coarse_bytes(int l) const;
   int coop_start_ = -1, coop_grid_ = 0;
   DArray<unsigned char> coop_levels_;
   DArray<unsigned int> coop_bar_;  // grid barrier: arrivals, generation

@@ -23,6 +23,11 @@ class CPRSolver {
   // whole preconditioner, not replayed from a graph), by CUDA events on the
   // solver's stream, after one untimed application.
   double time_stage(int stage, const double* r, double* z, int reps);
+  // Algorithmic bytes (every array read or written once per launch, storage
+  // types): [AMG cycle, one second-stage sweep, operator product, pressure
+  // restriction + prolongation of one application, one setup without
+  // aggregation, FGMRES vector length, AMG refresh, 0].
+  void bytes(double* out) const;
 
  private:
   void precond(const double* r, double* z);

@@ -30,22 +30,26 @@ from .ow_model import GpuOilWaterModel, OWState, _torch, default_cpr_options, fa
 from .params import fluid_params, pore_volume
 
 
-# -- the reference's ensemble interface ---------------------------------------------
+# -- the reference's ensemble interface (ensemble_impl.py:17-67) ----------------------
 
 @dataclass
 class EnsembleResult:
-    """The quantity of interest for every member, and its statistics."""
+    """Members' parameters, shape (n_par, N), and quantities of interest,
+    shape (n_obs, N): one column per member.  The statistics run across the
+    members (axis 1); the spread is the sample standard deviation."""
 
-    parameters: np.ndarray       # (n_par, N)
-    qoi: np.ndarray              # (n_obs, N)
+    parameters: np.ndarray
+    qoi: np.ndarray
 
     @property
     def mean(self) -> np.ndarray:
-        return self.qoi.mean(axis=1)
+        return np.mean(self.qoi, axis=1)
 
     @property
     def std(self) -> np.ndarray:
-        return self.qoi.std(axis=1, ddof=1)
+        n = self.qoi.shape[1]
+        dev = self.qoi - self.mean[:, None]
+        return np.sqrt(np.sum(dev * dev, axis=1) / (n - 1))
 
     def percentile(self, q) -> np.ndarray:
         return np.percentile(self.qoi, q, axis=1)
@@ -53,14 +57,17 @@ class EnsembleResult:
 
 def gaussian_samples(mean: np.ndarray, cov: np.ndarray, n: int,
                      rng: Optional[np.random.Generator] = None) -> np.ndarray:
-    """An (n_par, N) prior ensemble from a Gaussian (ensemble_impl.py:35-45)."""
-    rng = np.random.default_rng() if rng is None else rng
-    mean = np.asarray(mean, float).ravel()
-    cov = np.asarray(cov, float)
-    if cov.ndim == 1:
-        cov = np.diag(cov)
-    chol = np.linalg.cholesky(cov)
-    return mean[:, None] + chol @ rng.standard_normal((mean.size, n))
+    """n draws of N(mean, cov) as the columns of an (n_par, n) array; `cov`
+    may be given as its diagonal.  Each column is mean + L z with L the lower
+    Cholesky factor of cov and z a column of standard normals drawn as one
+    (n_par, n) block, so a generator in a given state yields the same
+    ensemble as the reference's sampler does."""
+    gen = rng if rng is not None else np.random.default_rng()
+    mu = np.ravel(np.asarray(mean, dtype=float))
+    c = np.asarray(cov, dtype=float)
+    L = np.linalg.cholesky(np.diag(c) if c.ndim == 1 else c)
+    z = gen.standard_normal((mu.size, n))
+    return L @ z + mu[:, None]
 
 
 def shard_members(costs: Sequence[float], world: int) -> List[Tuple[int, int]]:
@@ -107,9 +114,9 @@ def run_ensemble(parameters: np.ndarray, simulate: Callable[[np.ndarray], np.nda
         dist.all_gather_object(gathered, local)
         local = [item for part in gathered for item in part]
     cols = [c for _, c in sorted(local, key=lambda kc: kc[0])]
-    n_obs = {c.size for c in cols}
-    if len(n_obs) != 1:
-        raise ValueError(f"members returned different QoI lengths: {sorted(n_obs)}")
+    lengths = sorted({c.size for c in cols})
+    if len(lengths) > 1:
+        raise ValueError(f"every member must return a quantity of interest of one length; got {lengths}")
     return EnsembleResult(parameters=m, qoi=np.column_stack(cols))
 
 

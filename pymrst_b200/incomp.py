@@ -1,28 +1,36 @@
 """Incompressible TPFA pressure solve with the reference's interface
-(`incomp_tpfa`, pymrst/modules/incomp/incomp_tpfa.py:55-243).
+(`incomp_tpfa`, pymrst/modules/incomp/incomp_tpfa.py:55-211).
 
-The pressure system is assembled on the host exactly as the reference
-describes it: mobility-weighted one-sided T, harmonic face T, gravity /
-Dirichlet / Neumann / source right-hand side, well rows, and the pin when
-nothing fixes the pressure level.  It is then solved on the GPU by AMG-
-preconditioned conjugate gradients (`pmb_pcg_*`), which replaces the
-reference's SuperLU call (:172-184, 98% of its time); face pressures, face
-fluxes and well fluxes follow (:186-211).  A caller's `LinSolve` is honoured.
+The pressure system is assembled, solved and post-processed on the device
+through the `pmb_tpfa_*` entry points (`csrc/tpfa.cu`): mobility-weighted
+transmissibilities, the gravity / boundary / source right-hand side, the
+well rows and the pressure pin are formed by kernels that gather per cell
+row and per well; the solve is AMG-preconditioned conjugate gradients; face
+pressures, face fluxes and well fluxes are reconstructed by kernels.  The host
+side only evaluates the caller's fluid object (its relative permeabilities and
+viscosities, which are Python callables) and converts the reference's bc / src
+/ well structures into arrays.
+
+A caller's `LinSolve(A, b)` is honoured (A is then copied to the host as a
+scipy CSR matrix), and so are `MatrixOutput` and `reduce` (the Schur
+complement on the well unknowns, formed on the host because it is an output
+of the call, not part of the device solve).
 
 Gravity is the `gravity` argument (a vector, default zero), used for both
 the half-face potentials and the well pressure drop; the reference's newer
 function reads a global setting for those, its earlier `incomp_tpfa_ad`
 (which the MATLAB goldens are replayed with) the argument.
-Not supported here: capillary pressure, periodic `bcp`, non-neighbouring
-connections, `reduce`.
+Not supported: capillary pressure, periodic `bcp`, non-neighbouring
+connections (NotImplementedError).
 """
 
 from __future__ import annotations
 
 import copy
 import hashlib
+import warnings
+from collections import OrderedDict
 from dataclasses import dataclass, field
-from types import SimpleNamespace
 from typing import Any, List, Optional
 
 import numpy as np
@@ -77,14 +85,33 @@ def init_single_fluid(mu, rho) -> SingleFluid:
     return SingleFluid(mu, rho)
 
 
-def _props(state, fluid):
-    mu, rho = fluid.properties(state)
-    s = fluid.saturation(state)
-    kr = np.atleast_2d(fluid.relperm(s))
-    return np.asarray(rho, float).ravel(), kr, np.asarray(mu, float).ravel()
+def _field(state, name):
+    return state.get(name) if isinstance(state, dict) else getattr(state, name, None)
 
 
-# ---- device pressure solver ---------------------------------------------------
+def fluid_mobilities(state, fluid):
+    """Phase densities (nph) and mobilities kr / mu (nc x nph) of the fluid
+    at the state, for both fluid kinds the reference's incompressible solver
+    accepts (get_incomp_props.py): an incompressible fluid with
+    `properties` / `saturation` / `relperm`, or an AD fluid evaluated at the
+    mean pressure."""
+    if hasattr(fluid, "properties"):
+        mu, rho = fluid.properties(state)
+        kr = np.atleast_2d(np.asarray(fluid.relperm(fluid.saturation(state)), float))
+        mu = np.asarray(mu, float)
+        return np.asarray(rho, float).ravel(), kr / (mu if mu.ndim == 2 else mu.ravel())
+    val = lambda v: np.asarray(getattr(v, "val", v), float)
+    p = _field(state, "pressure")
+    p_mean = float(np.mean(p)) if p is not None else 101325.0
+    rho = np.array([float(fluid.rhoWS * val(fluid.bW(p_mean))), float(fluid.rhoOS * val(fluid.bO(p_mean)))])
+    mu = np.column_stack([val(fluid.muW(p)) * np.ones(np.size(p)), val(fluid.muO(p)) * np.ones(np.size(p))])
+    sw = np.atleast_2d(np.asarray(_field(state, "s"), float))[:, 0]
+    kro = fluid.krOW if hasattr(fluid, "krOW") else fluid.krO
+    kr = np.column_stack([val(fluid.krW(sw)), val(kro(1.0 - sw))])
+    return rho, kr / mu
+
+
+# ---- device pressure solver (LinSolve plug) ----------------------------------------
 
 _SOLVERS = {}
 
@@ -127,175 +154,282 @@ class GpuLinSolve:
         return xd.cpu().numpy()
 
 
-# ---- incomp_tpfa ----------------------------------------------------------------
+# ---- the device system ----------------------------------------------------------------
 
-def _cell_faces(G):
-    cf = np.asarray(G.cells.faces, dtype=np.int64)
-    cf = cf[:, 0] if cf.ndim > 1 else cf
-    cell_no = np.repeat(np.arange(G.cells.num, dtype=np.int64), np.diff(np.asarray(G.cells.facePos)))
-    return cell_no, cf
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a).ravel(), dtype=np.int32)
 
 
-def incomp_tpfa(state: Any, G, T, fluid, bc=None, src=None, wells=None, gravity=None, *, W=None,
-                LinSolve=None, MatrixOutput=False, use_trans=False, pc_form="nonwetting", **unsupported):
+def _f64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+
+
+def _is_injector(w) -> bool:
+    """The reference's injector test for the mixture density
+    (compute_incomp_well_pressure_drop.py): every sign positive, or a rate
+    well with a positive target."""
+    sign = getattr(w, "sign", None)
+    if sign is not None and np.size(sign) > 0 and bool(np.all(np.asarray(sign) > 0)):
+        return True
+    return str(w.type).lower() == "rate" and float(np.sum(w.val)) > 0
+
+
+class TpfaSystem:
+    """One grid + well set on the device (a `pmb_tpfa` handle): the pattern
+    of the pressure system and its workspaces.  `solve` assembles, solves and
+    reconstructs; the arrays stay on the device until `result` copies them."""
+
+    def __init__(self, G, wells, use_trans=False, stream=None):
+        import torch
+        self.torch = torch
+        nc, nf = int(G.cells.num), int(G.faces.num)
+        cf = np.asarray(G.cells.faces)
+        cf = cf[:, 0] if cf.ndim > 1 else cf
+        self.nc, self.nf, self.nhf, self.nw = nc, nf, int(cf.size), len(wells)
+        self.dim = int(getattr(G, "griddim", np.asarray(G.cells.centroids).shape[1]))
+        perf_ptr = np.zeros(self.nw + 1, dtype=np.int64)
+        for k, w in enumerate(wells):
+            perf_ptr[k + 1] = perf_ptr[k] + np.asarray(w.cells).size
+        self._keep = dict(
+            face_pos=_i32(G.cells.facePos), cell_faces=_i32(cf), nbr=_i32(G.faces.neighbors),
+            cc=_f64(np.asarray(G.cells.centroids)[:, :self.dim]), fc=_f64(np.asarray(G.faces.centroids)[:, :self.dim]),
+            perf_ptr=_i32(perf_ptr), perf_cell=_i32(np.concatenate([np.asarray(w.cells).ravel() for w in wells])
+                                                    if wells else np.zeros(0)),
+            well_rate=_i32([str(w.type).lower() == "rate" for w in wells]))
+        k = self._keep
+        d = N.TpfaDesc()
+        d.nc, d.nf, d.nhf, d.dim = nc, nf, self.nhf, self.dim
+        d.h_face_pos, d.h_cell_faces = N.as_p(k["face_pos"], N.C.c_int32), N.as_p(k["cell_faces"], N.C.c_int32)
+        d.h_neighbors = N.as_p(k["nbr"], N.C.c_int32)
+        d.h_cell_centroids, d.h_face_centroids = N.as_p(k["cc"], N.C.c_double), N.as_p(k["fc"], N.C.c_double)
+        d.nw = self.nw
+        d.h_perf_ptr, d.h_perf_cell = N.as_p(k["perf_ptr"], N.C.c_int32), N.as_p(k["perf_cell"], N.C.c_int32)
+        d.h_well_rate = N.as_p(k["well_rate"], N.C.c_int32)
+        d.use_trans = int(bool(use_trans))
+        self.stream = torch.cuda.current_stream().cuda_stream if stream is None else stream
+        self.handle = N.c_vp()
+        N.check(N.lib().pmb_tpfa_create(N.C.byref(d), self.stream, N.C.byref(self.handle)))
+        sz = (N.c_i64 * 4)()
+        N.check(N.lib().pmb_tpfa_sizes(self.handle, sz))
+        self.n, self.nnz, self.nperf = int(sz[0]), int(sz[1]), int(sz[2])
+        self.row_ptr = np.zeros(self.n + 1, np.int32)
+        self.col = np.zeros(self.nnz, np.int32)
+        N.check(N.lib().pmb_tpfa_pattern(self.handle, N.as_p(self.row_ptr, N.C.c_int32),
+                                         N.as_p(self.col, N.C.c_int32)))
+        dev = "cuda"
+        self.vals = torch.empty(self.nnz, dtype=torch.float64, device=dev)
+        self.rhs = torch.empty(self.n, dtype=torch.float64, device=dev)
+        self.p = torch.empty(self.n, dtype=torch.float64, device=dev)
+        self.flux = torch.empty(max(nf, 1), dtype=torch.float64, device=dev)
+        self.fpress = torch.empty(max(nf, 1), dtype=torch.float64, device=dev)
+        self.perf_flux = torch.empty(max(self.nperf, 1), dtype=torch.float64, device=dev)
+        self.perf_dp = torch.empty(max(self.nperf, 1), dtype=torch.float64, device=dev)
+        self.last_iterations = 0
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            try:
+                N.lib().pmb_tpfa_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    def assemble(self, T, mob, rho, gvec, norm_g, bc, src, wells):
+        torch = self.torch
+        mob = np.ascontiguousarray(np.atleast_2d(np.asarray(mob, float)))
+        if mob.shape[0] != self.nc:
+            mob = np.ascontiguousarray(np.broadcast_to(mob, (self.nc, mob.shape[1])))
+        nph = mob.shape[1]
+        if nph > 4:
+            raise NotImplementedError("at most four phases")
+        keep = {}
+        keep["T"] = torch.as_tensor(_f64(T), device="cuda")
+        keep["mob"] = torch.as_tensor(mob, device="cuda")
+        keep["rho"] = _f64(np.resize(np.asarray(rho, float), nph))
+        fr = N.TpfaForces()
+        fr.d_T, fr.d_mob, fr.nph = N.ptr(keep["T"]), N.ptr(keep["mob"]), nph
+        fr.h_rho = N.as_p(keep["rho"], N.C.c_double)
+        for i in range(3):
+            fr.gravity[i] = float(gvec[i])
+        fr.well_gravity = float(norm_g)
+        if bc is not None and np.size(bc.face):
+            faces = np.asarray(bc.face, dtype=np.int64).ravel()
+            types = np.resize(np.array([str(t).lower() for t in np.atleast_1d(bc.type)]), faces.size)
+            code = np.where(types == "pressure", 1, np.where(types == "flux", 2, 0))
+            if np.any(code == 0):
+                raise ValueError("boundary condition types must be 'pressure' or 'flux'")
+            keep["bcf"], keep["bct"] = _i32(faces), _i32(code)
+            keep["bcv"] = _f64(np.resize(np.asarray(bc.value, float).ravel(), faces.size))
+            fr.nbc = faces.size
+            fr.h_bc_face, fr.h_bc_type = N.as_p(keep["bcf"], N.C.c_int32), N.as_p(keep["bct"], N.C.c_int32)
+            fr.h_bc_value = N.as_p(keep["bcv"], N.C.c_double)
+        if src is not None and np.size(src.cell):
+            cells = np.asarray(src.cell, dtype=np.int64).ravel()
+            keep["sc"], keep["sr"] = _i32(cells), _f64(np.resize(np.asarray(src.rate, float).ravel(), cells.size))
+            fr.nsrc = cells.size
+            fr.h_src_cell, fr.h_src_rate = N.as_p(keep["sc"], N.C.c_int32), N.as_p(keep["sr"], N.C.c_double)
+        if wells:
+            keep["wv"] = _f64([float(np.ravel(w.val)[0]) for w in wells])
+            keep["WI"] = torch.as_tensor(np.concatenate([_f64(w.WI) for w in wells]), device="cuda")
+            keep["dZ"] = torch.as_tensor(np.concatenate([_f64(np.resize(np.asarray(w.dZ, float), np.size(w.cells)))
+                                                         for w in wells]), device="cuda")
+            compis = [np.atleast_1d(np.asarray(w.compi, float)).ravel() for w in wells]
+            nci = max(c.size for c in compis)
+            ca = np.zeros((len(wells), max(nci, 1)))
+            for k, c in enumerate(compis):
+                ca[k, :c.size] = c
+            keep["compi"] = np.ascontiguousarray(ca)
+            keep["inj"] = _i32([_is_injector(w) for w in wells])
+            fr.h_well_val = N.as_p(keep["wv"], N.C.c_double)
+            fr.d_perf_WI, fr.d_perf_dZ = N.ptr(keep["WI"]), N.ptr(keep["dZ"])
+            fr.ncompi = ca.shape[1]
+            fr.h_compi = N.as_p(keep["compi"], N.C.c_double)
+            fr.h_injector = N.as_p(keep["inj"], N.C.c_int32)
+        N.check(N.lib().pmb_tpfa_assemble(self.handle, N.C.byref(fr), N.ptr(self.vals), N.ptr(self.rhs)))
+        self._inputs = keep  # device inputs stay alive until the next assembly
+
+    def matrix(self):
+        return sp.csr_array((self.vals.cpu().numpy(), self.col, self.row_ptr), shape=(self.n, self.n))
+
+    def solve_device(self, rtol=1e-12, maxiter=1000):
+        info = (N.C.c_double * 3)()
+        N.check(N.lib().pmb_tpfa_solve(self.handle, N.ptr(self.vals), N.ptr(self.rhs), N.ptr(self.p),
+                                       float(rtol), int(maxiter), info))
+        self.last_iterations = int(info[0])
+        self.last_relres = float(info[1])
+
+    def set_solution(self, p):
+        self.p.copy_(self.torch.as_tensor(_f64(p), device="cuda"))
+
+    def reconstruct(self):
+        N.check(N.lib().pmb_tpfa_reconstruct(self.handle, N.ptr(self.p), N.ptr(self.flux), N.ptr(self.fpress),
+                                             N.ptr(self.perf_flux), N.ptr(self.perf_dp)))
+
+
+_SYSTEMS: "OrderedDict[tuple, TpfaSystem]" = OrderedDict()
+_MAX_SYSTEMS = 4
+
+
+def _system(G, wells, use_trans) -> TpfaSystem:
+    """The cached device system of this grid and well set (the few most
+    recently used are kept)."""
+    cf = np.asarray(G.cells.faces)
+    h = hashlib.sha1()
+    for a in (np.asarray(G.cells.facePos), cf, np.asarray(G.faces.neighbors)):
+        h.update(np.ascontiguousarray(a).tobytes())
+    for w in wells:
+        h.update(np.ascontiguousarray(np.asarray(w.cells, dtype=np.int64)).tobytes())
+        h.update(str(w.type).lower().encode())
+    key = (int(G.cells.num), int(G.faces.num), bool(use_trans), h.hexdigest(),
+           hashlib.sha1(np.ascontiguousarray(np.asarray(G.cells.centroids, float)).tobytes()).hexdigest())
+    s = _SYSTEMS.get(key)
+    if s is None:
+        s = TpfaSystem(G, wells, use_trans)
+        _SYSTEMS[key] = s
+        while len(_SYSTEMS) > _MAX_SYSTEMS:
+            _SYSTEMS.popitem(last=False)
+    else:
+        _SYSTEMS.move_to_end(key)
+    return s
+
+
+def _driving_forces(G, gvec, bc, src, wells, MatrixOutput) -> bool:
+    """Whether the solve has anything to do (checkDrivingForcesIncomp), with
+    its warnings: unbalanced rates when nothing fixes the pressure level, and
+    no driving force at all."""
+    pressure_bc = bc is not None and any(str(t).lower() == "pressure" for t in np.atleast_1d(bc.type))
+    bhp = any(str(w.type).lower() == "bhp" for w in wells)
+    if not (pressure_bc or bhp):
+        total = sum(float(np.sum(w.val)) for w in wells)
+        total += float(np.sum(src.rate)) if src is not None else 0.0
+        total += float(np.sum(bc.value)) if bc is not None else 0.0
+        if abs(total) > 1e-12:
+            warnings.warn("Well rates and flux bc must sum up to 0 \nwhen there are no bhp "
+                          "constrained wells or pressure bc.Results may not be reliable.\n")
+    grav_on = np.linalg.norm(gvec[:int(G.griddim)]) > 0
+    if grav_on or bc is not None or src is not None or wells or MatrixOutput:
+        return True
+    warnings.warn("No external driving forces present in model--state remains unchanged.\n")
+    return False
+
+
+def incomp_tpfa(state: Any, G, T, fluid, bc=None, src=None, wells=None, gravity=None, *, W=None, bcp=None,
+                LinSolve=None, MatrixOutput=False, Verbose=False, condition_number=False,
+                pc_form="nonwetting", reduce=False, use_trans=False, rtol=1e-12, maxiter=1000):
     """Incompressible TPFA pressure; returns a new state (the input is not
-    modified).  Arguments as the reference's `incomp_tpfa`."""
-    for k, v in unsupported.items():
-        if v not in (None, False):
-            raise NotImplementedError(f"incomp_tpfa option {k!r} is not supported by this path")
+    modified).  Arguments as the reference's `incomp_tpfa`; `rtol` and
+    `maxiter` bound the device PCG solve (the reference solves directly)."""
+    if bcp is not None:
+        raise NotImplementedError("periodic boundary conditions (bcp) are not supported by this path")
+    if getattr(G, "nnc", None) is not None and np.size(getattr(G.nnc, "cells", [])):
+        raise NotImplementedError("non-neighbouring connections are not supported by this path")
+    pc_fn = getattr(fluid, "pc", None) if hasattr(fluid, "properties") else getattr(fluid, "pcOW", None)
+    if pc_fn is not None:
+        pc = np.asarray(getattr(pc_fn(state), "val", pc_fn(state)) if hasattr(fluid, "properties") else
+                        getattr(pc_fn(np.atleast_2d(np.asarray(state.s, float))[:, 0]), "val", 0.0), float)
+        if np.any(np.abs(pc) > 0):
+            raise NotImplementedError("capillary pressure is not supported by this path")
     wells = list(wells if wells is not None else (W or []))
+    for w in wells:
+        if str(w.type).lower() not in ("bhp", "rate"):
+            raise ValueError("Unsupported well type.")
     state = copy.copy(state)
-    g_vec = np.zeros(3) if gravity is None else np.resize(np.asarray(gravity, float), 3)
-    dim = int(G.griddim)
-    nbr = np.asarray(G.faces.neighbors, dtype=np.int64)
-    nf = G.faces.num
-    nc = G.cells.num
-    nw = len(wells)
-    n = nc + nw
-    cell_no, cf = _cell_faces(G)
-    internal = np.all(nbr >= 0, axis=1)
-
-    rho, kr, mu = _props(state, fluid)
-    mob = kr / mu
-    totmob = mob.sum(axis=1)
-    omega = (mob * rho).sum(axis=1) / totmob
-
-    # mobility-weighted transmissibilities (incomp_tpfa.py:223-243)
+    gvec = np.zeros(3) if gravity is None else np.resize(np.asarray(gravity, float), 3)
+    if not _driving_forces(G, gvec, bc, src, wells, MatrixOutput):
+        return state
+    nc, nw = int(G.cells.num), len(wells)
     T = np.asarray(T, float).ravel()
+    cf = np.asarray(G.cells.faces)
     if use_trans:
-        assert T.size == nf
-        cnt = (nbr >= 0).sum(axis=1)
-        fmob = np.bincount(cf, totmob[cell_no], minlength=nf) / cnt
-        ft = T * fmob
-        Th = (ft * cnt)[cf]
+        assert T.size == G.faces.num, (
+            f"Expected one transmissibility for each interface (={G.faces.num}) but got {T.size}.")
     else:
-        assert T.size == cf.size, "one one-sided transmissibility per half-face expected"
-        Th = T * totmob[cell_no]
-        with np.errstate(divide="ignore"):
-            ft = 1.0 / np.bincount(cf, 1.0 / Th, minlength=nf)
-
-    # right-hand-side pieces (compute_pressure_rhs.py:17-55)
-    if np.linalg.norm(g_vec[:dim]) > 0:
-        cvec = np.asarray(G.faces.centroids)[cf, :dim] - np.asarray(G.cells.centroids)[cell_no, :dim]
-        grav = omega[cell_no] * (cvec @ g_vec[:dim])
+        assert T.size == (cf.shape[0] if cf.ndim > 1 else cf.size), (
+            f"Expected one one-sided transmissibility for each half face, but got {T.size}.")
+    rho, mob = fluid_mobilities(state, fluid)
+    syst = _system(G, wells, use_trans)
+    syst.assemble(T, mob, rho, gvec, float(np.linalg.norm(gvec)), bc, src, wells)
+    A = None
+    if MatrixOutput or reduce or LinSolve is not None or condition_number:
+        A = syst.matrix()
+        rhs = syst.rhs.cpu().numpy()
+    if condition_number:
+        print(f"condition number of the pressure matrix: {np.linalg.cond(A.toarray()):.6e}")
+    if MatrixOutput:
+        state.A, state.rhs = A, rhs
+    if reduce:
+        # Schur complement on the well unknowns: D is diagonal
+        Dinv = sp.diags_array(1.0 / A.diagonal()[nc:], shape=(nw, nw))
+        C = A[nc:, :nc]
+        A_r = (A[:nc, :nc] - A[:nc, nc:] @ Dinv @ C).tocsr()
+        rhs_r = rhs[:nc] - A[:nc, nc:] @ (Dinv @ rhs[nc:])
+        state.A, state.rhs = A_r, rhs_r
+        if LinSolve is not None:
+            p_r = np.asarray(LinSolve(A_r, rhs_r)).ravel()
+            syst.set_solution(np.concatenate([p_r, Dinv @ (rhs[nc:] - C @ p_r)]))
+        else:
+            syst.solve_device(rtol, maxiter)
+    elif LinSolve is not None:
+        syst.set_solution(np.asarray(LinSolve(A, rhs)).ravel())
     else:
-        grav = np.zeros(cf.size)
-    ff = np.zeros(cf.size)
-    gg = np.zeros(nc)
-    hh = np.zeros(nf)
-    dF = np.zeros(nf, dtype=bool)
-    dC = np.zeros(0)
-    if src is not None and np.size(src.cell):
-        cells = np.asarray(src.cell, dtype=np.int64).ravel()
-        gg += np.bincount(cells, np.asarray(src.rate, float).ravel(), minlength=nc)
-    if bc is not None and np.size(bc.face):
-        faces = np.asarray(bc.face, dtype=np.int64).ravel()
-        vals = np.asarray(bc.value, float).ravel()
-        types = np.resize(np.array([str(t).lower() for t in np.atleast_1d(bc.type)]), faces.size)
-        isp = types == "pressure"
-        pos = np.zeros(nf, dtype=np.int64)
-        pos[faces[isp]] = np.arange(isp.sum())
-        dF[faces[isp]] = True
-        i = dF[cf]
-        ff[i] = -vals[isp][pos[cf[i]]]
-        dC = vals[isp][pos[dF]]
-        isf = types == "flux"
-        hh[faces[isf]] = -vals[isf]
-
-    sgn = 2.0 * (nbr[cf, 0] == cell_no) - 1.0
-    j = internal[cf] | dF[cf]
-    fg = np.bincount(cf[j], grav[j] * sgn[j], minlength=nf)
-    rhs = np.zeros(n)
-    rhs[:nc] += np.bincount(cell_no, -ft[cf] * (sgn * fg[cf] + ff), minlength=nc)
-    rhs[:nc] += gg
-    rhs[:nc] += np.bincount(cell_no, -hh[cf], minlength=nc)
-
-    # wells (incomp_tpfa.py:126-148)
-    d = np.zeros(nc)
-    Cr, Cc, Cv = [], [], []
-    D = np.zeros(nw)
-    norm_g = float(np.linalg.norm(g_vec))
+        syst.solve_device(rtol, maxiter)
+    syst.reconstruct()
+    p = syst.p.cpu().numpy()
+    state.pressure = p[:nc]
+    state.flux = syst.flux.cpu().numpy()[:G.faces.num]
+    state.facePressure = syst.fpress.cpu().numpy()[:G.faces.num]
     well_sols = [copy.copy(ws) for ws in (getattr(state, "wellSol", None) or [])]
     while len(well_sols) < nw:
         well_sols.append(WellSol())
-    for k, w in enumerate(wells):
-        wc = np.asarray(w.cells, dtype=np.int64).ravel()
-        wi = np.asarray(w.WI, float).ravel() * totmob[wc]
-        compi = np.atleast_1d(np.asarray(w.compi, float)).ravel()
-        injector = (np.all(np.asarray(getattr(w, "sign", 0)) > 0) and getattr(w, "sign", 0) != 0) or \
-                   (str(w.type).lower() == "rate" and float(np.sum(w.val)) > 0)
-        if injector:
-            m = min(rho.size, compi.size)
-            rho_mix = rho[:m] @ compi[:m]
-        else:
-            mw = mob[wc]
-            f = mw / mw.sum(axis=1, keepdims=True)
-            m = min(rho.size, mob.shape[1])
-            WI = np.asarray(w.WI, float).ravel()
-            rho_mix = np.sum(WI * (f[:, :m] @ rho[:m])) / np.sum(WI)
-        dp = norm_g * (np.asarray(w.dZ, float).ravel() * rho_mix)
-        np.add.at(d, wc, wi)
-        well_sols[k].cdp = dp
-        kind = str(w.type).lower()
-        val = float(np.ravel(w.val)[0])
-        if kind == "bhp":
-            ww = wi.max()
-            rhs[nc + k] += ww * val
-            np.add.at(rhs, wc, wi * (val + dp))
-            D[k] = ww
-        elif kind == "rate":
-            rhs[nc + k] += val
-            np.add.at(rhs, wc, wi * dp)
-            Cr.extend([k] * wc.size)
-            Cc.extend(wc.tolist())
-            Cv.extend((-wi).tolist())
-            D[k] = wi.sum()
-            rhs[nc + k] -= wi @ dp
-        else:
-            raise ValueError("Unsupported well type.")
-    C = sp.csr_array((Cv, (Cr, Cc)), shape=(nw, nc))
-    d = (d + np.bincount(cell_no[dF[cf]], Th[dF[cf]], minlength=nc)
-         + np.bincount(nbr[internal].ravel(order="F"), np.tile(ft[internal], 2), minlength=nc))
-    I = np.concatenate([nbr[internal, 0], nbr[internal, 1], np.arange(nc)])
-    J = np.concatenate([nbr[internal, 1], nbr[internal, 0], np.arange(nc)])
-    V = np.concatenate([-ft[internal], -ft[internal], d])
-    A = sp.csr_array((V, (I, J)), shape=(nc, nc))
-    A = sp.block_array([[A, C.T], [C, sp.diags_array(D, shape=(nw, nw))]], format="csr")
-    A.sum_duplicates()
-    A.sort_indices()
-    if not np.any(dF) and not any(str(w.type).lower() == "bhp" for w in wells):
-        diag = A.diagonal()
-        jpin = 0 if diag[0] > 0 else int(np.argmax(diag))
-        A = A.tolil()
-        A[jpin, jpin] = 2 * A[jpin, jpin]
-        A = A.tocsr()
-        A.sort_indices()
-    if MatrixOutput:
-        state.A, state.rhs = A, rhs
-    solve = LinSolve if LinSolve is not None else GpuLinSolve()
-    p = np.asarray(solve(A, rhs)).ravel()
-
-    # reconstruction (incomp_tpfa.py:186-211)
-    fpress = (np.bincount(cf, (p[cell_no] + grav) * Th, minlength=nf)
-              / np.bincount(cf, Th, minlength=nf))
-    bnd = np.any(nbr < 0, axis=1)
-    fpress[bnd] = fpress[bnd] - hh[bnd] / ft[bnd]
-    fpress[dF] = dC
-    ext = ~internal
-    sgn_b = 2.0 * (nbr[ext, 1] < 0) - 1.0
-    ni = nbr[internal]
-    flux = np.zeros(nf)
-    flux[internal] = -(ft[internal] * (p[ni[:, 1]] - p[ni[:, 0]] - fg[internal]))
-    cext = nbr[ext].max(axis=1)
-    fg_all = np.bincount(cf, grav, minlength=nf)
-    flux[ext] = -sgn_b * ft[ext] * (fpress[ext] - p[cext] - fg_all[ext])
-    state.pressure = p[:nc]
-    state.flux = flux
-    state.facePressure = fpress
-    for k, w in enumerate(wells):
-        wc = np.asarray(w.cells, dtype=np.int64).ravel()
-        well_sols[k].flux = np.asarray(w.WI, float).ravel() * totmob[wc] * (p[nc + k] + well_sols[k].cdp - p[wc])
-        well_sols[k].pressure = float(p[nc + k])
+    if nw:
+        pf = syst.perf_flux.cpu().numpy()
+        pdp = syst.perf_dp.cpu().numpy()
+        for k in range(nw):
+            a, b = syst._keep["perf_ptr"][k], syst._keep["perf_ptr"][k + 1]
+            well_sols[k].flux = pf[a:b].copy()
+            well_sols[k].cdp = pdp[a:b].copy()
+            well_sols[k].pressure = float(p[nc + k])
     if nw or well_sols:
         state.wellSol = well_sols
     return state

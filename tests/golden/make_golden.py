@@ -2,7 +2,11 @@
 
 Run once, where the reference's Python package is importable:
 
-    PYTHONPATH=<reference checkout> python tests/golden/make_golden.py [reference checkout]
+    python tests/golden/make_golden.py <reference checkout> [--only NAME,...]
+
+NAME selects fixture groups: small (the toy-grid fixtures), cfg0 (incomp_tpfa
+at 64x64x8), cfg1 (the first oil-water steps at 100x100x10), cfg4 (the
+adjoint at 64x64x4).  Without --only every group is written.
 
 It writes small .npz files holding inputs and the reference's own outputs
 (grid arrays, transmissibilities, oil-water residuals and Jacobians, Newton
@@ -18,8 +22,14 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).parent
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path(os.environ.get("PYMRST_REFERENCE", "/root/reference"))
+if len(sys.argv) < 2 or sys.argv[1].startswith("-"):
+    sys.exit(__doc__)
+REF = Path(sys.argv[1])
+ONLY = None
+if "--only" in sys.argv:
+    ONLY = set(sys.argv[sys.argv.index("--only") + 1].split(","))
 sys.path.insert(0, str(REF))
+sys.path.insert(1, str(HERE.parent.parent))  # the repository: the seeded case generators
 
 import scipy.io  # noqa: E402
 from scipy.ndimage import uniform_filter  # noqa: E402
@@ -264,14 +274,118 @@ def adjoint_fixture(name, dims, phys, seed, fluid_kind, gravity, nsteps, dt_days
          bhp_hist=np.vstack([s.bhp for s in res.states[1:]]), **wells0)
 
 
+def _sample_idx(n, k, seed):
+    """k sorted distinct indices of range(n), seeded (the entries a fixture keeps
+    of an array too large to store whole)."""
+    return np.sort(np.random.default_rng(seed).choice(n, size=min(k, n), replace=False))
+
+
+def cfg0_fixture():
+    """Benchmark config 0: incomp_tpfa on 64x64x8 cells of 10x10x2 m, the
+    seeded lognormal permeability, rate injector 1e-3 m^3/s down column
+    (0, 0), bhp producer at 100 bar down column (63, 63), gravity off."""
+    from pymrst.modules.incomp import incomp_tpfa, init_single_fluid
+    from pymrst.solvers import init_state
+    from pymrst_b200 import cases
+    dims = [64, 64, 8]
+    g = compute_geometry(cart_grid(dims, [640.0, 640.0, 16.0]))
+    perm = np.exp(cases.lognormal_logperm(dims, np.random.default_rng(0))).ravel(order="F") * MILLI * DARCY
+    rock = make_rock(g, perm[:, None], 0.2)
+    ht = compute_trans(g, rock)
+    fl = init_single_fluid(1 * CENTI * POISE, 1000.0)
+    nx, ny, nz = dims
+    w = add_well(None, g, rock, 0 + nx * (0 + ny * np.arange(nz)), well_type="rate", val=1e-3,
+                 radius=0.1, compi=np.array([1.0]))
+    w = add_well(w, g, rock, (nx - 1) + nx * ((ny - 1) + ny * np.arange(nz)), well_type="bhp",
+                 val=100 * BARSA, radius=0.1, compi=np.array([1.0]))
+    st = incomp_tpfa(init_state(g, w, 0.0), g, ht, fl, wells=w)
+    save("cfg0_incomp_64x64x8.npz", dims=np.array(dims), perm_sum=np.array(perm.sum()),
+         hT_sum=np.array(ht.sum()), p=st.pressure, flux=st.flux, facePressure=st.facePressure,
+         bhp=np.array([ws.pressure for ws in st.wellSol]),
+         wflux0=st.wellSol[0].flux, wflux1=st.wellSol[1].flux, **wells_arrays("w", w))
+
+
+def _five_spot_reference(case):
+    """The reference's model for a seeded five-spot case of the repository's
+    generator: same grid, rock, wells (the reference's add_well) and fluid."""
+    g = compute_geometry(cart_grid(list(case.grid.cartDims), list(np.asarray(case.grid.cartDims)
+                                                                   * _cell_size(case))))
+    rock = make_rock(g, np.asarray(case.rock.perm, float).reshape(g.cells.num, -1), np.asarray(case.rock.poro))
+    gvec = np.array([0.0, 0.0, case.gravity]) if case.gravity else None
+    w = None
+    for wc in case.wells:
+        w = add_well(w, g, rock, np.asarray(wc.cells), well_type=wc.type, val=float(np.ravel(wc.val)[0]),
+                     compi=np.asarray(wc.compi, float), sign=int(wc.sign), gravity=gvec)
+    model = TwoPhaseOilWaterModelAD(g, rock, ow_fluid("cfg"), w, gravity=case.gravity)
+    return g, rock, w, model
+
+
+def _cell_size(case):
+    c = np.asarray(case.grid.cells.centroids)
+    dims = case.grid.cartDims
+    return np.array([2 * c[0, 0], 2 * c[0, 1], 2 * c[0, 2]]) if np.prod(dims) else np.ones(3)
+
+
+def cfg1_fixture(nsteps=2):
+    """Benchmark config 1: the oil-water five-spot on 100x100x10 cells with
+    gravity, the first `nsteps` 10-day steps of the reference's own
+    simulate_schedule_ad with its default (direct) linear solver."""
+    import time
+    from pymrst_b200 import cases
+    case = cases.five_spot(dims=(100, 100, 10), seed=1)
+    g, rock, w, model = _five_spot_reference(case)
+    st0 = model.initial_state(case.p0, case.sw0)
+    t0 = time.perf_counter()
+    states, its = simulate_schedule_ad(st0, model, np.full(nsteps, case.dt), verbose=False)
+    el = time.perf_counter() - t0
+    save("cfg1_ow_100x100x10.npz", dims=np.array(case.grid.cartDims), perm_sum=np.array(np.sum(rock.perm)),
+         wi_sum=np.array(sum(np.sum(x.WI) for x in w)), its=np.asarray(its),
+         p_hist=np.vstack([s.pressure for s in states]), sw_hist=np.vstack([s.sW for s in states]),
+         qws_hist=np.vstack([s.qWs for s in states]), qos_hist=np.vstack([s.qOs for s in states]),
+         bhp_hist=np.vstack([s.bhp for s in states]), seconds=np.array(el))
+
+
+def cfg4_fixture(nsteps=30):
+    """Benchmark config 4: compute_gradient_adjoint on the 64x64x4 five-spot,
+    30 steps of 10 days, objective cumulative produced oil
+    (npv_objective(oil_price=1, water_cost=0, water_inj_cost=0)), controls the
+    wells' own targets held over the schedule."""
+    import time
+    from pymrst.modules.optimization.adjoint import compute_gradient_adjoint, npv_objective
+    from pymrst_b200 import cases
+    case = cases.five_spot(dims=(64, 64, 4), seed=4, nsteps=nsteps)
+    g, rock, w, model = _five_spot_reference(case)
+    st0 = model.initial_state(case.p0, case.sw0)
+    controls = np.tile([float(np.ravel(x.val)[0]) for x in w], (nsteps, 1))
+    dts = np.full(nsteps, case.dt)
+    t0 = time.perf_counter()
+    res = compute_gradient_adjoint(model, st0, dts, controls,
+                                   npv_objective(oil_price=1.0, water_cost=0.0, water_inj_cost=0.0))
+    el = time.perf_counter() - t0
+    save("cfg4_adjoint_64x64x4.npz", dims=np.array(case.grid.cartDims), perm_sum=np.array(np.sum(rock.perm)),
+         controls=controls, dts=dts, value=np.array(res.value), gradient=res.gradient,
+         p_final=res.states[-1].pressure, sw_final=res.states[-1].sW, seconds=np.array(el))
+
+
+
 if __name__ == "__main__":
-    grid_fixture()
-    assemble_fixture("ow_assemble_nograv.npz", [6, 5, 3], [60.0, 50.0, 6.0], 3, "p5", 0.0, False)
-    assemble_fixture("ow_assemble_grav.npz", [6, 5, 4], [60.0, 50.0, 8.0], 4, "cfg", 9.80665, False)
-    assemble_fixture("ow_assemble_xflow.npz", [5, 5, 6], [50.0, 50.0, 30.0], 5, "cfg", 9.80665, True)
-    newton_fixture("ow_newton_grav.npz", [8, 6, 4], [80.0, 60.0, 8.0], 6, "cfg", 9.80665, 4, 10.0)
-    newton_fixture("ow_newton_nograv.npz", [10, 8, 3], [100.0, 80.0, 6.0], 7, "p5", 0.0, 4, 20.0)
-    phase5_fixture()
-    incomp_fixtures()
-    adjoint_fixture("adjoint_grav.npz", [7, 6, 3], [70.0, 60.0, 6.0], 8, "cfg", 9.80665, 4, 15.0)
-    adjoint_fixture("adjoint_nograv.npz", [8, 5, 2], [80.0, 50.0, 4.0], 9, "p5", 0.0, 3, 20.0)
+    def want(name):
+        return ONLY is None or name in ONLY
+
+    if want("small"):
+        grid_fixture()
+        assemble_fixture("ow_assemble_nograv.npz", [6, 5, 3], [60.0, 50.0, 6.0], 3, "p5", 0.0, False)
+        assemble_fixture("ow_assemble_grav.npz", [6, 5, 4], [60.0, 50.0, 8.0], 4, "cfg", 9.80665, False)
+        assemble_fixture("ow_assemble_xflow.npz", [5, 5, 6], [50.0, 50.0, 30.0], 5, "cfg", 9.80665, True)
+        newton_fixture("ow_newton_grav.npz", [8, 6, 4], [80.0, 60.0, 8.0], 6, "cfg", 9.80665, 4, 10.0)
+        newton_fixture("ow_newton_nograv.npz", [10, 8, 3], [100.0, 80.0, 6.0], 7, "p5", 0.0, 4, 20.0)
+        phase5_fixture()
+        incomp_fixtures()
+        adjoint_fixture("adjoint_grav.npz", [7, 6, 3], [70.0, 60.0, 6.0], 8, "cfg", 9.80665, 4, 15.0)
+        adjoint_fixture("adjoint_nograv.npz", [8, 5, 2], [80.0, 50.0, 4.0], 9, "p5", 0.0, 3, 20.0)
+    if want("cfg0"):
+        cfg0_fixture()
+    if want("cfg4"):
+        cfg4_fixture()
+    if want("cfg1"):
+        cfg1_fixture()

@@ -1,7 +1,8 @@
 """Incompressible TPFA on the GPU against the reference's MATLAB goldens
 (the validate_phase2 cases, tolerance rtol 1e-9 with atol 1e-9 of the field
-maximum, as the reference checks them) and the reference's own incomp_tpfa
-on a case with wells."""
+maximum, as the reference checks them), the reference's own incomp_tpfa on
+a case with wells and on the 64x64x8 benchmark case, and the oracle's
+matrix and right-hand side (device assembly, entry by entry)."""
 
 import numpy as np
 import pytest
@@ -115,3 +116,121 @@ def test_default_device_solve_matches_reference_incomp_tpfa():
     close(st.pressure, d["p"], 1e-8)
     close(st.flux, d["flux"], 1e-8)
     close([ws.pressure for ws in st.wellSol], d["bhp"], 1e-8)
+
+
+# ---- the device assembly and reconstruction (pmb_tpfa_*) -------------------------------
+
+from oracle import incomp as oinc  # noqa: E402
+from test_oracle import _incomp_matlab_cases  # noqa: E402
+
+
+@pytest.mark.parametrize("case", ["qfs", "bc", "wells", "gravity"])
+def test_device_path_matches_matlab(case):
+    """Assembly, PCG solve and reconstruction all on the device."""
+    m = load("incomp_matlab.npz")
+    g, ht, bc, src, wells, gz = _incomp_matlab_cases()[case]
+    st = incomp_tpfa(init_state(g, wells, 0.0), g, ht, FLUID, bc=bc, src=src, wells=wells, gravity=gz,
+                     rtol=1e-14, maxiter=3000)
+    close(st.pressure, m[case + "__p"])
+    close(st.flux, m[case + "__flux"])
+    if case in ("qfs", "bc"):
+        close(st.facePressure, m[case + "__fp"])
+    if case == "wells":
+        close(st.wellSol[0].flux, m["wells__wflux1"])
+        close(st.wellSol[1].flux, m["wells__wflux2"])
+        close([ws.pressure for ws in st.wellSol], np.concatenate([m["wells__bhp1"], m["wells__bhp2"]]))
+
+
+def _matrix_vs_oracle(g, ht, bc, src, wells, gz, use_trans=False, mob=None, rho=(1000.0,), fluid=FLUID):
+    st = incomp_tpfa(init_state(g, wells, 0.0), g, ht, fluid, bc=bc, src=src, wells=wells, gravity=gz,
+                     MatrixOutput=True, use_trans=use_trans, rtol=1e-13, maxiter=3000)
+    if mob is None:
+        mob = np.full((g.cells.num, 1), 1.0 / (1 * CENTI * POISE))
+    A, rhs, aux = oinc.pressure_system(g, ht, mob, rho, gz, bc, src, wells, use_trans)
+    D = (st.A - A).tocsr()
+    scale = np.abs(A.data).max()
+    assert (np.abs(D.data).max() if D.nnz else 0.0) <= 1e-13 * scale
+    np.testing.assert_allclose(st.rhs, rhs, rtol=1e-12, atol=1e-13 * np.abs(rhs).max())
+    p = np.linalg.solve(A.toarray(), rhs) if A.shape[0] < 4000 else None
+    return st, p, aux
+
+
+@pytest.mark.parametrize("case", ["qfs", "bc", "wells", "gravity"])
+def test_device_matrix_and_rhs_equal_oracle(case):
+    g, ht, bc, src, wells, gz = _incomp_matlab_cases()[case]
+    _matrix_vs_oracle(g, ht, bc, src, wells, gz)
+
+
+def test_interface_transmissibilities_two_phases_and_pin():
+    """use_trans (one T per interface), a two-phase incompressible fluid with
+    per-cell mobilities, sources only (the pressure pin), and a rate well
+    whose mixture density follows the fractional flow of its cells."""
+    from types import SimpleNamespace
+    g = cartesian_grid([7, 5, 3], [70.0, 50.0, 6.0])
+    rng = np.random.default_rng(5)
+    k = np.exp(rng.normal(np.log(100.0), 0.5, g.cells.num)) * MILLI * DARCY
+    rock = make_rock(g, k[:, None], 0.2)
+    T = face_transmissibility_device(g, rock)[0]
+    sw = rng.uniform(0.0, 1.0, g.cells.num)
+    mu = np.array([1.0, 4.0]) * CENTI * POISE
+
+    class TwoPhase:
+        def properties(self, state=None):
+            return mu, np.array([1000.0, 850.0])
+
+        def saturation(self, state):
+            return np.column_stack([sw, 1 - sw])
+
+        def relperm(self, s):
+            return s ** 2
+
+    w = add_well(None, g, rock, [3, 38, 73], well_type="rate", val=-2e-4, radius=0.1,
+                 compi=np.array([0.0, 1.0]), gravity=GVEC)
+    src = add_source(None, [0, 104], [1e-4, 1e-4])
+    mob = np.column_stack([sw, 1 - sw]) ** 2 / mu
+    st, p, aux = _matrix_vs_oracle(g, T, None, src, w, GVEC, use_trans=True, mob=mob, rho=(1000.0, 850.0),
+                                   fluid=TwoPhase())
+    fp, flux, wflux = oinc.reconstruct(g, p, aux, w)
+    close(st.pressure, p[:g.cells.num], 1e-8)
+    close(st.flux, flux, 1e-8)
+    close(st.wellSol[0].flux, wflux[0], 1e-8)
+
+
+def test_reduce_gives_the_same_pressures_and_the_schur_system():
+    m = load("incomp_matlab.npz")
+    g, ht, bc, src, wells, gz = _incomp_matlab_cases()["wells"]
+    st = incomp_tpfa(init_state(g, wells, 0.0), g, ht, FLUID, wells=wells, gravity=gz, reduce=True,
+                     rtol=1e-14, maxiter=3000)
+    close(st.pressure, m["wells__p"])
+    assert st.A.shape == (g.cells.num, g.cells.num) and st.rhs.shape == (g.cells.num,)
+    p_r = np.linalg.solve(st.A.toarray(), st.rhs)
+    close(p_r, m["wells__p"])
+
+
+def test_assembly_is_bitwise_repeatable():
+    g, ht, bc, src, wells, gz = _incomp_matlab_cases()["wells"]
+    a = incomp_tpfa(init_state(g, wells, 0.0), g, ht, FLUID, wells=wells, gravity=gz, MatrixOutput=True)
+    b = incomp_tpfa(init_state(g, wells, 0.0), g, ht, FLUID, wells=wells, gravity=gz, MatrixOutput=True)
+    assert np.array_equal(a.A.data, b.A.data) and np.array_equal(a.rhs, b.rhs)
+    assert np.array_equal(a.pressure, b.pressure) and np.array_equal(a.flux, b.flux)
+
+
+def test_benchmark_case_64x64x8_matches_reference():
+    """Benchmark config 0: 32,768 cells, rate injector and bhp producer down
+    opposite corner columns, gravity off; against the reference's own
+    incomp_tpfa (SuperLU) output."""
+    from pymrst_b200 import cases
+    d = load("cfg0_incomp_64x64x8.npz")
+    g = cartesian_grid([64, 64, 8], [640.0, 640.0, 16.0])
+    perm = np.exp(cases.lognormal_logperm((64, 64, 8), np.random.default_rng(0))).ravel(order="F") * MILLI * DARCY
+    rock = make_rock(g, perm[:, None], 0.2)
+    ht = half_trans(g, rock)
+    np.testing.assert_allclose(ht.sum(), d["hT_sum"], rtol=1e-13)
+    wells = wells_from(d)
+    st = incomp_tpfa(init_state(g, wells, 0.0), g, ht, FLUID, wells=wells, rtol=1e-14, maxiter=3000)
+    close(st.pressure, d["p"])
+    close(st.flux, d["flux"])
+    close(st.facePressure, d["facePressure"])
+    close([ws.pressure for ws in st.wellSol], d["bhp"])
+    close(st.wellSol[0].flux, d["wflux0"])
+    close(st.wellSol[1].flux, d["wflux1"])

@@ -133,3 +133,86 @@ def test_oracle_adjoint_matches_reference(name):
         ref = d["gradient"][:, j]
         assert np.abs(res.gradient[:, j] - ref).max() <= 1e-6 * np.abs(ref).max()
     assert np.abs(res.initial_state_gradient - d["dx0"]).max() <= 1e-6 * np.abs(d["dx0"]).max()
+
+
+# ---- incompressible TPFA -----------------------------------------------------------
+
+def _incomp_close(mine, ref, rtol=1e-9):
+    mine = np.asarray(mine, float).ravel()
+    ref = np.asarray(ref, float).ravel()
+    np.testing.assert_allclose(mine, ref, rtol=rtol, atol=rtol * max(np.abs(ref).max(), 1e-300) + 1e-15)
+
+
+def _incomp_matlab_cases():
+    """The four MATLAB incompTPFA golden cases (validate_phase2's setups):
+    name -> (grid, half-face T, bc, src, wells, gravity vector)."""
+    from pymrst_b200.params import BARSA, DARCY, MILLI, add_bc, add_source, add_well
+    gz = np.array([0.0, 0.0, 9.80665])
+    out = {}
+    g = cartesian_grid([32, 32, 1], [500.0, 500.0, 10.0])
+    rock = make_rock(g, ((10 + (7 * np.arange(g.cells.num)) % 100) * MILLI * DARCY)[:, None], 0.2)
+    src = add_source(add_source(None, [0], 1e-3), [g.cells.num - 1], -1e-3)
+    out["qfs"] = (g, otrans.compute_trans(g, rock), None, src, [], None)
+    g = cartesian_grid([20, 10, 5], [200.0, 100.0, 50.0])
+    rock = make_rock(g, ((1 + (3 * np.arange(g.cells.num)) % 50) * MILLI * DARCY)[:, None], 0.25)
+    bd = np.any(g.faces.neighbors == -1, axis=1)
+    fc = g.faces.centroids
+    bc = add_bc(None, np.flatnonzero(bd & (fc[:, 0] < 1e-10)), "pressure", 200 * BARSA)
+    bc = add_bc(bc, np.flatnonzero(bd & (fc[:, 0] > 200 - 1e-10)), "pressure", 100 * BARSA)
+    bc = add_bc(bc, np.flatnonzero(bd & (fc[:, 1] < 1e-10)), "flux", 1e-6)
+    out["bc"] = (g, otrans.compute_trans(g, rock), bc, None, [], None)
+    g = cartesian_grid([10, 10, 3], [1000.0, 1000.0, 30.0])
+    rock = make_rock(g, np.tile(np.array([100.0, 100.0, 10.0]) * MILLI * DARCY, (g.cells.num, 1)), 0.3)
+    w = add_well(None, g, rock, [0, 100, 200], well_type="rate", val=5e-3, radius=0.1,
+                 compi=np.array([1.0]), gravity=gz)
+    w = add_well(w, g, rock, [99, 199, 299], well_type="bhp", val=100 * BARSA, radius=0.1,
+                 compi=np.array([1.0]), gravity=gz)
+    out["wells"] = (g, otrans.compute_trans(g, rock), None, None, w, gz)
+    g = cartesian_grid([1, 1, 30], [1.0, 1.0, 300.0])
+    rock = make_rock(g, 100 * MILLI * DARCY, 0.2)
+    bd = np.any(g.faces.neighbors == -1, axis=1)
+    bc = add_bc(None, np.flatnonzero(bd & (g.faces.centroids[:, 2] < 1e-10)), "pressure", 100 * BARSA)
+    out["gravity"] = (g, otrans.compute_trans(g, rock), bc, None, [], gz)
+    return out
+
+
+@pytest.mark.parametrize("case", ["qfs", "bc", "wells", "gravity"])
+def test_oracle_incomp_matches_matlab(case):
+    from oracle import incomp as oinc
+    from pymrst_b200.params import CENTI, POISE
+    m = load("incomp_matlab.npz")
+    g, ht, bc, src, wells, gz = _incomp_matlab_cases()[case]
+    mob = np.full((g.cells.num, 1), 1.0 / (1 * CENTI * POISE))
+    p, bhp, fp, flux, wflux = oinc.incomp_tpfa(g, ht, mob, [1000.0], gz, bc, src, wells)
+    _incomp_close(p, m[case + "__p"])
+    _incomp_close(flux, m[case + "__flux"])
+    if case in ("qfs", "bc"):
+        _incomp_close(fp, m[case + "__fp"])
+    if case == "wells":
+        _incomp_close(wflux[0], m["wells__wflux1"])
+        _incomp_close(wflux[1], m["wells__wflux2"])
+        _incomp_close(bhp, np.concatenate([m["wells__bhp1"], m["wells__bhp2"]]))
+
+
+def test_oracle_incomp_matches_reference_at_64x64x8():
+    """Benchmark config 0 (32,768 cells), against the reference's own
+    incomp_tpfa output."""
+    from oracle import incomp as oinc
+    from pymrst_b200 import cases
+    from pymrst_b200.params import CENTI, DARCY, MILLI, POISE
+    from fixtures import wells_from
+    d = load("cfg0_incomp_64x64x8.npz")
+    g = cartesian_grid([64, 64, 8], [640.0, 640.0, 16.0])
+    perm = np.exp(cases.lognormal_logperm((64, 64, 8), np.random.default_rng(0))).ravel(order="F") * MILLI * DARCY
+    assert np.isclose(perm.sum(), float(d["perm_sum"]), rtol=1e-14)
+    ht = otrans.compute_trans(g, make_rock(g, perm[:, None], 0.2))
+    assert np.isclose(ht.sum(), float(d["hT_sum"]), rtol=1e-13)
+    wells = wells_from(d)
+    mob = np.full((g.cells.num, 1), 1.0 / (1 * CENTI * POISE))
+    p, bhp, fp, flux, wflux = oinc.incomp_tpfa(g, ht, mob, [1000.0], None, None, None, wells)
+    _incomp_close(p, d["p"])
+    _incomp_close(bhp, d["bhp"])
+    _incomp_close(flux, d["flux"])
+    _incomp_close(fp, d["facePressure"])
+    _incomp_close(wflux[0], d["wflux0"])
+    _incomp_close(wflux[1], d["wflux1"])
