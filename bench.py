@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--dims", default=None, help="override grid dims, e.g. 30,110,40")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison arm")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the measurements of the other benchmark configurations")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--cpr", default="", help="CPR option overrides, e.g. amg_cycle=2,local_sweeps=1")
     ap.add_argument("--probe", type=int, default=0,
@@ -257,6 +259,121 @@ def kernel_roofline(model, x, x0, dt, torch, N, reps=20):
     return out
 
 
+# ---------------------------------------------------------------------------
+# The other benchmark configurations, measured beside the headline one
+# ---------------------------------------------------------------------------
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def measure_incomp(torch, reps=5):
+    """Config 0: incomp_tpfa on the 64x64x8 (32,768-cell) quarter five-spot,
+    gravity off.  GPU: the public call (host arrays in and out, device
+    assembly, PCG-AMG solve and reconstruction) and the device part alone,
+    both CUDA-event timed after a warm-up call; CPU: the oracle's numpy
+    assembly with SuperLU (the reference's algorithm), one run."""
+    from oracle import incomp as oinc
+    from pymrst_b200 import cases
+    from pymrst_b200.incomp import _system, incomp_tpfa, init_single_fluid, init_state
+    from pymrst_b200.ow_model import face_transmissibility_device
+    c = cases.incompressible_quarter_five_spot()
+    ht = face_transmissibility_device(c.grid, c.rock)[1]
+    fluid = init_single_fluid(c.mu, c.rho)
+    st0 = init_state(c.grid, c.wells, 0.0)
+    run = lambda: incomp_tpfa(st0, c.grid, ht, fluid, wells=c.wells, rtol=1e-12, maxiter=1000)
+    st = run()
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    e0.record()
+    for _ in range(reps):
+        st = run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / reps
+    syst = _system(c.grid, c.wells, False)
+    mob = np.full((c.grid.cells.num, 1), 1.0 / c.mu)
+
+    def device_part():
+        syst.solve_device(1e-12, 1000)
+        syst.reconstruct()
+
+    device_part()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        device_part()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_dev = e0.elapsed_time(e1) / reps
+    t0 = time.perf_counter()
+    p_ref, bhp_ref, fp_ref, flux_ref, _ = oinc.incomp_tpfa(c.grid, ht, mob, [c.rho], None, None, None, c.wells)
+    ms_cpu = (time.perf_counter() - t0) * 1e3
+    return {"workload": "incompressible TPFA, 64x64x8 (32,768 cells), rate injector + bhp producer",
+            "gpu_ms_per_call_e2e": ms_e2e, "gpu_ms_solve_and_reconstruct": ms_dev,
+            "pcg_iterations": syst.last_iterations, "cpu_ms": ms_cpu,
+            "cpu": "oracle restatement of incomp_tpfa (numpy assembly, SuperLU), one core",
+            "speedup_e2e": ms_cpu / ms_e2e,
+            "max_rel_pressure_vs_cpu": float(np.abs(st.pressure - p_ref).max() / np.abs(p_ref).max()),
+            "max_rel_flux_vs_cpu": float(np.abs(st.flux - flux_ref).max() / np.abs(flux_ref).max())}
+
+
+def measure_ow_fp64(torch, N, GpuOilWaterModel, run_report_step, cpu_budget=20.0):
+    """Config 1: the FP64 oil-water five-spot on 100x100x10 cells, 20 steps of
+    10 days from the initial state, all FP64 (library-default CPR); the
+    whole schedule CUDA-event timed after a one-step warm-up on a copy.  CPU:
+    Newton iterations of its first step by the oracle with SuperLU, at full
+    size (one iteration, about 25 s on one core)."""
+    import scipy.sparse.linalg as spla
+    from oracle import ow as oow
+    from pymrst_b200 import cases
+    case = cases.five_spot(dims=(100, 100, 10), seed=1)
+    model = GpuOilWaterModel(case.grid, case.rock, case.fluid, case.wells, gravity=case.gravity,
+                             cpr_options=dict(precision=0))
+    x = model.to_device(model.initial_state(case.p0, case.sw0))
+    warm = x.clone()
+    model.step_device(warm, case.dt)
+    model.reset_cdp()
+    saved = x.clone()
+
+    def attempt(h):
+        saved.copy_(x)
+        ok, nit, _ = model.step_device(x, h)
+        if not ok:
+            x.copy_(saved)
+        return ok, nit
+
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    its = 0
+    e0.record()
+    for _ in range(case.nsteps):
+        its += run_report_step(attempt, case.dt, max_cuts=6)[0]
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) * 1e-3
+    prob = oow.build_problem(case.grid, case.rock, case.fluid.params, case.wells, gravity=case.gravity)
+    st0 = oow.initial_state(prob, case.p0, case.sw0)
+    st = st0.copy()
+    cdp = oow.compute_cdp(prob, st0)
+    t0 = time.perf_counter()
+    cits = 0
+    while True:
+        res, J = oow.assemble(prob, st0, st, case.dt, cdp)
+        oow.apply_update(prob, st, spla.spsolve(J.tocsc(), -res))
+        cits += 1
+        if time.perf_counter() - t0 >= cpu_budget or cits >= 25:
+            break
+    csec = time.perf_counter() - t0
+    gpu_v = model.nc * its / sec
+    cpu_v = prob.nc * cits / csec
+    return {"workload": "oil-water five-spot 100x100x10 (100,000 cells), 20 x 10 days, FP64",
+            "value": gpu_v, "unit": UNIT, "ms_per_step": sec / case.nsteps * 1e3, "newton_iterations": its,
+            "cpu_value": cpu_v, "cpu": f"oracle (numpy assembly, SuperLU) on the full model: {cits} Newton "
+                                       f"iteration(s) of the first step in {csec:.1f} s, one core",
+            "speedup": gpu_v / cpu_v}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -449,6 +566,15 @@ def run_ours(args):
     del snaps
 
     kr = kernel_roofline(model, x, x_e2e_start, dt, torch, N)
+    configs = {}
+    if not args.no_configs and rank == 0 and world == 1:
+        for name, fn in (("incomp_64x64x8", lambda: measure_incomp(torch)),
+                         ("ow_fp64_100x100x10", lambda: measure_ow_fp64(torch, N, GpuOilWaterModel, run_report_step,
+                                                                        args.cpu_budget))):
+            try:
+                configs[name] = fn()
+            except Exception as e:  # a secondary measurement must not hide the headline line
+                configs[name] = {"error": f"{type(e).__name__}: {e}"}
     peak, peak_kind = peaks()
     # whole-step algorithmic bytes from the recorded counts: per Newton
     # iteration the assembly, the convergence check and update, and one
@@ -503,6 +629,8 @@ def run_ours(args):
                                      for k, v in kr.items() if k != "cpr_bytes"}},
             "clocks": clocks.summary(),
         }
+        if configs:
+            line["other_configs"] = configs
         if fp64 is not None:
             line["fp64"] = fp64
             line["mixed_vs_fp64"] = mixed_vs_fp64

@@ -120,6 +120,39 @@ int pmb_ow_reset_cdp(pmb_ow* h);
  * gradient with respect to permeability uses.  Uses the model's residual
  * workspace (not during a step on the same handle). */
 int pmb_ow_fluxes(pmb_ow* h, const double* d_x, const double* d_cdp, double* d_face_flux, double* d_perf_rate);
+/* Adjoint pieces (compute_gradient_adjoint, pymrst/modules/optimization/
+ * adjoint.py:163-225), all on the device and in the reference's
+ * variable-blocked layout [p (nc), sW (nc), qWs, qOs, bhp (nw each)]:
+ * pmb_ow_prev_jacobian_tmul: d_y = (dR_{n+1}/dx_n)^T d_lam, the coupling of
+ *   step n+1 to its start state x_n (d_x_prev, cell-major) through the
+ *   accumulation terms (_jac_wrt_previous, adjoint.py:83-105), dt the step
+ *   n+1; the well entries of d_y are 0.
+ * pmb_ow_csr_values: values of a CSR matrix (the Jacobian, or its transpose,
+ *   on a pattern the caller built once) whose entry e is the sum over terms
+ *   d_ptr[e] .. d_ptr[e+1]-1: t >= 0 is d_jac[t] (t < 4 nnzb) or
+ *   d_well[t - 4 nnzb]; t < 0 encodes -1 - ((i nperf + j) 4 + 2a + b), entry
+ *   (a, b) of the cross-flow product Up_i Vp_j of perforations i, j of one
+ *   well (counted where that well's mixture coupling is on).  This is the
+ *   device counterpart of combine_equations (pymrst/utils/adi/operators.py:
+ *   204-211) on the model's block layout.
+ * pmb_ow_perm_contract: d_out[c] += lam^T dR/d(log k_c) at d_x with the
+ *   well pressure drops 0, through every interface transmissibility of c
+ *   (dT_f/dlog k_c = T_f^2 / t_{c,f}; d_t0 / d_t1 the half-face T of N[f,0] /
+ *   N[f,1], nf each) and the well indices of c's perforations; no reference
+ *   counterpart (its adjoint has no permeability gradient).  d_face_flux
+ *   (2 nf) and d_perf_rate (2 nperf) are scratch.
+ * pmb_ow_get_last_cdp / pmb_ow_set_last_cdp: the previous timestep's well
+ *   pressure drops that the next pmb_ow_compute_cdp starts from (nperf
+ *   values; *h_have = 0 when there are none; d_in NULL forgets them): what
+ *   a forward segment recomputed from a checkpoint must be given to take
+ *   the same steps again. */
+int pmb_ow_prev_jacobian_tmul(pmb_ow* h, const double* d_x_prev, double dt, const double* d_lam, double* d_y);
+int pmb_ow_csr_values(pmb_ow* h, const double* d_jac, const double* d_well, int64_t n, const int64_t* d_ptr,
+                      const int64_t* d_terms, double* d_vals);
+int pmb_ow_perm_contract(pmb_ow* h, const double* d_x, const double* d_lam, const double* d_t0, const double* d_t1,
+                         double* d_face_flux, double* d_perf_rate, double* d_out);
+int pmb_ow_get_last_cdp(pmb_ow* h, double* d_out, int32_t* h_have);
+int pmb_ow_set_last_cdp(pmb_ow* h, const double* d_in);
 /* New well targets, one per well: bhp for bhp wells, total surface rate for
  * rate wells (_set_controls, pymrst/modules/optimization/adjoint.py:63-65,
  * which sets w.val between timesteps).  Also rescales the well convergence
@@ -270,6 +303,14 @@ int pmb_csr_cpr_solve(pmb_csr_cpr* h, const double* d_b, double* d_x, double* h_
 /* y = A x with the values d_values on the handle's pattern. */
 int pmb_csr_spmv(pmb_csr_cpr* h, const double* d_values, const double* d_x, double* d_y);
 int pmb_csr_cpr_levels(const pmb_csr_cpr* h, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
+
+/* Each row of the CSR matrix (device row pointers, values) divided by its
+ * largest |entry|; d_scale[r] receives the factor (1 for an empty or zero
+ * row).  The transposed adjoint systems need it: the rows of J^T span many
+ * orders of magnitude (well-control columns of J are O(1), cell columns
+ * O(1e-10)), and unit rows make the Krylov residual test uniform.  No
+ * reference counterpart (the reference solves J^T directly). */
+int pmb_csr_row_scale(int32_t n, const int32_t* d_row_ptr, double* d_vals, double* d_scale, void* stream);
 
 /* d_inv = d_a^-1 for a dense row-major n x n FP64 matrix (1 <= n <= 4096),
  * the AMG coarsest-level solver: Gauss-Jordan with row pivoting.  Returns

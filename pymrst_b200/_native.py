@@ -87,6 +87,11 @@ SIGNATURES = {
     "pmb_ow_compute_cdp": (c_int, [c_vp, c_vp, c_vp]),
     "pmb_ow_reset_cdp": (c_int, [c_vp]),
     "pmb_ow_set_controls": (c_int, [c_vp, P_dbl]),
+    "pmb_ow_prev_jacobian_tmul": (c_int, [c_vp, c_vp, c_dbl, c_vp, c_vp]),
+    "pmb_ow_csr_values": (c_int, [c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp]),
+    "pmb_ow_perm_contract": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "pmb_ow_get_last_cdp": (c_int, [c_vp, c_vp, P_i32]),
+    "pmb_ow_set_last_cdp": (c_int, [c_vp, c_vp]),
     "pmb_ow_fluxes": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_ow_assemble": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp, c_vp, c_int]),
     "pmb_ow_spmv": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
@@ -109,6 +114,7 @@ SIGNATURES = {
     "pmb_csr_cpr_setup": (c_int, [c_vp, c_vp, P_dbl]),
     "pmb_csr_cpr_solve": (c_int, [c_vp, c_vp, c_vp, P_dbl]),
     "pmb_csr_spmv": (c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "pmb_csr_row_scale": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp]),
     "pmb_csr_cpr_levels": (c_int, [c_vp, c_int, P_i64, P_i32]),
     "pmb_pcg_create": (c_int, [c_int, P_i32, P_i32, c_dbl, c_int, c_vp, C.POINTER(c_vp)]),
     "pmb_pcg_destroy": (c_int, [c_vp]),

@@ -13,6 +13,11 @@ value distributions (all seeded with numpy's default_rng):
   sinusoidal channels (2000 mD in 1 mD) with amplitude, wavelength and width
   drawn per layer; porosity 0.05 + 0.30 * normalised log-permeability; same
   well pattern.
+* `incompressible_quarter_five_spot(dims=(64, 64, 8), cell_size=(10, 10, 2),
+  seed)`: the lognormal permeability (sigma 1) of `five_spot`, porosity 0.2,
+  one rate injector of 1e-3 m^3/s down column (0, 0) and one bhp producer at
+  100 bar down the opposite corner column, a single-phase fluid of 1 cP and
+  1000 kg/m^3; gravity off.
 * `ow_fluid()`: Corey n = 2 with Swc = Sor = 0.1, mu_w = 1 cP, mu_o = 5 cP,
   rho 1000 / 800 kg/m^3, compressibility 1e-5 / bar for both phases,
   p_ref = 200 bar.
@@ -157,3 +162,28 @@ def ensemble_realisations(n: int = 256, seed: int = 3, nx_range=(16, 64), nz_ran
         out.append(five_spot(dims=(nx, ny, nz), cell_size=cell_size, seed=int(rng.integers(1 << 30)),
                              nsteps=nsteps, dt_days=dt_days, gravity=gravity, pv_fraction=pv_fraction))
     return out
+
+
+@dataclass
+class IncompCase:
+    name: str
+    grid: Grid
+    rock: Rock
+    wells: List[Well]
+    mu: float
+    rho: float
+
+
+def incompressible_quarter_five_spot(dims=(64, 64, 8), cell_size=(10.0, 10.0, 2.0), seed=0) -> IncompCase:
+    rng = np.random.default_rng(seed)
+    dims = tuple(int(v) for v in dims)
+    g = cartesian_grid(dims, [d * s for d, s in zip(dims, cell_size)])
+    perm = np.exp(lognormal_logperm(dims, rng, 1.0)).ravel(order="F") * MD
+    rock = make_rock(g, perm[:, None], 0.2)
+    nx, ny, nz = dims
+    k = np.arange(nz)
+    wells = add_well(None, g, rock, cell_index(g, 0, 0, k), well_type="rate", val=1e-3, radius=0.1,
+                     compi=np.array([1.0]))
+    wells = add_well(wells, g, rock, cell_index(g, nx - 1, ny - 1, k), well_type="bhp", val=100 * BARSA,
+                     radius=0.1, compi=np.array([1.0]))
+    return IncompCase(f"incomp_{nx}x{ny}x{nz}", g, rock, wells, 1 * CENTI * POISE, 1000.0)

@@ -262,17 +262,30 @@ inline int lanes_for(long long n, long long nnz) {
 
 // Coefficients of step `step` of the Chebyshev recurrence on [lm/10, lm].
 __device__ __forceinline__ void cheb_coeffs(double lm, int step, double& c1, double& c2) {
-  const double lo = lm / 10.0;
-  const double theta = 0.5 * (lm + lo), delta = 0.5 * (lm - lo), sigma = theta / delta;
-  double rho = 1.0 / sigma;
+  // explicit roundings: the per-step and the cluster tail kernels must agree
+  const double lo = __ddiv_rn(lm, 10.0);
+  const double theta = __dmul_rn(0.5, __dadd_rn(lm, lo)), delta = __dmul_rn(0.5, __dsub_rn(lm, lo));
+  const double sigma = __ddiv_rn(theta, delta);
+  double rho = __ddiv_rn(1.0, sigma);
   c1 = 0.0;
-  c2 = 1.0 / theta;
+  c2 = __ddiv_rn(1.0, theta);
   for (int k = 1; k <= step; ++k) {
-    const double rho1 = 1.0 / (2.0 * sigma - rho);
-    c1 = rho1 * rho;
-    c2 = 2.0 * rho1 / delta;
+    const double rho1 = __ddiv_rn(1.0, __dsub_rn(__dmul_rn(2.0, sigma), rho));
+    c1 = __dmul_rn(rho1, rho);
+    c2 = __ddiv_rn(__dmul_rn(2.0, rho1), delta);
     rho = rho1;
   }
+}
+
+// The arithmetic of one Chebyshev row update, shared by the per-step kernels
+// and the cluster tail kernel below so that both produce the same bits:
+// explicit roundings leave the compiler no choice of contraction.
+__device__ __forceinline__ double cheb_res(double b, double ax, double dinv) {
+  return __dmul_rn(__dsub_rn(b, ax), dinv);
+}
+__device__ __forceinline__ double cheb_dir(int step, double c1, double c2, double d_old, double r) {
+  const double t = __dmul_rn(c2, r);
+  return step == 0 ? t : __fma_rn(c1, d_old, t);
 }
 
 // Chebyshev on D^{-1} A over [lmax/10, lmax]: step `step` of the
@@ -285,7 +298,7 @@ template <class T, bool PRO>
 __device__ __forceinline__ double cheb_x(const T* __restrict__ xin, const int* __restrict__ agg,
                                          const T* __restrict__ xc, int j) {
   if (!PRO) return (double)xin[j];
-  return (double)(T)((double)xin[j] + (double)xc[agg[j]]);
+  return (double)(T)__dadd_rn((double)xin[j], (double)xc[agg[j]]);
 }
 
 template <class T, bool ZERO, int LANES, bool PRO = false>
@@ -305,16 +318,16 @@ __global__ void __launch_bounds__(256) cheb_step_kernel(int n, const int* __rest
   if (!ZERO) {
     if (i < n)
       for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES)
-        ax += (double)a[k] * cheb_x<T, PRO>(xin, agg, xc, ci[k]);
+        ax = __fma_rn((double)a[k], cheb_x<T, PRO>(xin, agg, xc, ci[k]), ax);
     ax = group_sum<LANES>(ax);
   }
   __syncthreads();
   if (i >= n || sub != 0) return;
   const double c1 = s_c[0], c2 = s_c[1];
-  const double r = ((double)b[i] - ax) * (double)dinv[i];
-  const double dn = (step == 0 ? 0.0 : c1 * (double)d[i]) + c2 * r;
+  const double r = cheb_res((double)b[i], ax, (double)dinv[i]);
+  const double dn = cheb_dir(step, c1, c2, step == 0 ? 0.0 : (double)d[i], r);
   d[i] = (T)dn;
-  xout[i] = (T)((ZERO ? 0.0 : cheb_x<T, PRO>(xin, agg, xc, (int)i)) + dn);
+  xout[i] = (T)__dadd_rn(ZERO ? 0.0 : cheb_x<T, PRO>(xin, agg, xc, (int)i), dn);
 }
 
 // b_c[I] = sum over members i of (b_i - (A x)_i); LANES threads per aggregate
@@ -366,15 +379,15 @@ __global__ void __launch_bounds__(256) restrict_rows_kernel(const int* __restric
     double s = 0.0;
     if (m < m1) {
       i = cmem[m];
-      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s -= (double)a[k] * (double)x[ci[k]];
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s = __fma_rn(-(double)a[k], (double)x[ci[k]], s);
     }
     s = group_sum<LANES>(s);
-    if (m < m1 && sub == 0) rr_smem[m - m0] = (double)b[i] + s;
+    if (m < m1 && sub == 0) rr_smem[m - m0] = __dadd_rn((double)b[i], s);
   }
   __syncthreads();
   for (int I = I0 + threadIdx.x; I < I1; I += blockDim.x) {
     double v = 0.0;
-    for (int m = cptr[I]; m < cptr[I + 1]; ++m) v += rr_smem[m - m0];
+    for (int m = cptr[I]; m < cptr[I + 1]; ++m) v = __dadd_rn(v, rr_smem[m - m0]);
     bc[I] = (T)v;
   }
 }
@@ -385,7 +398,7 @@ __global__ void prolong_add_kernel(int n, const int* __restrict__ agg, const T* 
   pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  x[i] = (T)((double)x[i] + (double)xc[agg[i]]);
+  x[i] = (T)__dadd_rn((double)x[i], (double)xc[agg[i]]);
 }
 
 template <class T>
@@ -562,9 +575,181 @@ __global__ void dense_apply_kernel(int n, const double* __restrict__ Inv, const 
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= n) return;
   double s = 0.0;
-  for (int j = lane; j < n; j += 32) s += Inv[(size_t)row * n + j] * (double)b[j];
+  for (int j = lane; j < n; j += 32) s = __fma_rn(Inv[(size_t)row * n + j], (double)b[j], s);
   s = warp_sum(s);
   if (lane == 0) x[row] = (T)s;
+}
+
+// Sum over a group of `lanes` consecutive lanes (a power of two <= 32), the
+// order of group_sum<LANES>.
+__device__ __forceinline__ double group_sum_rt(double v, int lanes) {
+  for (int o = lanes >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Cluster tail cycle --------------------------------------------------------
+//
+// The V-cycle from level `first` (the first level below the K-cycle levels)
+// down to the dense coarsest solve runs as ONE launch of one thread-block
+// cluster: the steps of the per-step path (Chebyshev steps, member residuals,
+// aggregate sums, the dense coarsest product, the post-smoothing with the
+// prolongation folded into its first step) separated by the hardware cluster
+// barrier instead of kernel boundaries.  Each step uses the same row grouping,
+// summation order and explicit roundings as its per-step kernel, and the
+// same buffers, so the result is bitwise that of the per-step path.  The
+// tail levels are small (the largest a few tens of thousands of rows) and
+// L2-resident; launched per step they are latency-bound, at 5 to 10 us per
+// kernel, and under the K-cycle every cycle visits them 8 times.
+//
+// Vectors written inside the kernel are read with ld.global.cg (L2, never a
+// stale L1 line of another SM); the barrier orders the writes before it.
+constexpr int kTailThreads = 1024;
+constexpr int kTailMaxRows = 65536;
+
+template <class T>
+struct TailLevel {
+  int n, lanes, steps;
+  const int* rp;
+  const int* ci;
+  const T* val;
+  const T* dinv;
+  const double* lmax;
+  T* b;  // right-hand side (level below the first: written by the restriction)
+  T* x;
+  T* d;  // Chebyshev direction
+  T* t;
+  T* u;
+  const int* cptr;  // members of each aggregate of the next level
+  const int* cmem;
+  const int* agg;
+};
+
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+template <class T>
+__device__ __forceinline__ double ldv(const T* p) {
+  return (double)__ldcg(p);
+}
+
+template <class T, bool ZERO, bool PRO>
+__device__ void tail_cheb(const TailLevel<T>& L, const T* b, const T* xin, T* xout, int step, const T* xc,
+                          long long tid, long long nthr) {
+  double c1, c2;
+  cheb_coeffs(L.lmax[0], step, c1, c2);
+  const int LN = L.lanes;
+  const long long total = ((long long)L.n * LN + 31) / 32 * 32;
+  for (long long t = tid; t < total; t += nthr) {
+    const long long i = t / LN;
+    const int sub = (int)(t % LN);
+    double ax = 0.0;
+    if (!ZERO) {
+      if (i < L.n)
+        for (int k = L.rp[i] + sub; k < L.rp[i + 1]; k += LN) {
+          const int j = L.ci[k];
+          const double xv = PRO ? (double)(T)__dadd_rn(ldv(xin + j), ldv(xc + L.agg[j])) : ldv(xin + j);
+          ax = __fma_rn((double)L.val[k], xv, ax);
+        }
+      ax = group_sum_rt(ax, LN);
+    }
+    if (i < L.n && sub == 0) {
+      const double r = cheb_res(ldv(b + i), ax, (double)L.dinv[i]);
+      const double dn = cheb_dir(step, c1, c2, step == 0 ? 0.0 : ldv(L.d + i), r);
+      double xo = 0.0;
+      if (!ZERO) xo = PRO ? (double)(T)__dadd_rn(ldv(xin + i), ldv(xc + L.agg[i])) : ldv(xin + i);
+      L.d[i] = (T)dn;
+      xout[i] = (T)__dadd_rn(xo, dn);
+    }
+  }
+  cluster_barrier();
+}
+
+// AMG<T>::smooth, step for step (the same output buffer of every step)
+template <class T>
+__device__ void tail_smooth(const TailLevel<T>& L, const T* b, T* x, bool zero_start, const T* xc, long long tid,
+                            long long nthr) {
+  const int steps = L.steps;
+  T* cur = x;
+  int step = 0;
+  if (zero_start) {
+    T* out = (steps % 2 == 1) ? x : L.t;
+    tail_cheb<T, true, false>(L, b, nullptr, out, 0, nullptr, tid, nthr);
+    cur = out;
+    step = 1;
+  }
+  for (; step < steps; ++step) {
+    T* out = ((steps - 1 - step) % 2 == 0) ? x : L.t;
+    if (out == cur) out = L.u;
+    if (xc && step == 0)
+      tail_cheb<T, false, true>(L, b, cur, out, step, xc, tid, nthr);
+    else
+      tail_cheb<T, false, false>(L, b, cur, out, step, nullptr, tid, nthr);
+    cur = out;
+  }
+  if (cur != x) {
+    for (long long i = tid; i < L.n; i += nthr) x[i] = __ldcg(cur + i);
+    cluster_barrier();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kTailThreads, 1) amg_tail_kernel(const TailLevel<T>* __restrict__ lv, int nlev,
+                                                                   int nco, const double* __restrict__ co_inv,
+                                                                   T* co_b, T* co_x, const T* b_top, T* x_top,
+                                                                   double* rr) {
+  pdl_enter();
+  const long long nthr = (long long)gridDim.x * blockDim.x;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (int j = 0; j < nlev; ++j) {
+    const TailLevel<T> L = lv[j];
+    const T* b = j == 0 ? b_top : L.b;
+    T* x = j == 0 ? x_top : L.x;
+    tail_smooth(L, b, x, true, (const T*)nullptr, tid, nthr);
+    // restrict_rows_kernel: member residuals b_i - (A x)_i ...
+    const int LN = L.lanes;
+    const long long total = ((long long)L.n * LN + 31) / 32 * 32;
+    for (long long t = tid; t < total; t += nthr) {
+      const long long m = t / LN;
+      const int sub = (int)(t % LN);
+      int i = 0;
+      double sres = 0.0;
+      if (m < L.n) {
+        i = L.cmem[m];
+        for (int k = L.rp[i] + sub; k < L.rp[i + 1]; k += LN) sres = __fma_rn(-(double)L.val[k], ldv(x + L.ci[k]), sres);
+      }
+      sres = group_sum_rt(sres, LN);
+      if (m < L.n && sub == 0) rr[m] = __dadd_rn(ldv(b + i), sres);
+    }
+    cluster_barrier();
+    // ... summed per aggregate in member order
+    T* bc = j + 1 < nlev ? lv[j + 1].b : co_b;
+    const int nn = j + 1 < nlev ? lv[j + 1].n : nco;
+    for (long long I = tid; I < nn; I += nthr) {
+      double v = 0.0;
+      for (int m = L.cptr[I]; m < L.cptr[I + 1]; ++m) v = __dadd_rn(v, __ldcg(rr + m));
+      bc[I] = (T)v;
+    }
+    cluster_barrier();
+  }
+  // dense_apply_kernel: one warp per row of the coarsest inverse
+  {
+    const long long lane = tid & 31, nwarp = nthr >> 5;
+    for (long long row = tid >> 5; row < nco; row += nwarp) {
+      double sv = 0.0;
+      for (long long jj = lane; jj < nco; jj += 32) sv = __fma_rn(co_inv[row * nco + jj], ldv(co_b + jj), sv);
+      sv = warp_sum(sv);
+      if (lane == 0) co_x[row] = (T)sv;
+    }
+    cluster_barrier();
+  }
+  for (int j = nlev - 1; j >= 0; --j) {
+    const TailLevel<T> L = lv[j];
+    const T* b = j == 0 ? b_top : L.b;
+    T* x = j == 0 ? x_top : L.x;
+    const T* xc = j + 1 < nlev ? lv[j + 1].x : co_x;
+    tail_smooth(L, b, x, false, xc, tid, nthr);  // prolongation folded into the first step
+  }
 }
 
 // Fused coarse cycle (opt-in) ----------------------------------------------
@@ -608,12 +793,6 @@ __device__ __forceinline__ void grid_barrier(unsigned int* bar, int* status) {
   __syncthreads();
 }
 
-// Sum over a group of `lanes` consecutive lanes (a power of two <= 32), the
-// order of group_sum<LANES>.
-__device__ __forceinline__ double group_sum_rt(double v, int lanes) {
-  for (int o = lanes >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
 
 template <class T, bool ZERO>
 __device__ void fused_cheb_rows(const CoopLevel<T>& L, const T* b, const T* xin, T* xout, int step, long long tid,
@@ -912,7 +1091,107 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
   gj_layout(nco_, gj_rows_, gj_smem_);
   bits_.resize(std::max<size_t>(levels_.size(), 1));
   build_fused(s);
+  build_tail(s);
   PMB_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class T>
+void AMG<T>::build_tail(cudaStream_t s) {
+  tail_start_ = -1;
+  tail_cluster_ = 0;
+  const char* e = std::getenv("PMB_AMG_TAIL");
+  if (e && e[0] == '0') return;
+  const int L = (int)levels_.size();
+  int first = -1;
+  for (int l = std::max(0, k_levels); l < L; ++l)
+    if (levels_[l].n <= kTailMaxRows) {
+      first = l;
+      break;
+    }
+  if (first < 0) return;
+  // 16 CTAs of 1024 threads where the device schedules such a cluster
+  // (a non-portable size), else 8, else 4
+  int cs = 0;
+  for (int c : {16, 8, 4}) {
+    if (c > 8 && cudaFuncSetAttribute(amg_tail_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                     cudaSuccess) {
+      (void)cudaGetLastError();
+      continue;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(kTailThreads);
+    cudaLaunchAttribute a[1];
+    a[0].id = cudaLaunchAttributeClusterDimension;
+    a[0].val.clusterDim.x = c;
+    a[0].val.clusterDim.y = 1;
+    a[0].val.clusterDim.z = 1;
+    cfg.attrs = a;
+    cfg.numAttrs = 1;
+    int active = 0;
+    if (cudaOccupancyMaxActiveClusters(&active, amg_tail_kernel<T>, &cfg) == cudaSuccess && active > 0) {
+      cs = c;
+      break;
+    }
+    (void)cudaGetLastError();
+  }
+  if (!cs) return;
+  std::vector<TailLevel<T>> h;
+  int maxn = 1;
+  for (int l = first; l < L; ++l) {
+    AMGLevel<T>& V = levels_[l];
+    TailLevel<T> t;
+    t.n = V.n;
+    t.lanes = V.lanes;
+    t.steps = std::max(1, V.degree > 0 ? V.degree : degree);
+    t.rp = V.row_ptr;
+    t.ci = V.col;
+    t.val = V.val.get();
+    t.dinv = V.dinv.get();
+    t.lmax = V.lmax.get();
+    t.b = V.b.get();
+    t.x = V.x.get();
+    t.d = V.r.get();
+    t.t = V.t.get();
+    t.u = V.u.get();
+    t.cptr = V.cptr.get();
+    t.cmem = V.cmem.get();
+    t.agg = V.agg.get();
+    h.push_back(t);
+    maxn = std::max(maxn, V.n);
+  }
+  tail_levels_.resize(sizeof(TailLevel<T>) * h.size());
+  PMB_CUDA(cudaMemcpyAsync(tail_levels_.get(), h.data(), sizeof(TailLevel<T>) * h.size(), cudaMemcpyHostToDevice, s));
+  tail_rr_.resize(maxn);
+  tail_start_ = first;
+  tail_cluster_ = cs;
+}
+
+template <class T>
+void AMG<T>::launch_tail(const T* b, T* x, cudaStream_t s) {
+  const TailLevel<T>* lv = reinterpret_cast<const TailLevel<T>*>(tail_levels_.get());
+  const int nlev = (int)levels_.size() - tail_start_;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(tail_cluster_);
+  cfg.blockDim = dim3(kTailThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = tail_cluster_;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 2;
+  int nco = nco_;
+  const double* inv = co_inv_.get();
+  T* cob = co_b_.get();
+  T* cox = co_x_.get();
+  double* rr = tail_rr_.get();
+  PMB_CUDA(cudaLaunchKernelEx(&cfg, amg_tail_kernel<T>, lv, nlev, nco, inv, cob, cox, b, x, rr));
+  PMB_CHECK_LAUNCH();
 }
 
 template <class T>
@@ -1088,6 +1367,11 @@ static const char* level_phase(int l, int kind) {
 
 template <class T>
 void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
+  if (tail_start_ >= 0 && l == tail_start_) {
+    PhaseTimer pt("amg.tail", s);
+    launch_tail(b, x, s);
+    return;
+  }
   if (coop_start_ >= 0 && l == coop_start_) {
     launch_fused(b, x, s);
     return;

@@ -232,6 +232,49 @@ int pmb_ow_reset_cdp(pmb_ow* h) {
   });
 }
 
+int pmb_ow_prev_jacobian_tmul(pmb_ow* h, const double* d_x_prev, double dt, const double* d_lam, double* d_y) {
+  return guarded([&] {
+    PMB_REQUIRE(h && d_x_prev && d_lam && d_y, "NULL argument");
+    require_aligned(d_x_prev, 16, "x_prev");
+    h->m->prev_jacobian_tmul(d_x_prev, dt, d_lam, d_y);
+  });
+}
+
+int pmb_ow_csr_values(pmb_ow* h, const double* d_jac, const double* d_well, int64_t n, const int64_t* d_ptr,
+                      const int64_t* d_terms, double* d_vals) {
+  return guarded([&] {
+    PMB_REQUIRE(h, "NULL argument");
+    h->m->csr_values(d_jac, d_well, n, d_ptr, d_terms, d_vals);
+  });
+}
+
+int pmb_ow_perm_contract(pmb_ow* h, const double* d_x, const double* d_lam, const double* d_t0, const double* d_t1,
+                         double* d_face_flux, double* d_perf_rate, double* d_out) {
+  return guarded([&] {
+    PMB_REQUIRE(h, "NULL argument");
+    require_aligned(d_x, 16, "x");
+    require_aligned(d_face_flux, 16, "face_flux");
+    if (h->m->nw()) require_aligned(d_perf_rate, 16, "perf_rate");
+    h->m->perm_contract(d_x, d_lam, d_t0, d_t1, d_face_flux, d_perf_rate, d_out);
+  });
+}
+
+int pmb_ow_get_last_cdp(pmb_ow* h, double* d_out, int32_t* h_have) {
+  return guarded([&] {
+    PMB_REQUIRE(h && h_have, "NULL argument");
+    int have = 0;
+    h->m->get_last_cdp(d_out, &have);
+    *h_have = have;
+  });
+}
+
+int pmb_ow_set_last_cdp(pmb_ow* h, const double* d_in) {
+  return guarded([&] {
+    PMB_REQUIRE(h, "NULL argument");
+    h->m->set_last_cdp(d_in);
+  });
+}
+
 int pmb_ow_fluxes(pmb_ow* h, const double* d_x, const double* d_cdp, double* d_face_flux, double* d_perf_rate) {
   return guarded([&] {
     PMB_REQUIRE(h && d_x && d_face_flux, "NULL argument");

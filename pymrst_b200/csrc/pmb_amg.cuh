@@ -107,8 +107,20 @@ class AMG {
   double cycle_bytes() const { return num_levels() ? cycle_bytes_from(0) : 0.0; }
   double refresh_bytes() const;
   long long level_nnz(int l) const { return l < (int)levels_.size() ? levels_[l].nnz : co_nnz_; }
+  // The levels from tail_first_level() down (the first level below the
+  // K-cycle levels with at most 65,536 rows, and all coarser ones) run as one
+  // thread-block-cluster launch per visit (amg_tail_kernel), bitwise the
+  // per-step path; -1 when off (PMB_AMG_TAIL=0 in the environment at build
+  // time, or no cluster launch possible).
+  int tail_first_level() const { return tail_start_; }
+  int tail_cluster_size() const { return tail_cluster_; }
 
  private:
+  int tail_start_ = -1, tail_cluster_ = 0;
+  DArray<unsigned char> tail_levels_;
+  DArray<double> tail_rr_;
+  void build_tail(cudaStream_t s);
+  void launch_tail(const T* b, T* x, cudaStream_t s);
   double cycle_bytes_from(int l) const;
   double coarse_bytes(int l) const;
   int coop_start_ = -1, coop_grid_ = 0;

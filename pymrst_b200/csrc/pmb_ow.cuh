@@ -123,6 +123,29 @@ class OWModel {
   // x += sgn * dx with the reference update limits
   void update(double* x, const double* dx, double sgn = 1.0);
 
+  // Adjoint support (adjoint.cu).  y = (dR_{n+1}/dx_n)^T lam for the
+  // accumulation terms, the only ones that see the previous state, with
+  // x_prev the state x_n (cell-major) and dt the step n+1; lam and y in the
+  // variable-blocked layout [p, sW, qWs, qOs, bhp] (y's well entries 0).
+  void prev_jacobian_tmul(const double* x_prev, double dt, const double* lam, double* y);
+  // Values of a CSR matrix each of whose entries e is the sum, over the
+  // terms ptr[e] .. ptr[e+1]-1, of one Jacobian entry (term t >= 0: jac[t]
+  // for t < 4 nnzb, else well[t - 4 nnzb]) or one entry of a cross-flow
+  // mixture product (t < 0: code -1 - t = ((i nperf + j) 4 + 2a + b), entry
+  // (a, b) of Up_i Vp_j, counted where the well's mixture coupling is on).
+  void csr_values(const double* jac, const double* well, int64_t n, const int64_t* ptr, const int64_t* terms,
+                  double* vals);
+  // out[c] += lam^T dR/d(log k_c) at state x (cdp = 0): through the
+  // interface transmissibilities (dT_f/dlog k_c = T_f^2 / t_{c,f}, t0 / t1
+  // the half-face T of N[f,0] / N[f,1]) and the well indices of the
+  // perforations of c; face_flux (2 nf) and perf_rate (2 nperf) are scratch.
+  void perm_contract(const double* x, const double* lam, const double* t0, const double* t1, double* face_flux,
+                     double* perf_rate, double* out);
+  // The previous timestep's well pressure drops, kept for the next
+  // compute_cdp (nperf values; *have = 0 when there are none).
+  void get_last_cdp(double* out, int* have);
+  void set_last_cdp(const double* in);
+
   // internal buffers
   double* jac() { return jac_.get(); }
   double* well() { return well_.get(); }
@@ -143,7 +166,7 @@ class OWModel {
   DArray<double> T_, gdz_, pv_, perf_WI_, perf_dZ_, well_val_, compi_;
   std::vector<int> h_well_type_;
   // scratch / state
-  DArray<double> pf_cq_, pf_dloc_, last_cdp_, conv_part_, conv_out_;
+  DArray<double> pf_cq_, pf_dloc_, last_cdp_, conv_part_, conv_out_, cdp_zero_;
   DArray<double> jac_, well_, res_, cdp_, x0_, dx_;
   bool have_last_cdp_ = false;
   double pv_tot_ = 0.0;

@@ -42,6 +42,18 @@ class OWState:
                          (self.pressure, self.sW, self.qWs, self.qOs, self.bhp)))
 
 
+class Equation:
+    """One equation block: values and the Jacobian blocks with respect to
+    each primary variable (the fields of the reference's ADI)."""
+
+    def __init__(self, val, jac):
+        self.val = np.asarray(val, float)
+        self.jac = list(jac)
+
+    def __len__(self):
+        return self.val.size
+
+
 def _torch():
     import torch
     if not torch.cuda.is_available():
@@ -349,6 +361,10 @@ class GpuOilWaterModel:
         if self.nw:
             N.check(N.lib().pmb_ow_set_controls(self._handle, N.as_p(u, N.C.c_double)))
 
+    def reset_cdp(self) -> None:
+        """Forget the previous timestep's well pressure drops (a fresh run)."""
+        N.check(N.lib().pmb_ow_reset_cdp(self._handle))
+
     # -- assembly export (parity / protocol) ---------------------------------
     def compute_cdp(self, st0: OWState):
         torch = _torch()
@@ -448,6 +464,88 @@ class GpuOilWaterModel:
         out = (N.C.c_double * 8)()
         N.check(N.lib().pmb_ow_convergence(self._handle, N.ptr(res_dev), N.ptr(x_dev), float(dt), out))
         return list(out)
+
+    # -- the legacy nonlinear-solver protocol ------------------------------
+    # What the reference's NonLinearSolver.solve_ministep calls
+    # (ad_core/simulators/nonlinear_solver.py:239-381) on a model, with the
+    # meaning GenericBlackOilModelAD gives them (generic_black_oil_model.py:
+    # 472-684): get_equations -> the equation list, get_convergence -> (ok,
+    # residual report), update_state -> the limited Newton update.  The
+    # residual, Jacobian, convergence values and update are computed on the
+    # device; the equation list is a host copy, because the solver combines
+    # it on the host (combine_equations) before its linear solve.
+
+    def _protocol_start(self, state0, dt):
+        """Device start state and well pressure drops of the timestep that
+        `state0` and `dt` open (computed once per timestep, as `step` does)."""
+        torch = _torch()
+        p0 = np.asarray(state0.pressure, float)
+        key = (id(state0), float(dt), p0[:8].tobytes(), np.asarray(state0.sW, float)[:8].tobytes())
+        if getattr(self, "_proto_key", None) != key:
+            self._proto_x0 = self.to_device(state0)
+            self._proto_cdp = torch.zeros(max(self.sizes["nperf"], 1), dtype=torch.float64, device="cuda")
+            N.check(N.lib().pmb_ow_compute_cdp(self._handle, N.ptr(self._proto_x0), N.ptr(self._proto_cdp)))
+            self._proto_key = key
+        return self._proto_x0, self._proto_cdp
+
+    def get_equations(self, state0: OWState, state: OWState, dt: float):
+        """[water, oil, eq_w, eq_o, ctrl] at `state` for the step from
+        `state0` over `dt`, each with its values and its Jacobian blocks with
+        respect to [p, sW, qWs, qOs, bhp], as `assemble` returns them
+        (two_phase_oil_water_model.py:493-546).  The objects are the
+        reference's ADI type where that package is importable (so that its
+        combine_equations accepts them), else `Equation`."""
+        x0, cdp = self._protocol_start(state0, dt)
+        x = self.to_device(state)
+        res, jac, well = self.assemble_device(x, x0, dt, cdp, True)
+        self._proto_eval = (x, res, float(dt))
+        r = self.export_residual(res.cpu().numpy())
+        J = self.export_jacobian(jac.cpu().numpy(), well.cpu().numpy()).tocsr()
+        nc, nw = self.nc, self.nw
+        cuts = [0, nc, 2 * nc, 2 * nc + nw, 2 * nc + 2 * nw, 2 * nc + 3 * nw]
+        try:
+            from pymrst.utils.adi import ADI as make
+        except ImportError:
+            make = Equation
+        eqs = []
+        for i in range(5):
+            rows = J[cuts[i]:cuts[i + 1]]
+            eqs.append(make(r[cuts[i]:cuts[i + 1]].copy(),
+                            [sp.csr_matrix(rows[:, cuts[j]:cuts[j + 1]]) for j in range(5)]))
+        return eqs
+
+    def get_convergence(self, eqs, dt: float):
+        """(converged, {"CNV", "MB", "well", "control"}) of the equations of
+        the last get_equations: the device CNV / MB / well test of `step`
+        (_converged, two_phase_oil_water_model.py:549-567); "control" is the
+        largest control residual scaled by 1 bar (bhp) or the reference rate."""
+        if getattr(self, "_proto_eval", None) is None:
+            raise RuntimeError("get_convergence needs the equations of a preceding get_equations")
+        x, res, _ = self._proto_eval
+        out = self.convergence(res, x, dt)
+        ctrl = np.abs(np.asarray(getattr(eqs[4], "val", eqs[4]), float))
+        rates = [abs(float(np.ravel(w.val)[0])) for w in self.wells if str(w.type).lower() == "rate"]
+        q_ref = max(max(rates), 1e-12) if rates else 1.0
+        scale = np.array([1e5 if str(w.type).lower() == "bhp" else q_ref for w in self.wells])
+        control = float(np.max(ctrl / scale)) if self.nw else 0.0
+        return bool(out[5]), {"CNV": float(out[0]), "MB": float(out[1]), "well": float(max(out[2], out[3])),
+                              "control": control}
+
+    def update_state(self, state: OWState, increment) -> OWState:
+        """The Newton update of `step` (two_phase_oil_water_model.py:641-651)
+        on the device: dp limited to dp_max_rel |p|, dsW to ds_max, sW kept in
+        [0, 1]; `increment` in the variable-blocked layout [p, sW, qWs, qOs,
+        bhp]."""
+        torch = _torch()
+        dx = np.asarray(increment, float).ravel()
+        nc, nw = self.nc, self.nw
+        if dx.size != 2 * nc + 3 * nw:
+            raise ValueError(f"increment of length {dx.size}, expected {2 * nc + 3 * nw}")
+        d = self.pack(OWState(pressure=dx[:nc], sW=dx[nc:2 * nc], qWs=dx[2 * nc:2 * nc + nw],
+                              qOs=dx[2 * nc + nw:2 * nc + 2 * nw], bhp=dx[2 * nc + 2 * nw:]))
+        x = self.to_device(state)
+        N.check(N.lib().pmb_ow_update(self._handle, N.ptr(x), N.ptr(torch.as_tensor(d, device="cuda")), 1.0))
+        return self.from_device(x)
 
     def cpr_levels(self):
         sizes = (N.C.c_int64 * 64)()

@@ -1,0 +1,106 @@
+"""The reference's own drivers and models with this package's GPU pieces
+plugged in, through the reference's public objects, against the reference's
+own Newton histories (ow_newton_grav.npz: 8 x 6 x 4 cells with gravity, four
+10-day steps, made by the reference's TwoPhaseOilWaterModelAD and
+simulate_schedule_ad with its direct solver):
+
+* the reference's TwoPhaseOilWaterModelAD with `linear_solver=GpuCPRSolver()`,
+  driven by the reference's simulate_schedule_ad;
+* GpuOilWaterModel, built from the reference's grid, rock, fluid and wells,
+  driven by the reference's simulate_schedule_ad (its `step`);
+* GpuOilWaterModel driven by the reference's legacy NonLinearSolver through
+  get_equations / get_convergence / update_state, with the solver's own
+  direct solve and with GpuCPRSolver.
+
+The reference package comes from its install under baseline/_ref; the module
+is skipped where that install is absent."""
+
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from fixtures import load
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+REF = Path(__file__).resolve().parents[1] / "baseline" / "_ref"
+if not (REF / "pymrst").is_dir():
+    pytest.skip("the reference package is not installed under baseline/_ref", allow_module_level=True)
+sys.path.insert(0, str(REF))
+
+from pymrst.gridprocessing import cart_grid, compute_geometry  # noqa: E402
+from pymrst.modules.ad_blackoil import TwoPhaseOilWaterModelAD  # noqa: E402
+from pymrst.modules.ad_core import simulate_schedule_ad  # noqa: E402
+from pymrst.modules.ad_core.simulators.nonlinear_solver import NonLinearSolver  # noqa: E402
+from pymrst.modules.ad_props import init_simple_adi_fluid  # noqa: E402
+from pymrst.params import add_well, make_rock  # noqa: E402
+from pymrst.utils.units import BARSA, CENTI, DAY, POISE  # noqa: E402
+
+from pymrst_b200.build import build  # noqa: E402
+from pymrst_b200.linear_solvers import GpuCPRSolver  # noqa: E402
+from pymrst_b200.ow_model import GpuOilWaterModel  # noqa: E402
+
+build()
+
+
+def _reference_case():
+    """The fixture's model, built from the reference's own constructors (as
+    tests/golden/make_golden.py's newton_fixture builds it)."""
+    d = load("ow_newton_grav.npz")
+    dims = [int(v) for v in d["dims"]]
+    g = compute_geometry(cart_grid(dims, [float(v) for v in d["phys"]]))
+    rock = make_rock(g, d["perm"][:, None], 0.2)
+    fluid = init_simple_adi_fluid(mu=np.array([1.0, 5.0]) * CENTI * POISE, rho=[1000.0, 800.0], n=[2, 2],
+                                  c=[1e-5 / BARSA, 1e-5 / BARSA], p_ref=200 * BARSA, smin=[0.1, 0.1])
+    nx, ny, nz = dims
+    col = lambda i, j: i + nx * (j + ny * np.arange(nz))
+    grav = float(d["gravity"])
+    gvec = np.array([0, 0, grav])
+    nsteps, dt_days = int(d["nsteps"]), float(d["dt_days"])
+    rate = 0.25 * float(np.sum(0.2 * g.cells.volumes)) / (nsteps * dt_days * DAY) / 2
+    w = add_well(None, g, rock, col(0, 0), well_type="rate", val=rate, compi=np.array([1.0, 0.0]), sign=1,
+                 gravity=gvec)
+    w = add_well(w, g, rock, col(nx - 1, 0), well_type="rate", val=rate, compi=np.array([1.0, 0.0]), sign=1,
+                 gravity=gvec)
+    w = add_well(w, g, rock, col(nx // 2, ny - 1), well_type="bhp", val=150 * BARSA, compi=np.array([0.0, 1.0]),
+                 sign=-1, gravity=gvec)
+    return d, g, rock, fluid, w, grav, np.full(nsteps, dt_days * DAY)
+
+
+def _check_history(d, states, its):
+    assert list(np.asarray(its)) == list(d["its"])
+    for k, st in enumerate(states):
+        p, sw = np.asarray(st.pressure), np.asarray(st.sW)
+        assert np.abs(p - d["p_hist"][k]).max() <= 1e-8 * np.abs(d["p_hist"][k]).max()
+        assert np.abs(sw - d["sw_hist"][k]).max() <= 1e-7
+
+
+def test_reference_model_with_the_gpu_linear_solver():
+    d, g, rock, fluid, w, grav, dts = _reference_case()
+    model = TwoPhaseOilWaterModelAD(g, rock, fluid, w, gravity=grav, linear_solver=GpuCPRSolver(rtol=1e-12))
+    states, its = simulate_schedule_ad(model.initial_state(200 * BARSA, 0.1), model, dts, verbose=False)
+    _check_history(d, states, its)
+
+
+def test_reference_driver_runs_the_gpu_model():
+    d, g, rock, fluid, w, grav, dts = _reference_case()
+    model = GpuOilWaterModel(g, rock, fluid, w, gravity=grav, cpr_options=dict(rtol=1e-12, maxiter=400))
+    states, its = simulate_schedule_ad(model.initial_state(200 * BARSA, 0.1), model, dts, verbose=False)
+    _check_history(d, states, its)
+
+
+@pytest.mark.parametrize("solver", ["direct", "gpu_cpr"])
+def test_reference_nonlinear_solver_drives_the_gpu_model(solver):
+    d, g, rock, fluid, w, grav, dts = _reference_case()
+    model = GpuOilWaterModel(g, rock, fluid, w, gravity=grav)
+    nls = NonLinearSolver(max_iterations=25, verbose=False,
+                          linear_solver=None if solver == "direct" else GpuCPRSolver(rtol=1e-12))
+    states, report = nls.simulate_schedule(model, model.initial_state(200 * BARSA, 0.1), dts)
+    assert all(r.converged for r in report.steps)
+    _check_history(d, states, [r.iterations for r in report.steps])
