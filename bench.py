@@ -374,6 +374,62 @@ def measure_ow_fp64(torch, N, GpuOilWaterModel, run_report_step, cpu_budget=20.0
             "speedup": gpu_v / cpu_v}
 
 
+def measure_adjoint(torch, GpuOilWaterModel, cpu_steps=3):
+    """Config 4: the adjoint gradient of cumulative produced oil on the
+    64x64x4 (16,384-cell) five-spot over 30 steps of 10 days, with respect
+    to every well control of every step and every cell's log-permeability.
+    GPU: one forward simulation alone, then the whole gradient (forward with
+    checkpoints, recomputed segments, transposed solves), both CUDA-event
+    timed after a 3-step warm-up; CPU: the oracle's forward and adjoint
+    (SuperLU, the reference's algorithm) on the first `cpu_steps` steps."""
+    from oracle import adjoint as oadj
+    from oracle import ow as oow
+    from pymrst_b200 import cases
+    from pymrst_b200.adjoint import compute_gradient_adjoint, npv_objective
+    c = cases.five_spot(dims=(64, 64, 4), seed=4, nsteps=30)
+    m = GpuOilWaterModel(c.grid, c.rock, c.fluid, c.wells, gravity=c.gravity,
+                         cpr_options=dict(amg_rebuild_interval=1_000_000))
+    st0 = m.initial_state(c.p0, c.sw0)
+    dts = np.full(c.nsteps, c.dt)
+    u = np.tile([float(np.ravel(w.val)[0]) for w in c.wells], (c.nsteps, 1))
+    obj = npv_objective(oil_price=1.0, water_cost=0.0, water_inj_cost=0.0)
+    compute_gradient_adjoint(m, st0, dts[:3], u[:3], obj, perm_gradient=True)
+    m.reset_cdp()
+    x = m.to_device(st0)
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    e0.record()
+    its = 0
+    for n in range(c.nsteps):
+        m.set_controls(u[n])
+        ok, nit, _ = m.step_device(x, c.dt)
+        its += nit
+        if not ok:
+            raise RuntimeError("forward step failed")
+    e1.record()
+    torch.cuda.synchronize()
+    t_fwd = e0.elapsed_time(e1) * 1e-3
+    m.reset_cdp()
+    e0.record()
+    res = compute_gradient_adjoint(m, st0, dts, u, obj, perm_gradient=True)
+    e1.record()
+    torch.cuda.synchronize()
+    t_adj = e0.elapsed_time(e1) * 1e-3
+    prob = oow.build_problem(c.grid, c.rock, c.fluid.params, c.wells, gravity=c.gravity)
+    t0 = time.perf_counter()
+    oadj.compute_gradient_adjoint(prob, oow.initial_state(prob, c.p0, c.sw0), dts[:cpu_steps], u[:cpu_steps])
+    t_cpu = time.perf_counter() - t0
+    return {"workload": "adjoint gradient, oil-water five-spot 64x64x4 (16,384 cells), 30 x 10 days, "
+                        "d(cumulative oil)/d(controls, log k)",
+            "gpu_forward_s": t_fwd, "gpu_gradient_s": t_adj, "gradient_over_forward": t_adj / t_fwd,
+            "forward_newton_iterations": its, "checkpoint_every": res.stats["checkpoint_every"],
+            "recomputed_steps": res.stats["recomputed_steps"],
+            "transposed_krylov_iterations": res.stats["krylov_iterations"],
+            "cpu_s_per_step": t_cpu / cpu_steps, "gpu_s_per_step": t_adj / c.nsteps,
+            "speedup_per_step": (t_cpu / cpu_steps) / (t_adj / c.nsteps),
+            "cpu": f"oracle forward + adjoint (numpy, SuperLU) over the first {cpu_steps} steps, one core"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -570,7 +626,8 @@ def run_ours(args):
     if not args.no_configs and rank == 0 and world == 1:
         for name, fn in (("incomp_64x64x8", lambda: measure_incomp(torch)),
                          ("ow_fp64_100x100x10", lambda: measure_ow_fp64(torch, N, GpuOilWaterModel, run_report_step,
-                                                                        args.cpu_budget))):
+                                                                        args.cpu_budget)),
+                         ("adjoint_64x64x4", lambda: measure_adjoint(torch, GpuOilWaterModel))):
             try:
                 configs[name] = fn()
             except Exception as e:  # a secondary measurement must not hide the headline line

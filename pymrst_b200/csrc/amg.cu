@@ -1099,12 +1099,22 @@ template <class T>
 void AMG<T>::build_tail(cudaStream_t s) {
   tail_start_ = -1;
   tail_cluster_ = 0;
-  const char* e = std::getenv("PMB_AMG_TAIL");
-  if (e && e[0] == '0') return;
+  // Off by default: measured on the channelised model (1.12M cells, mixed
+  // precision) with every level below the K-cycle levels in the tail
+  // (29,438 rows and down), one AMG cycle took 2.90 ms against 1.43 ms for
+  // the per-step kernels: 16 SMs move the level of 29k rows far slower than
+  // the whole GPU does.  PMB_AMG_TAIL_ROWS=<n> turns it on for the levels of
+  // at most n rows (n <= 65,536), PMB_AMG_TAIL_CLUSTER=<c> picks the cluster
+  // size (16, 8 or 4).
+  const char* e = std::getenv("PMB_AMG_TAIL_ROWS");
+  const int max_rows = e ? std::min(std::atoi(e), kTailMaxRows) : 0;
+  if (max_rows <= 0) return;
+  const char* ec = std::getenv("PMB_AMG_TAIL_CLUSTER");
+  const int want_cluster = ec ? std::atoi(ec) : 16;
   const int L = (int)levels_.size();
   int first = -1;
   for (int l = std::max(0, k_levels); l < L; ++l)
-    if (levels_[l].n <= kTailMaxRows) {
+    if (levels_[l].n <= max_rows) {
       first = l;
       break;
     }
@@ -1113,6 +1123,7 @@ void AMG<T>::build_tail(cudaStream_t s) {
   // (a non-portable size), else 8, else 4
   int cs = 0;
   for (int c : {16, 8, 4}) {
+    if (c > want_cluster) continue;
     if (c > 8 && cudaFuncSetAttribute(amg_tail_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
                      cudaSuccess) {
       (void)cudaGetLastError();

@@ -108,10 +108,10 @@ class AMG {
   double refresh_bytes() const;
   long long level_nnz(int l) const { return l < (int)levels_.size() ? levels_[l].nnz : co_nnz_; }
   // The levels from tail_first_level() down (the first level below the
-  // K-cycle levels with at most 65,536 rows, and all coarser ones) run as one
-  // thread-block-cluster launch per visit (amg_tail_kernel), bitwise the
-  // per-step path; -1 when off (PMB_AMG_TAIL=0 in the environment at build
-  // time, or no cluster launch possible).
+  // K-cycle levels with at most PMB_AMG_TAIL_ROWS rows, and all coarser
+  // ones) run as one thread-block-cluster launch per visit
+  // (amg_tail_kernel), bitwise the per-step path; -1 when off (the default,
+  // or no cluster launch possible).
   int tail_first_level() const { return tail_start_; }
   int tail_cluster_size() const { return tail_cluster_; }
 

@@ -250,5 +250,99 @@ class GpuCPRSolver:
         model contract as `solve` does."""
         return self.solve(A, b, model, state)
 
+    # -- the AD-OO linear-solver protocol (linear_solver_ad.py:779-1060) ------
+    def setup_solver(self, A=None, b=None, **kwargs):
+        """Hook before a solve; the device handles are made on first use."""
+        return self
+
+    def cleanup_solver(self, A=None, b=None, **kwargs):
+        return self
+
+    setupSolver, cleanupSolver = setup_solver, cleanup_solver
+
+    def get_solve_report(self, **kwargs) -> dict:
+        report = {"Iterations": int(self.last_iterations), "Residual": float(self.last_relres),
+                  "SolverTime": 0.0, "LinearSolutionTime": 0.0, "PreparationTime": 0.0, "PostProcessTime": 0.0,
+                  "Converged": True}
+        report.update(kwargs)
+        return report
+
+    getSolveReport = get_solve_report
+
+    @staticmethod
+    def _assembled_system(problem):
+        """(A, rhs) of a linearized problem: the problem assembles itself
+        (its assemble_system); a LinearizedProblemAD stores the residual, so
+        its right-hand side is the negated b (linear_solver_ad.py:37-52)."""
+        out = problem.assemble_system()
+        problem = problem if out is None else out
+        b = np.asarray(problem.b, dtype=float).ravel()
+        stores_residual = any(c.__name__ == "LinearizedProblemAD" for c in type(problem).__mro__)
+        return problem, problem.A, (-b if stores_residual else b)
+
+    @staticmethod
+    def store_increments(problem, result) -> list:
+        """The solution split into one block per primary variable: by the
+        first equation's Jacobian block widths, or the problem's declared
+        sizes (storeIncrements)."""
+        result = np.asarray(result, dtype=float).ravel()
+        sample = next((eq for eq in getattr(problem, "equations", []) if hasattr(eq, "jac")), None)
+        num_vars = getattr(problem, "num_vars", None)
+        if sample is not None:
+            widths = [blk.shape[1] for blk in sample.jac]
+            if num_vars is not None and sum(num_vars) == sum(widths):
+                widths = list(num_vars)
+        elif getattr(problem, "var_sizes", None):
+            widths = list(problem.var_sizes)
+        else:
+            return [result] if result.size else []
+        cuts = np.concatenate([[0], np.cumsum(widths)])
+        return [result[cuts[i]:cuts[i + 1]] for i in range(len(widths))]
+
+    def solve_linear_problem(self, problem, model=None):
+        """`(dx, result, report)` for a linearized problem
+        (LinearSolverAD.solve_linear_problem, linear_solver_ad.py:832-895):
+        the problem's assembled system solved by the device CPR, the solution
+        split per primary variable.  The reference's optional reordering,
+        Schur reduction and diagonal scaling are not applied: the device CPR
+        solves the full system."""
+        import time
+        t0 = time.perf_counter()
+        problem, A, b = self._assembled_system(problem)
+        if not np.all(np.isfinite(b)):
+            raise ValueError("the linear system's right-hand side has non-finite entries")
+        t1 = time.perf_counter()
+        result = self.solve(A, b, model, getattr(problem, "state", None) or {})
+        t2 = time.perf_counter()
+        dx = self.store_increments(problem, result)
+        report = self.get_solve_report(SolverTime=time.perf_counter() - t0, LinearSolutionTime=t2 - t1,
+                                       PreparationTime=t1 - t0, PostProcessTime=time.perf_counter() - t2)
+        return dx, result, report
+
+    solveLinearProblem = solve_linear_problem
+
+    def solve_adjoint_problem(self, problem_prev, problem_curr, next_lambda_vec, objective, model=None, **kwargs):
+        """One backward step of an adjoint recursion
+        (LinearSolverAD.solve_adjoint_problem, linear_solver_ad.py:1018-1060):
+        (dF_i/dx_i)^T lambda_i = -(dg_i/dx_i)^T - (dF_{i+1}/dx_i)^T lambda_{i+1},
+        the transposed system solved by the device CPR with transposed
+        transfer operators."""
+        problem_curr, A, _ = self._assembled_system(problem_curr)
+        if objective is None:
+            rhs = np.zeros(A.shape[0])
+        else:
+            g = objective.jac if hasattr(objective, "jac") else objective
+            if isinstance(g, (list, tuple)):
+                g = sp.hstack([sp.csr_array(blk) for blk in g]).toarray()
+            rhs = -np.asarray(g, dtype=float).ravel()
+        if next_lambda_vec is not None and problem_prev is not None:
+            if getattr(problem_prev, "A", None) is None:
+                problem_prev, _, _ = self._assembled_system(problem_prev)
+            rhs = rhs - sp.csr_array(problem_prev.A).T @ np.asarray(next_lambda_vec, dtype=float).ravel()
+        lam = self.solve_transposed(A, rhs, model, getattr(problem_curr, "state", None) or {})
+        return self.store_increments(problem_curr, lam), lam, self.get_solve_report(Adjoint=True, **kwargs)
+
+    solveAdjointProblem = solve_adjoint_problem
+
 
 CPRSolver = GpuCPRSolver

@@ -1,6 +1,6 @@
 """The cluster tail cycle (the AMG levels below the K-cycle levels as one
 thread-block-cluster launch per visit) against the per-step kernels
-(PMB_AMG_TAIL=0): the same Newton step, run in two processes, gives bitwise
+(the default): the same Newton step, run in two processes, gives bitwise
 the same states and the same Newton and Krylov iteration counts, in FP64 and
 in mixed precision, with fewer kernel launches."""
 
@@ -46,7 +46,7 @@ print(json.dumps({"its": int(its), "krylov": float(m.last_stats[2]), "launches":
 def _run(tmp_path, tail, precision, cycle):
     env = dict(os.environ)
     env.pop("PMB_FUSED_COARSE", None)
-    env["PMB_AMG_TAIL"] = "1" if tail else "0"
+    env["PMB_AMG_TAIL_ROWS"] = "65536" if tail else "0"
     out = tmp_path / f"state_{int(tail)}_{precision}_{cycle}.npy"
     r = subprocess.run([sys.executable, "-c", SNIPPET, str(ROOT), str(out), str(precision), str(cycle)], env=env,
                        capture_output=True, text=True, timeout=600)

@@ -42,7 +42,7 @@ print(json.dumps({"ok": bool(ok), "its": int(its), "krylov": float(m.last_stats[
 def _run(tmp_path, fused):
     env = dict(os.environ)
     env.pop("PMB_FUSED_COARSE", None)
-    env["PMB_AMG_TAIL"] = "0"  # the cluster tail cycle would take these levels first
+    env["PMB_AMG_TAIL_ROWS"] = "0"  # the cluster tail cycle would take these levels first
     if fused:
         env["PMB_FUSED_COARSE"] = "1"
     out = tmp_path / f"state_{int(fused)}.npy"

@@ -40,6 +40,7 @@ from pymrst.modules.ad_core import simulate_schedule_ad  # noqa: E402
 from pymrst.modules.ad_core.simulators.nonlinear_solver import NonLinearSolver  # noqa: E402
 from pymrst.modules.ad_props import init_simple_adi_fluid  # noqa: E402
 from pymrst.params import add_well, make_rock  # noqa: E402
+from pymrst.utils.adi import combine_equations  # noqa: E402
 from pymrst.utils.units import BARSA, CENTI, DAY, POISE  # noqa: E402
 
 from pymrst_b200.build import build  # noqa: E402
@@ -104,3 +105,34 @@ def test_reference_nonlinear_solver_drives_the_gpu_model(solver):
     states, report = nls.simulate_schedule(model, model.initial_state(200 * BARSA, 0.1), dts)
     assert all(r.converged for r in report.steps)
     _check_history(d, states, [r.iterations for r in report.steps])
+
+
+@pytest.mark.parametrize("kind", ["LinearizedProblem", "LinearizedProblemAD"])
+def test_reference_linearized_problem_solved_by_the_gpu_solver(kind):
+    """solve_linear_problem on the reference's own problem objects built from
+    the GPU model's equations (MRST's LinearizedProblem, whose b is the
+    right-hand side, and LinearizedProblemAD, which stores the residual):
+    the increments per primary variable equal a direct solve."""
+    import scipy.sparse.linalg as spla
+    from pymrst.modules.ad_core.solvers.linear_solver_ad import LinearizedProblemAD
+    from pymrst.modules.ad_core.solvers.linearized_problem import LinearizedProblem
+    d, g, rock, fluid, w, grav, dts = _reference_case()
+    model = GpuOilWaterModel(g, rock, fluid, w, gravity=grav)
+    st0 = model.initial_state(200 * BARSA, 0.1)
+    st = st0.copy()
+    st.pressure = st.pressure + np.linspace(0.0, 5.0 * BARSA, st.pressure.size)
+    eqs = model.get_equations(st0, st, float(dts[0]))
+    names = ["water", "oil", "waterWells", "oilWells", "closure"]
+    types = ["cell", "cell", "well", "well", "well"]
+    pvars = ["pressure", "sW", "qWs", "qOs", "bhp"]
+    state = {"pressure": st.pressure}
+    if kind == "LinearizedProblem":
+        problem = LinearizedProblem(eqs, types, names, pvars, state, float(dts[0]))
+    else:
+        problem = LinearizedProblemAD.from_equations(eqs, types, names, pvars, state, float(dts[0]))
+    dx, result, report = GpuCPRSolver(rtol=1e-12).solve_linear_problem(problem, model)
+    A = combine_equations(*eqs)
+    ref = spla.spsolve(A.jac[0].tocsc(), -A.val)
+    assert np.abs(result - ref).max() <= 1e-7 * np.abs(ref).max()
+    assert [x.size for x in dx] == [model.nc, model.nc, model.nw, model.nw, model.nw]
+    assert report["Iterations"] > 0

@@ -91,3 +91,38 @@ def test_csr_create_rejects_bad_patterns(lib):
     assert rc == 2 and "nph * nc" in msg
     rc, msg = _create(lib, 4, 1, 4, [0, 1, 2, 3, 4], [0, 1, 2, 3])
     assert rc == 2 and "nph must be" in msg
+
+
+def test_linearized_problem_assembly_sign_and_increment_split():
+    """The AD-OO protocol's host logic: a LinearizedProblemAD stores the
+    residual (its right-hand side is -b), MRST's LinearizedProblem the
+    right-hand side itself; the solution splits by the first equation's
+    Jacobian block widths."""
+    from types import SimpleNamespace
+
+    import scipy.sparse as sp
+    from pymrst_b200.linear_solvers import GpuCPRSolver
+
+    class LinearizedProblem:
+        def __init__(self, eqs):
+            self.equations = eqs
+            self.A = None
+            self.b = None
+            self.num_vars = None
+
+        def assemble_system(self):
+            self.A = sp.bmat([[sp.csr_array(j) for j in e.jac] for e in self.equations], format="csr")
+            self.b = np.concatenate([e.val for e in self.equations])
+            return self
+
+    class LinearizedProblemAD(LinearizedProblem):
+        pass
+
+    eqs = [SimpleNamespace(val=np.array([1.0, 2.0]), jac=[np.eye(2), np.zeros((2, 1))]),
+           SimpleNamespace(val=np.array([3.0]), jac=[np.zeros((1, 2)), np.ones((1, 1))])]
+    _, A, b = GpuCPRSolver._assembled_system(LinearizedProblem(eqs))
+    assert A.shape == (3, 3) and np.array_equal(b, [1.0, 2.0, 3.0])
+    _, _, b = GpuCPRSolver._assembled_system(LinearizedProblemAD(eqs))
+    assert np.array_equal(b, [-1.0, -2.0, -3.0])
+    parts = GpuCPRSolver.store_increments(LinearizedProblem(eqs), np.arange(3.0))
+    assert [p.tolist() for p in parts] == [[0.0, 1.0], [2.0]]
