@@ -301,20 +301,39 @@ def fluid_params(fluid) -> FluidParams:
 
 @dataclass
 class BoundaryCondition:
-    """Boundary conditions on faces (reference params/wells_and_bc/types.py)."""
+    """Boundary conditions on faces (reference params/wells_and_bc/types.py);
+    `sat` the saturations of what flows in (transport)."""
     face: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int64))
     type: List[str] = field(default_factory=list)
     value: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    sat: np.ndarray = field(default_factory=lambda: np.zeros((0, 0)))
 
 
 @dataclass
 class Source:
-    """Volumetric cell sources, injection positive."""
+    """Volumetric cell sources, injection positive; `sat` the saturations of
+    what is injected (transport)."""
     cell: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int64))
     rate: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    sat: np.ndarray = field(default_factory=lambda: np.zeros((0, 0)))
 
 
-def add_bc(bc, faces, bctype, values) -> BoundaryCondition:
+def _sat_rows(sat, n):
+    if sat is None:
+        return np.zeros((n, 0))
+    a = np.atleast_2d(np.asarray(sat, float))
+    return np.ascontiguousarray(np.broadcast_to(a, (n, a.shape[1])))
+
+
+def _append_rows(old, new):
+    if old.size == 0:
+        return new
+    if new.shape[1] != old.shape[1]:
+        raise ValueError("saturation columns do not match the existing ones")
+    return np.vstack([old, new])
+
+
+def add_bc(bc, faces, bctype, values, sat=None) -> BoundaryCondition:
     """Append boundary conditions of one type (reference add_bc.py:13-41)."""
     faces = np.asarray(faces, dtype=np.int64).ravel()
     if faces.size == 0:
@@ -326,13 +345,17 @@ def add_bc(bc, faces, bctype, values) -> BoundaryCondition:
     bc.face = np.concatenate([bc.face, faces])
     bc.type = list(bc.type) + [str(bctype).lower()] * faces.size
     bc.value = np.concatenate([bc.value, vals])
+    bc.sat = _append_rows(bc.sat, _sat_rows(sat, faces.size))
     return bc
 
 
-def add_source(src, cells, rates) -> Source:
+def add_source(src, cells, rates, sat=None) -> Source:
     """Append cell sources (reference add_source)."""
     cells = np.asarray(cells, dtype=np.int64).ravel()
     src = Source() if src is None else src
+    if np.isin(cells, src.cell).any():
+        raise ValueError("new source terms conflict with existing source terms")
     src.cell = np.concatenate([src.cell, cells])
     src.rate = np.concatenate([src.rate, np.broadcast_to(np.asarray(rates, float), cells.shape)])
+    src.sat = _append_rows(src.sat, _sat_rows(sat, cells.size))
     return src

@@ -326,9 +326,9 @@ def _cell_size(case):
     return np.array([2 * c[0, 0], 2 * c[0, 1], 2 * c[0, 2]]) if np.prod(dims) else np.ones(3)
 
 
-def cfg1_fixture(nsteps=2):
+def cfg1_fixture(nsteps=1):
     """Benchmark config 1: the oil-water five-spot on 100x100x10 cells with
-    gravity, the first `nsteps` 10-day steps of the reference's own
+    gravity, the first `nsteps` 10-day step(s) of the reference's own
     simulate_schedule_ad with its default (direct) linear solver."""
     import time
     from pymrst_b200 import cases

@@ -136,3 +136,40 @@ def test_reference_linearized_problem_solved_by_the_gpu_solver(kind):
     assert np.abs(result - ref).max() <= 1e-7 * np.abs(ref).max()
     assert [x.size for x in dx] == [model.nc, model.nc, model.nw, model.nw, model.nw]
     assert report["Iterations"] > 0
+
+
+def test_reference_adoo_simulation_with_the_gpu_cpr_solver_ad():
+    """The reference's AD-OO oil-water model (its own equations through its
+    FacilityModel) and AD-OO simulate_schedule_ad, with GpuCPRSolverAD as the
+    linear solver: the same Newton iterations per step and the same states
+    (p 1e-8, sW 1e-7) as with the reference's direct solver."""
+    from pymrst.modules.ad_blackoil.models.two_phase_oil_water_model import TwoPhaseOilWaterModel
+    from pymrst.modules.ad_core.ad_oo.simulate_schedule_ad import simulate_schedule_ad as sim_adoo
+    from pymrst.modules.ad_core.solvers.concrete_solvers import BackslashSolverAD
+    from pymrst.modules.ad_core.utils.schedule import simple_schedule
+    from pymrst.params.wells_and_bc.vertical_well import vertical_well
+    from pymrst.solvers.init_res_sol import init_res_sol
+    from pymrst.utils.units import DARCY, MILLI
+    from pymrst_b200.linear_solvers import GpuCPRSolverAD
+    G = compute_geometry(cart_grid([10, 8, 3], [100.0, 80.0, 6.0]))
+    rng = np.random.default_rng(0)
+    rock = make_rock(G, np.exp(rng.normal(np.log(100), 0.5, G.cells.num))[:, None] * MILLI * DARCY, 0.2)
+    fluid = init_simple_adi_fluid(mu=np.array([1, 5]) * CENTI * POISE, rho=np.array([1000.0, 800.0]), n=[2, 2],
+                                  c=[1e-5 / BARSA, 1e-5 / BARSA], p_ref=200 * BARSA, phases="wo")
+    rate = 0.2 * float(np.sum(0.2 * G.cells.volumes)) / (100 * DAY)
+    W = vertical_well([], G, rock, 0, 0, None, val=rate, well_type="rate", compi=np.array([1.0, 0.0]), name="I")
+    W = vertical_well(W, G, rock, 9, 7, None, val=150 * BARSA, well_type="bhp", compi=np.array([0.0, 1.0]),
+                      name="P")
+    schedule = simple_schedule(np.full(3, 10 * DAY), W=W)
+    runs = {}
+    for name, ls in (("direct", BackslashSolverAD()), ("gpu", GpuCPRSolverAD(tolerance=1e-12))):
+        model = TwoPhaseOilWaterModel(G, rock, fluid)
+        _, states, rep = sim_adoo(init_res_sol(G, 200 * BARSA, np.array([0.1, 0.9])), model, schedule,
+                                  LinearSolver=ls)
+        runs[name] = (states, [r["Iterations"] for r in rep["ControlstepReports"]])
+    (sd, itd), (sg, itg) = runs["direct"], runs["gpu"]
+    assert itd == itg
+    for a, b in zip(sg, sd):
+        pa, pb = np.asarray(a["pressure"]), np.asarray(b["pressure"])
+        assert np.abs(pa - pb).max() <= 1e-8 * np.abs(pb).max()
+        assert np.abs(np.asarray(a["s"])[:, 0] - np.asarray(b["s"])[:, 0]).max() <= 1e-7

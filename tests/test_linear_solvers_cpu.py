@@ -126,3 +126,65 @@ def test_linearized_problem_assembly_sign_and_increment_split():
     assert np.array_equal(b, [-1.0, -2.0, -3.0])
     parts = GpuCPRSolver.store_increments(LinearizedProblem(eqs), np.arange(3.0))
     assert [p.tolist() for p in parts] == [[0.0, 1.0], [2.0]]
+
+
+def _reference_adoo_problem():
+    """A linearized problem of the reference's AD-OO oil-water model (its own
+    get_equations through its FacilityModel), from the reference package
+    installed under baseline/_ref; skipped where that install is absent."""
+    import sys
+    from pathlib import Path
+    ref = Path(__file__).resolve().parents[1] / "baseline" / "_ref"
+    if not (ref / "pymrst").is_dir():
+        pytest.skip("the reference package is not installed under baseline/_ref")
+    if str(ref) not in sys.path:
+        sys.path.insert(0, str(ref))
+    from pymrst.gridprocessing import cart_grid, compute_geometry
+    from pymrst.modules.ad_blackoil.models.two_phase_oil_water_model import TwoPhaseOilWaterModel
+    from pymrst.modules.ad_core.utils.schedule import simple_schedule
+    from pymrst.modules.ad_props import init_simple_adi_fluid as ref_fluid
+    from pymrst.params import make_rock
+    from pymrst.params.wells_and_bc.vertical_well import vertical_well
+    from pymrst.solvers.init_res_sol import init_res_sol
+    from pymrst.utils.units import BARSA as B, CENTI as C_, DARCY, DAY, MILLI, POISE as P_
+    G = compute_geometry(cart_grid([10, 8, 3], [100.0, 80.0, 6.0]))
+    rng = np.random.default_rng(0)
+    rock = make_rock(G, np.exp(rng.normal(np.log(100), 0.5, G.cells.num))[:, None] * MILLI * DARCY, 0.2)
+    fluid = ref_fluid(mu=np.array([1, 5]) * C_ * P_, rho=np.array([1000.0, 800.0]), n=[2, 2],
+                      c=[1e-5 / B, 1e-5 / B], p_ref=200 * B, phases="wo")
+    rate = 0.2 * float(np.sum(0.2 * G.cells.volumes)) / (100 * DAY)
+    W = vertical_well([], G, rock, 0, 0, None, val=rate, well_type="rate", compi=np.array([1.0, 0.0]), name="I")
+    W = vertical_well(W, G, rock, 9, 7, None, val=150 * B, well_type="bhp", compi=np.array([0.0, 1.0]), name="P")
+    schedule = simple_schedule(np.full(1, 10 * DAY), W=W)
+    model = TwoPhaseOilWaterModel(G, rock, fluid)
+    state = init_res_sol(G, 200 * B, np.array([0.1, 0.9]))
+    forces = model.get_driving_forces(schedule.controls[0])
+    model = model.validate_model(forces)
+    state = model.validate_state(state)
+    dt = float(schedule.step_val[0])
+    model, st = model.prepare_timestep(state, state, dt, forces)
+    model.FacilityModel = model.FacilityModel.validate_model(forces)
+    model, st = model.prepare_report_step(st, state, dt, forces)
+    model, st = model.prepare_timestep(st, state, dt, forces)
+    st["pressure"] = st["pressure"] + np.linspace(0.0, 3.0 * B, G.cells.num)
+    problem, _ = model.get_equations(state, st, dt, forces, iteration=1)
+    return model, problem
+
+
+def test_cpr_ad_decoupling_keeps_the_solution_of_the_reference_problem():
+    """GpuCPRSolverAD's dynamic row-sum decoupling is an invertible row
+    transformation (plus a pressure column scaling): solving the decoupled
+    system gives the increments of the reference problem's own direct solve
+    and of the reference's CPRSolverAD."""
+    import scipy.sparse.linalg as spla
+    model, problem = _reference_adoo_problem()
+    from pymrst.modules.ad_core.solvers.concrete_solvers import BackslashSolverAD
+    from pymrst.modules.ad_core.solvers.cpr_solver_ad import CPRSolverAD
+    from pymrst_b200.linear_solvers import GpuCPRSolverAD
+    A, b, colscale, widths, p, ncell, nc = GpuCPRSolverAD().decoupled_system(problem, model)
+    assert p == 0 and ncell == 2 and A.shape[0] == sum(widths)
+    x = spla.spsolve(A.tocsc(), b) * colscale
+    _, ref, _ = BackslashSolverAD().solve_linear_problem(problem, model)
+    np.testing.assert_allclose(x, ref, rtol=1e-9, atol=1e-12 * np.abs(ref).max())
+    _, ref_cpr, _ = CPRSolverAD(tolerance=1e-12, maxIterations=200).solve_linear_problem(problem, model)
+    np.testing.assert_allclose(x, ref_cpr, rtol=1e-6, atol=1e-9 * np.abs(ref).max())
