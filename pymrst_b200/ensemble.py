@@ -269,23 +269,52 @@ class GpuOilWaterEnsemble(GpuOilWaterModel):
 
 def simulate_members_concurrently(members: Sequence, fluid, states0: Sequence[OWState], timesteps: Sequence[float],
                                   gravity: float = 0.0, workers: int = 16, max_cuts: int = 6,
-                                  model_options: Optional[dict] = None):
-    """Every member on its own device model and CUDA stream, `workers` host
-    threads stepping members concurrently; each member follows exactly the
+                                  model_options: Optional[dict] = None, replay_graph: bool = False):
+    """Every member on its own device model, `workers` host threads each
+    stepping members on its own CUDA stream; each member follows exactly the
     single-run path (simulate_schedule_ad), so its results are those of a
-    single run (the preconditioner is launched kernel by kernel rather than
-    replayed from a CUDA graph; the kernels are the same).  `members` are
-    (grid, rock, wells).  Returns
-    (states[member][step], iterations[member, step])."""
+    single run.  `members` are (grid, rock, wells).  Returns
+    (states[member][step], iterations[member, step]).
+
+    replay_graph=False launches each member's preconditioner kernel by
+    kernel, building and releasing the models inside the threads.  With
+    replay_graph=True every model is built before any thread steps and kept
+    until all have finished, so that no thread allocates or frees device
+    memory (which synchronises the device) while another captures its
+    preconditioner graph; the preconditioner is then replayed as a graph.  A
+    capture that is disturbed all the same falls back to direct launches for
+    that application."""
     import threading
     from concurrent.futures import ThreadPoolExecutor
     from .schedule import simulate_schedule_ad
     torch = _torch()
     opts = dict(model_options or {})
-    # A graph capture in one thread and device-wide work in another (a free,
-    # a device synchronisation) do not mix: the members launch directly,
-    # and the concurrency of the streams hides the launch latency instead.
-    opts["cpr_options"] = dict(opts.get("cpr_options") or {}, replay_graph=0)
+    opts["cpr_options"] = dict(opts.get("cpr_options") or {}, replay_graph=int(bool(replay_graph)))
+    workers = max(1, min(int(workers), len(members)))
+    if replay_graph:
+        streams = [torch.cuda.Stream() for _ in range(workers)]
+        models = []
+        for k, (g, rock, wells) in enumerate(members):
+            with torch.cuda.stream(streams[k % workers]):
+                models.append(GpuOilWaterModel(g, rock, fluid, wells, gravity=gravity, **opts))
+        torch.cuda.synchronize()
+
+        def run_share(w):
+            out = {}
+            with torch.cuda.stream(streams[w]):
+                for k in range(w, len(members), workers):
+                    out[k] = simulate_schedule_ad(states0[k], models[k], timesteps, max_cuts=max_cuts,
+                                                  verbose=False)
+                streams[w].synchronize()
+            return out
+
+        with ThreadPoolExecutor(max_workers=workers) as pool:
+            parts = list(pool.map(run_share, range(workers)))
+        torch.cuda.synchronize()
+        del models
+        merged = {k: v for part in parts for k, v in part.items()}
+        results = [merged[k] for k in range(len(members))]
+        return [r[0] for r in results], np.array([r[1] for r in results])
     local = threading.local()
 
     def run(k):
@@ -299,6 +328,6 @@ def simulate_members_concurrently(members: Sequence, fluid, states0: Sequence[OW
             del m
         return states, its
 
-    with ThreadPoolExecutor(max_workers=max(1, int(workers))) as pool:
+    with ThreadPoolExecutor(max_workers=workers) as pool:
         results = list(pool.map(run, range(len(members))))
     return [r[0] for r in results], np.array([r[1] for r in results])
