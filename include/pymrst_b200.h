@@ -419,6 +419,107 @@ int pmb_tpfa_reconstruct(pmb_tpfa* h, const double* d_p, double* d_flux, double*
                          double* d_perf_flux, double* d_perf_dp);
 int pmb_tpfa_levels(const pmb_tpfa* h, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
 
+/* ------------------------------------------------------------------------
+ * Three-phase black-oil model with dissolved gas (ThreePhaseBlackOilModelAD,
+ * pymrst/modules/ad_blackoil/models/three_phase_black_oil_model.py:93-565)
+ * and the deck-table fluid of init_deck_blackoil_fluid
+ * (pymrst/modules/ad_props/props/init_deck_adi_fluid.py:60-200).
+ *
+ * State (device, doubles): [p | sW | sO | sG | rs | status | qWs | qOs | qGs
+ * | bhp], nc entries per cell field and nw per well field; status is 1.0
+ * (undersaturated: the third unknown is rs) or 3.0 (free gas: it is sG).
+ * Residual and Jacobian are in the reference's variable-blocked order:
+ * equations water, oil, gas of every cell, then the water, oil and gas rate
+ * equations and the control equation of every well; unknowns p, sW, x of
+ * every cell, then qWs, qOs, qGs, bhp (combine_equations of assemble's
+ * seven equations).  The Jacobian's CSR pattern is fixed per handle
+ * (pmb_bo_pattern): every cell row holds its cell, its interface neighbours,
+ * the other cells of its well, and its well's four unknowns.
+ * Tables are piecewise linear with strictly increasing abscissae; interp_table
+ * (weights form, linear extrapolation) for gas, Rs_sat and saturation tables,
+ * the keyed 'parallel' interpolation for the live oil. */
+typedef struct pmb_bo pmb_bo;
+
+typedef struct pmb_bo_desc {
+  int32_t nc, nf, nw;
+  const int32_t* h_N;      /* nf x 2 interior interface neighbours */
+  const double* h_T;       /* nf transmissibilities */
+  const double* h_gdz;     /* nf gravity * (z[N1] - z[N0]) */
+  const double* h_pv;      /* nc reference pore volumes */
+  double rhoS[3];          /* surface densities water, oil, gas */
+  double pvtw[4];          /* p_ref, Bw at p_ref, compressibility, viscosity (assignPVTW) */
+  double rock[2];          /* p_ref, compressibility (assignROCK) */
+  double swcon;            /* connate water (first SWOF row) */
+  int32_t n_gas;           /* dry gas (PVDG with a p = 0 row): p, 1/Bg, mu_g */
+  const double* h_gas_p;
+  const double* h_gas_b;
+  const double* h_gas_mu;
+  int32_t n_rssat;         /* saturated Rs against pressure */
+  const double* h_rssat_p;
+  const double* h_rssat_rs;
+  int32_t n_key;           /* live oil (PVTO): Rs keys; rows of key k are branch_ptr[k] .. branch_ptr[k+1]-1 */
+  const double* h_key;
+  const int32_t* h_branch_ptr;
+  const double* h_branch_p;
+  const double* h_branch_b;   /* 1/Bo */
+  const double* h_branch_mu;
+  int32_t n_sw;            /* SWOF (flat-extended): sW, krW, pcOW (may be NULL) */
+  const double* h_sw;
+  const double* h_krw;
+  const double* h_pcow;
+  int32_t n_sow;           /* oil in water: sO, krOW */
+  const double* h_sow;
+  const double* h_krow;
+  int32_t n_sg;            /* SGOF (flat-extended): sG, krG, pcOG (may be NULL) */
+  const double* h_sg;
+  const double* h_krg;
+  const double* h_pcog;
+  int32_t n_sog;           /* oil in gas: sO, krOG */
+  const double* h_sog;
+  const double* h_krog;
+  /* wells: perforations of well k are perf_ptr[k] .. perf_ptr[k+1]-1 (1 to
+   * 16 each); a cell is perforated at most once */
+  const int32_t* h_perf_ptr;
+  const int32_t* h_perf_cell;
+  const double* h_perf_WI;
+  const int32_t* h_well_type;  /* 0 bhp, 1 rate (total surface rate), 2 orat */
+  const double* h_well_val;
+  const double* h_compi;       /* nw x 3 */
+  double tol_cnv, tol_mb, tol_well, ds_max;
+} pmb_bo_desc;
+
+int pmb_bo_create(const pmb_bo_desc* desc, void* stream, pmb_bo** out);
+int pmb_bo_destroy(pmb_bo* h);
+/* h_out3 = [unknowns 3 nc + 4 nw, Jacobian nonzeros, state length 6 nc + 4 nw]. */
+int pmb_bo_sizes(const pmb_bo* h, int64_t* h_out3);
+int pmb_bo_pattern(const pmb_bo* h, int32_t* h_row_ptr, int32_t* h_col);
+/* Residual and Jacobian values at d_state, with d_state0 the state at the
+ * start of the step (assemble, three_phase_black_oil_model.py:314-381). */
+int pmb_bo_assemble(pmb_bo* h, const double* d_state, const double* d_state0, double dt, double* d_res,
+                    double* d_vals);
+/* Convergence of an assembled residual (_converged, :528-539): h_out14 =
+ * [cnv water, oil, gas, mb water, oil, gas, max well-rate residual / q_ref,
+ * max |control residual| / scale, converged, CPR weights 1/bW 1/bO 1/bG at
+ * the mean pressure (get_scaling_factors_cpr, :205-245), mean pressure,
+ * total pore volume].  Synchronises the stream. */
+int pmb_bo_convergence(pmb_bo* h, const double* d_res, const double* d_state, double dt, double* h_out14);
+/* Newton update with the reference's limits and the black-oil flash
+ * (update_state and _flash, :439-508); d_dx in the unknowns' order. */
+int pmb_bo_update(pmb_bo* h, double* d_state, const double* d_dx);
+/* One step by Newton (step, :541-565) with the CSR CPR-GMRES as the linear
+ * solver; d_state holds the start state and receives the last iterate.
+ * h_stats4 = [iterations, converged, Krylov iterations, linear solves that
+ * missed their tolerance]. */
+int pmb_bo_step(pmb_bo* h, double* d_state, double dt, int32_t max_iterations, const pmb_cpr_opts* opts,
+                double* h_stats4);
+/* The fluid at n points (tests and the host's fluid check): d_out7 =
+ * [bW(p), bO(p, rs, sat), muO(p, rs, sat), bG(p), muG(p), Rs_sat(p),
+ * pore-volume multiplier(p)], n entries each. */
+int pmb_bo_pvt_points(pmb_bo* h, int32_t n, const double* d_p, const double* d_rs, const double* d_sat,
+                      double* d_out7);
+/* d_out5 = [krW, krO, krG, pcOW, pcOG] at (sW, sG), sO = 1 - sW - sG. */
+int pmb_bo_relperm_points(pmb_bo* h, int32_t n, const double* d_sw, const double* d_sg, double* d_out5);
+
 /* Host-side aggregation of the AMG hierarchy for a CSR matrix (no device
  * needed): unknowns per level into h_sizes (up to max_levels), count in
  * *n_levels.  Exposed for testing the set-up logic. */

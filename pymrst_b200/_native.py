@@ -71,6 +71,25 @@ class TpfaForces(C.Structure):
     ]
 
 
+class BODesc(C.Structure):
+    _fields_ = [
+        ("nc", c_int), ("nf", c_int), ("nw", c_int),
+        ("h_N", P_i32), ("h_T", P_dbl), ("h_gdz", P_dbl), ("h_pv", P_dbl),
+        ("rhoS", c_dbl * 3), ("pvtw", c_dbl * 4), ("rock", c_dbl * 2), ("swcon", c_dbl),
+        ("n_gas", c_int), ("h_gas_p", P_dbl), ("h_gas_b", P_dbl), ("h_gas_mu", P_dbl),
+        ("n_rssat", c_int), ("h_rssat_p", P_dbl), ("h_rssat_rs", P_dbl),
+        ("n_key", c_int), ("h_key", P_dbl), ("h_branch_ptr", P_i32), ("h_branch_p", P_dbl),
+        ("h_branch_b", P_dbl), ("h_branch_mu", P_dbl),
+        ("n_sw", c_int), ("h_sw", P_dbl), ("h_krw", P_dbl), ("h_pcow", P_dbl),
+        ("n_sow", c_int), ("h_sow", P_dbl), ("h_krow", P_dbl),
+        ("n_sg", c_int), ("h_sg", P_dbl), ("h_krg", P_dbl), ("h_pcog", P_dbl),
+        ("n_sog", c_int), ("h_sog", P_dbl), ("h_krog", P_dbl),
+        ("h_perf_ptr", P_i32), ("h_perf_cell", P_i32), ("h_perf_WI", P_dbl), ("h_well_type", P_i32),
+        ("h_well_val", P_dbl), ("h_compi", P_dbl),
+        ("tol_cnv", c_dbl), ("tol_mb", c_dbl), ("tol_well", c_dbl), ("ds_max", c_dbl),
+    ]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "pmb_last_error": (C.c_char_p, []),
@@ -129,6 +148,16 @@ SIGNATURES = {
     "pmb_tpfa_solve": (c_int, [c_vp, c_vp, c_vp, c_vp, c_dbl, c_int, P_dbl]),
     "pmb_tpfa_reconstruct": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_tpfa_levels": (c_int, [c_vp, c_int, P_i64, P_i32]),
+    "pmb_bo_create": (c_int, [C.POINTER(BODesc), c_vp, C.POINTER(c_vp)]),
+    "pmb_bo_destroy": (c_int, [c_vp]),
+    "pmb_bo_sizes": (c_int, [c_vp, P_i64]),
+    "pmb_bo_pattern": (c_int, [c_vp, P_i32, P_i32]),
+    "pmb_bo_assemble": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp]),
+    "pmb_bo_convergence": (c_int, [c_vp, c_vp, c_vp, c_dbl, P_dbl]),
+    "pmb_bo_update": (c_int, [c_vp, c_vp, c_vp]),
+    "pmb_bo_step": (c_int, [c_vp, c_vp, c_dbl, c_int, C.POINTER(CPROpts), P_dbl]),
+    "pmb_bo_pvt_points": (c_int, [c_vp, c_int, c_vp, c_vp, c_vp, c_vp]),
+    "pmb_bo_relperm_points": (c_int, [c_vp, c_int, c_vp, c_vp, c_vp]),
     "pmb_amg_hierarchy_host": (c_int, [c_int, P_i32, P_i32, P_dbl, c_dbl, c_int, c_int, P_i64, P_i32]),
 }
 

@@ -1,0 +1,440 @@
+"""Three-phase black-oil model with dissolved gas on the GPU, with the
+interface of the reference's ThreePhaseBlackOilModelAD
+(pymrst/modules/ad_blackoil/models/three_phase_black_oil_model.py:93-565):
+the constructor `(g, rock, fluid, wells, gravity, ds_max, tol_cnv, tol_mb,
+tol_well, max_iterations)`, a state with fields pressure, s (nc x 3), rs,
+status (1 undersaturated, 3 free gas), qWs, qOs, qGs, bhp, and
+`step(state, dt) -> (state, converged, iterations)`.
+
+Assembly, convergence, the Newton update with the flash, and the linear
+solve all run on the device (`csrc/bo.cu` through the `pmb_bo_*` entry
+points, the CPR-GMRES of `csrc/csrcpr.cu`); the host converts states and
+reads one small convergence record per Newton iteration.
+
+The fluid is a deck-table fluid: either the reference's BlackOilFluid built
+by init_deck_blackoil_fluid (its tables are read from the fluid's functions
+and checked point by point against them on the device), a parsed deck
+dictionary of the same layout (pvtw, rock_cp, pvdg, pvto, swof, sgof, rhoS),
+or `BlackOilTables`.  Not supported (ValueError): wet gas (PVTG / vaporised
+oil), J-function scaling, water viscosibility, a cell perforated twice.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Any, Dict, Optional, Sequence
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _native as N
+from .ow_model import _opts_struct, _torch, default_cpr_options, face_transmissibility_device
+from .params import pore_volume
+
+NORM_GRAVITY = 9.80665
+
+
+@dataclass
+class BOState:
+    """Black-oil state (the reference's BOState fields)."""
+    pressure: np.ndarray
+    s: np.ndarray
+    rs: np.ndarray
+    status: np.ndarray
+    qWs: np.ndarray
+    qOs: np.ndarray
+    qGs: np.ndarray
+    bhp: np.ndarray
+
+    def copy(self) -> "BOState":
+        return BOState(*(np.array(v, copy=True) for v in (self.pressure, self.s, self.rs, self.status,
+                                                           self.qWs, self.qOs, self.qGs, self.bhp)))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+
+
+def _extend(tab: np.ndarray, pm: float = 1.0) -> np.ndarray:
+    """One flat row added at each end, at x[0] - pm and x[-1] + pm (the
+    reference's extend_tab, ad_props/utils/extend_tab.py:25-38)."""
+    tab = np.asarray(tab, dtype=float)
+    first, last = tab[0].copy(), tab[-1].copy()
+    first[0] -= pm
+    last[0] += pm
+    return np.vstack([first, tab, last])
+
+
+@dataclass
+class BlackOilTables:
+    """The piecewise-linear tables of a live-oil / dry-gas fluid, in the form
+    the device evaluates (abscissae strictly increasing)."""
+    rhoS: np.ndarray
+    pvtw: np.ndarray          # p_ref, Bw at p_ref, compressibility, viscosity
+    rock: np.ndarray          # p_ref, compressibility
+    swcon: float
+    gas_p: np.ndarray
+    gas_b: np.ndarray         # 1 / Bg
+    gas_mu: np.ndarray
+    rssat_p: np.ndarray
+    rssat_rs: np.ndarray
+    key: np.ndarray           # Rs keys of the live-oil branches
+    branch_ptr: np.ndarray
+    branch_p: np.ndarray
+    branch_b: np.ndarray      # 1 / Bo
+    branch_mu: np.ndarray
+    sw: np.ndarray
+    krw: np.ndarray
+    sow: np.ndarray
+    krow: np.ndarray
+    sg: np.ndarray
+    krg: np.ndarray
+    sog: np.ndarray
+    krog: np.ndarray
+    pcow: Optional[np.ndarray] = None
+    pcog: Optional[np.ndarray] = None
+
+    @classmethod
+    def from_deck(cls, deck: Dict[str, Any]) -> "BlackOilTables":
+        """The tables of a parsed deck, prepared as init_deck_blackoil_fluid
+        prepares them (init_deck_adi_fluid.py:60-200): PVDG with a row at
+        p = 0 repeating the first one, PVTO branches keyed by Rs (a branch of
+        one row repeated one ulp higher in pressure), the saturated envelope
+        through (0, 0), SWOF / SGOF extended flat by one unit at both ends and
+        the oil curves as functions of sO."""
+        if "pvtg" in deck or "pvdg" not in deck:
+            raise ValueError("black-oil tables: wet gas (PVTG) is not supported; the deck needs PVDG")
+        if "pvto" not in deck:
+            raise ValueError("black-oil tables: the deck needs PVTO (live oil)")
+        if deck.get("jfunc") is not None or deck.get("JFUNC") is not None:
+            raise ValueError("black-oil tables: J-function scaling is not supported")
+        w, r = deck["pvtw"], deck["rock_cp"]
+        if float(w.get("viscosibility", 0.0)) != 0.0:
+            raise ValueError("black-oil tables: water viscosibility is not supported")
+        pvdg = np.asarray(deck["pvdg"], dtype=float)
+        gas_p = np.concatenate([[0.0], pvdg[:, 0]])
+        gas_b = np.concatenate([[1.0 / pvdg[0, 1]], 1.0 / pvdg[:, 1]])
+        gas_mu = np.concatenate([[pvdg[0, 2]], pvdg[:, 2]])
+        keys, rows_all, ptr, p_bub = [], [], [0], []
+        for key, original in deck["pvto"]:
+            rows = np.asarray(original, dtype=float)
+            p_bub.append(rows[0, 0])
+            if rows.shape[0] == 1:
+                rows = np.vstack([rows, rows[0]])
+                rows[1, 0] = np.nextafter(rows[0, 0], np.inf)
+            keys.append(float(key))
+            rows_all.append(rows)
+            ptr.append(ptr[-1] + rows.shape[0])
+        rows = np.vstack(rows_all)
+        swof, sgof = _extend(deck["swof"]), _extend(deck["sgof"])
+        swcon = float(np.asarray(deck["swof"])[0, 0])
+        return cls(
+            rhoS=_f64(deck["rhoS"])[:3],
+            pvtw=np.array([w["p_ref"], w["b_ref"], w["c"], w["mu_ref"]], dtype=float),
+            rock=np.array([r["p_ref"], r["c"]], dtype=float),
+            swcon=swcon,
+            gas_p=gas_p, gas_b=gas_b, gas_mu=gas_mu,
+            rssat_p=np.concatenate([[0.0], p_bub]), rssat_rs=np.concatenate([[0.0], keys]),
+            key=np.array(keys), branch_ptr=np.array(ptr, dtype=np.int32),
+            branch_p=rows[:, 0].copy(), branch_b=1.0 / rows[:, 1], branch_mu=rows[:, 2].copy(),
+            sw=swof[:, 0].copy(), krw=swof[:, 1].copy(), pcow=swof[:, 3].copy() if swof.shape[1] > 3 else None,
+            sow=1.0 - swof[::-1, 0], krow=swof[::-1, 2].copy(),
+            sg=sgof[:, 0].copy(), krg=sgof[:, 1].copy(), pcog=sgof[:, 3].copy() if sgof.shape[1] > 3 else None,
+            sog=1.0 - (sgof[::-1, 0] + swcon), krog=sgof[::-1, 2].copy(),
+        )
+
+    @classmethod
+    def from_fluid(cls, fluid) -> "BlackOilTables":
+        """The tables held by a BlackOilFluid that init_deck_blackoil_fluid
+        built, read from the closures of its property functions."""
+        if getattr(fluid, "vapoil", False) or getattr(fluid, "rv_sat", None) is not None:
+            raise ValueError("black-oil tables: wet gas (vaporised oil) is not supported")
+
+        def cl(fn, *names):
+            fn = fn[0] if isinstance(fn, (list, tuple)) else fn
+            code = getattr(fn, "__code__", None)
+            cells = getattr(fn, "__closure__", None) or ()
+            env = dict(zip(code.co_freevars, (c.cell_contents for c in cells))) if code else {}
+            missing = [n for n in names if n not in env]
+            if missing:
+                raise ValueError("black-oil tables: the fluid's functions are not those of a deck-table "
+                                 f"fluid (no {', '.join(missing)} in {getattr(fn, '__name__', fn)!r})")
+            return [env[n] for n in names]
+
+        (w,) = cl(fluid.b_w, "w")
+        (r,) = cl(fluid.pv_mult, "r")
+        p_g, bg = cl(fluid.b_g, "p_g", "bg_tab")
+        (mug,) = cl(fluid.mu_g, "mug_tab")
+        (bo_tab,) = cl(fluid.b_o, "bo_tab")
+        (muo_tab,) = cl(fluid.mu_o, "muo_tab")
+        p_t, rs_t = cl(fluid.rs_sat, "p_t", "rs_t")
+        sw_tab, krw_tab = cl(fluid.kr_w, "sw_tab", "krw_tab")
+        sg_tab, krg_tab = cl(fluid.kr_g, "sg_tab", "krg_tab")
+        sow_tab, krow_tab = cl(fluid.kr_ow, "so_w_tab", "krow_tab")
+        sog_tab, krog_tab = cl(fluid.kr_og, "so_g_tab", "krog_tab")
+        pcow = cl(fluid.pc_ow, "pcow_tab")[0] if getattr(fluid, "pc_ow", None) is not None else None
+        pcog = cl(fluid.pc_og, "pcog_tab")[0] if getattr(fluid, "pc_og", None) is not None else None
+        if float(w.get("viscosibility", 0.0)) != 0.0:
+            raise ValueError("black-oil tables: water viscosibility is not supported")
+        if getattr(bo_tab, "matlab_interp1", False) or getattr(muo_tab, "matlab_interp1", False):
+            raise ValueError("black-oil tables: only the keyed tables of init_deck_blackoil_fluid are supported")
+        ptr = np.concatenate([[0], np.cumsum([np.asarray(b[0]).size for b in bo_tab.branches])]).astype(np.int32)
+        return cls(
+            rhoS=_f64(fluid.rhoS)[:3],
+            pvtw=np.array([w["p_ref"], w["b_ref"], w["c"], w["mu_ref"]], dtype=float),
+            rock=np.array([r["p_ref"], r["c"]], dtype=float),
+            swcon=float(fluid.swcon),
+            gas_p=_f64(p_g), gas_b=_f64(bg), gas_mu=_f64(mug),
+            rssat_p=_f64(p_t), rssat_rs=_f64(rs_t),
+            key=_f64(bo_tab.key), branch_ptr=ptr,
+            branch_p=np.concatenate([_f64(b[0]) for b in bo_tab.branches]),
+            branch_b=np.concatenate([_f64(b[1]) for b in bo_tab.branches]),
+            branch_mu=np.concatenate([_f64(b[1]) for b in muo_tab.branches]),
+            sw=_f64(sw_tab), krw=_f64(krw_tab), pcow=None if pcow is None else _f64(pcow),
+            sow=_f64(sow_tab), krow=_f64(krow_tab),
+            sg=_f64(sg_tab), krg=_f64(krg_tab), pcog=None if pcog is None else _f64(pcog),
+            sog=_f64(sog_tab), krog=_f64(krog_tab),
+        )
+
+
+def _tables(fluid) -> BlackOilTables:
+    if isinstance(fluid, BlackOilTables):
+        return fluid
+    if isinstance(fluid, dict):
+        return BlackOilTables.from_deck(fluid)
+    return BlackOilTables.from_fluid(fluid)
+
+
+_WELL_TYPES = {"bhp": 0, "rate": 1, "orat": 2}
+
+
+class GpuBlackOilModel:
+    """Fully-implicit black-oil model on the GPU (reference
+    ThreePhaseBlackOilModelAD)."""
+
+    n_phases = 3
+    disgas = True
+    vapoil = False
+
+    def __init__(self, g, rock, fluid, wells: Sequence, gravity: float = NORM_GRAVITY, ds_max: float = 0.2,
+                 tol_cnv: float = 1e-3, tol_mb: float = 1e-7, tol_well: float = 1e-6, max_iterations: int = 25,
+                 cpr_options: Optional[dict] = None, T: Optional[np.ndarray] = None):
+        torch = _torch()
+        self.g = g
+        self.rock = rock
+        self.fluid = fluid
+        self.raw_fluid = fluid
+        self.wells = list(wells)
+        self.gravity = float(gravity)
+        self.ds_max = float(ds_max)
+        self.tol_cnv, self.tol_mb, self.tol_well = float(tol_cnv), float(tol_mb), float(tol_well)
+        self.max_iterations = int(max_iterations)
+        self.tables = _tables(fluid)
+        Nall = np.asarray(g.faces.neighbors, dtype=np.int64)
+        internal = np.all(Nall >= 0, axis=1)
+        self.N = Nall[internal]
+        if T is None:
+            tf, _ = face_transmissibility_device(g, rock)
+            T = tf[internal]
+        self.T = _f64(T)
+        z = np.asarray(g.cells.centroids, dtype=float)[:, -1]
+        self.gdz = self.gravity * (z[self.N[:, 1]] - z[self.N[:, 0]])
+        self.pv_ref = pore_volume(g, rock)
+        self.nc = int(g.cells.num)
+        self.nw = len(self.wells)
+        self.cpr_options = default_cpr_options(**({"rtol": 1e-10, "maxiter": 400, "amg_rebuild_interval": 1}
+                                                  | dict(cpr_options or {})))
+        self._stream = torch.cuda.current_stream()
+        self._build()
+        if not isinstance(fluid, (BlackOilTables, dict)):
+            self._check_fluid(fluid)
+
+    @property
+    def G(self):
+        return self.g
+
+    # -- set-up -------------------------------------------------------------
+    def _build(self):
+        t = self.tables
+        nw = self.nw
+        for w in self.wells:
+            if str(w.type).lower() not in _WELL_TYPES:
+                raise ValueError(f"unsupported control '{w.type}'")
+        perf_cells = [np.asarray(w.cells, np.int64).ravel() for w in self.wells]
+        perf_ptr = np.zeros(nw + 1, dtype=np.int32)
+        if nw:
+            perf_ptr[1:] = np.cumsum([c.size for c in perf_cells])
+        cat = lambda xs, dt: np.ascontiguousarray(np.concatenate(xs), dtype=dt) if xs else np.zeros(1, dt)
+        h = dict(
+            N=np.ascontiguousarray(self.N, dtype=np.int32), T=self.T, gdz=_f64(self.gdz), pv=_f64(self.pv_ref),
+            perf_ptr=perf_ptr, perf_cell=cat(perf_cells, np.int32),
+            perf_WI=cat([_f64(w.WI) for w in self.wells], np.float64),
+            well_type=np.array([_WELL_TYPES[str(w.type).lower()] for w in self.wells] or [0], dtype=np.int32),
+            well_val=np.array([float(np.ravel(w.val)[0]) for w in self.wells] or [0.0]),
+            compi=np.ascontiguousarray([_f64(w.compi)[:3] for w in self.wells] if nw else np.zeros((1, 3))),
+        )
+        for name in ("gas_p", "gas_b", "gas_mu", "rssat_p", "rssat_rs", "key", "branch_p", "branch_b",
+                     "branch_mu", "sw", "krw", "sow", "krow", "sg", "krg", "sog", "krog"):
+            h[name] = _f64(getattr(t, name))
+        h["branch_ptr"] = np.ascontiguousarray(t.branch_ptr, dtype=np.int32)
+        for name in ("pcow", "pcog"):
+            v = getattr(t, name)
+            h[name] = None if v is None else _f64(v)
+        self._h = h
+        d = N.BODesc()
+        d.nc, d.nf, d.nw = self.nc, self.N.shape[0], nw
+        dp = lambda a: N.as_p(a, N.C.c_double) if a is not None else None
+        ip = lambda a: N.as_p(a, N.C.c_int32)
+        d.h_N, d.h_T, d.h_gdz, d.h_pv = ip(h["N"]), dp(h["T"]), dp(h["gdz"]), dp(h["pv"])
+        for i in range(3):
+            d.rhoS[i] = float(t.rhoS[i])
+        for i in range(4):
+            d.pvtw[i] = float(t.pvtw[i])
+        d.rock[0], d.rock[1] = float(t.rock[0]), float(t.rock[1])
+        d.swcon = float(t.swcon)
+        d.n_gas, d.h_gas_p, d.h_gas_b, d.h_gas_mu = h["gas_p"].size, dp(h["gas_p"]), dp(h["gas_b"]), dp(h["gas_mu"])
+        d.n_rssat, d.h_rssat_p, d.h_rssat_rs = h["rssat_p"].size, dp(h["rssat_p"]), dp(h["rssat_rs"])
+        d.n_key, d.h_key, d.h_branch_ptr = h["key"].size, dp(h["key"]), ip(h["branch_ptr"])
+        d.h_branch_p, d.h_branch_b, d.h_branch_mu = dp(h["branch_p"]), dp(h["branch_b"]), dp(h["branch_mu"])
+        d.n_sw, d.h_sw, d.h_krw, d.h_pcow = h["sw"].size, dp(h["sw"]), dp(h["krw"]), dp(h["pcow"])
+        d.n_sow, d.h_sow, d.h_krow = h["sow"].size, dp(h["sow"]), dp(h["krow"])
+        d.n_sg, d.h_sg, d.h_krg, d.h_pcog = h["sg"].size, dp(h["sg"]), dp(h["krg"]), dp(h["pcog"])
+        d.n_sog, d.h_sog, d.h_krog = h["sog"].size, dp(h["sog"]), dp(h["krog"])
+        d.h_perf_ptr, d.h_perf_cell, d.h_perf_WI = ip(h["perf_ptr"]), ip(h["perf_cell"]), dp(h["perf_WI"])
+        d.h_well_type, d.h_well_val, d.h_compi = ip(h["well_type"]), dp(h["well_val"]), dp(h["compi"])
+        d.tol_cnv, d.tol_mb, d.tol_well, d.ds_max = self.tol_cnv, self.tol_mb, self.tol_well, self.ds_max
+        hd = N.c_vp()
+        N.check(N.lib().pmb_bo_create(N.C.byref(d), self._stream.cuda_stream, N.C.byref(hd)))
+        self._handle = hd
+        sizes = (N.C.c_int64 * 3)()
+        N.check(N.lib().pmb_bo_sizes(hd, sizes))
+        self.n_unknowns, self.nnz, self.state_len = (int(v) for v in sizes)
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                N.lib().pmb_bo_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+    def _check_fluid(self, fluid, rtol: float = 1e-12) -> None:
+        """The device tables must reproduce the fluid's own functions."""
+        t = self.tables
+        p = np.linspace(0.0, 1.3 * max(t.branch_p.max(), t.gas_p.max()), 41)[1:]
+        rs = np.linspace(0.5 * t.key.min(), 1.1 * t.key.max(), p.size)
+        got = self.pvt_points(p, rs, np.zeros(p.size, bool))
+        got_sat = self.pvt_points(p, rs, np.ones(p.size, bool))
+        want = [fluid.b_w(p), fluid.b_o(p, rs, np.zeros(p.size, bool)), fluid.mu_o(p, rs, np.zeros(p.size, bool)),
+                fluid.b_g(p), fluid.mu_g(p), fluid.rs_sat(p), fluid.pv_mult(p)]
+        want_sat = [fluid.b_o(p, rs, np.ones(p.size, bool)), fluid.mu_o(p, rs, np.ones(p.size, bool))]
+        pairs = list(zip(got, want)) + list(zip(got_sat[1:3], want_sat))
+        sw = np.linspace(0.0, 1.0, 23)
+        sg = np.clip(np.linspace(0.4, 0.0, 23), 0.0, 1.0 - sw)
+        kr = self.relperm_points(sw, sg)
+        so = 1.0 - sw - sg
+        pairs += [(kr[0], fluid.kr_w(sw)), (kr[1], fluid.kr_o(sw, so, sg)), (kr[2], fluid.kr_g(sg))]
+        for a, b in pairs:
+            b = np.asarray(b, dtype=float).ravel() * np.ones(a.size)
+            if not np.allclose(a, b, rtol=rtol, atol=1e-300):
+                raise ValueError("black-oil tables: the tables read from the fluid do not reproduce its "
+                                 "functions; build the model from the deck instead")
+
+    # -- states -------------------------------------------------------------
+    def to_device(self, st):
+        torch = _torch()
+        s = np.asarray(st.s, dtype=float)
+        x = np.concatenate([_f64(st.pressure), s[:, 0], s[:, 1], s[:, 2], _f64(st.rs),
+                            np.asarray(st.status, dtype=float).ravel(), _f64(st.qWs), _f64(st.qOs), _f64(st.qGs),
+                            _f64(st.bhp)])
+        return torch.as_tensor(x, device="cuda")
+
+    def from_device(self, x, like=None):
+        v = x.detach().cpu().numpy()
+        nc, nw = self.nc, self.nw
+        f = lambda i: v[i * nc:(i + 1) * nc].copy()
+        w = lambda i: v[6 * nc + i * nw: 6 * nc + (i + 1) * nw].copy()
+        fields = dict(pressure=f(0), s=np.column_stack([f(1), f(2), f(3)]), rs=f(4),
+                      status=f(5).astype(np.int64), qWs=w(0), qOs=w(1), qGs=w(2), bhp=w(3))
+        cls = type(like) if like is not None else BOState
+        try:
+            return cls(**fields)
+        except TypeError:
+            return BOState(**fields)
+
+    # -- device primitives ----------------------------------------------------
+    def _sync(self):
+        self._stream.synchronize()
+
+    def assemble_system(self, st0, st, dt: float):
+        """(residual, Jacobian as scipy CSR) of the equations at `st` with
+        `st0` the state at the start of the step, in the reference's
+        variable-blocked order (combine_equations of assemble's output)."""
+        torch = _torch()
+        x, x0 = self.to_device(st), self.to_device(st0)
+        res = torch.empty(self.n_unknowns, dtype=torch.float64, device="cuda")
+        vals = torch.empty(self.nnz, dtype=torch.float64, device="cuda")
+        N.check(N.lib().pmb_bo_assemble(self._handle, N.ptr(x), N.ptr(x0), float(dt), N.ptr(res), N.ptr(vals)))
+        rp = np.empty(self.n_unknowns + 1, dtype=np.int32)
+        col = np.empty(self.nnz, dtype=np.int32)
+        N.check(N.lib().pmb_bo_pattern(self._handle, N.as_p(rp, N.C.c_int32), N.as_p(col, N.C.c_int32)))
+        jac = sp.csr_matrix((vals.cpu().numpy(), col, rp), shape=(self.n_unknowns, self.n_unknowns))
+        return res.cpu().numpy(), jac
+
+    def convergence(self, st0, st, dt: float) -> Dict[str, Any]:
+        """CNV / MB / well tests of the equations at `st`."""
+        torch = _torch()
+        x, x0 = self.to_device(st), self.to_device(st0)
+        res = torch.empty(self.n_unknowns, dtype=torch.float64, device="cuda")
+        vals = torch.empty(self.nnz, dtype=torch.float64, device="cuda")
+        N.check(N.lib().pmb_bo_assemble(self._handle, N.ptr(x), N.ptr(x0), float(dt), N.ptr(res), N.ptr(vals)))
+        out = (N.C.c_double * 14)()
+        N.check(N.lib().pmb_bo_convergence(self._handle, N.ptr(res), N.ptr(x), float(dt), out))
+        o = list(out)
+        return dict(cnv=o[0:3], mb=o[3:6], well=o[6], ctrl=o[7], converged=bool(o[8]), weights=o[9:12],
+                    p_mean=o[12], pv_total=o[13])
+
+    def update_state(self, st, upd):
+        """Newton update with the limits and flash of the reference."""
+        torch = _torch()
+        x = self.to_device(st)
+        dx = torch.as_tensor(_f64(upd), device="cuda")
+        N.check(N.lib().pmb_bo_update(self._handle, N.ptr(x), N.ptr(dx)))
+        return self.from_device(x, like=st)
+
+    def pvt_points(self, p, rs, sat):
+        torch = _torch()
+        n = int(np.size(p))
+        t = lambda a: torch.as_tensor(_f64(a), device="cuda")
+        out = torch.empty(7 * max(n, 1), dtype=torch.float64, device="cuda")
+        dp_, drs, dsat = t(p), t(rs), t(np.asarray(sat, dtype=float))  # alive until the kernel has run
+        N.check(N.lib().pmb_bo_pvt_points(self._handle, n, N.ptr(dp_), N.ptr(drs), N.ptr(dsat), N.ptr(out)))
+        return out.cpu().numpy()[:7 * n].reshape(7, n)
+
+    def relperm_points(self, sw, sg):
+        torch = _torch()
+        n = int(np.size(sw))
+        t = lambda a: torch.as_tensor(_f64(a), device="cuda")
+        out = torch.empty(5 * max(n, 1), dtype=torch.float64, device="cuda")
+        dsw, dsg = t(sw), t(sg)
+        N.check(N.lib().pmb_bo_relperm_points(self._handle, n, N.ptr(dsw), N.ptr(dsg), N.ptr(out)))
+        return out.cpu().numpy()[:5 * n].reshape(5, n)
+
+    # -- stepping -------------------------------------------------------------
+    def step_device(self, x, dt: float):
+        """One step on a device state vector in place: (converged, Newton
+        iterations, [iterations, converged, Krylov iterations, missed
+        linear tolerances])."""
+        stats = (N.C.c_double * 4)()
+        opts = _opts_struct(self.cpr_options)
+        N.check(N.lib().pmb_bo_step(self._handle, N.ptr(x), float(dt), self.max_iterations, N.C.byref(opts), stats))
+        return bool(stats[1]), int(stats[0]), list(stats)
+
+    def step(self, state, dt: float):
+        """(new state, converged, iterations) as the reference's step."""
+        x = self.to_device(state)
+        ok, its, stats = self.step_device(x, dt)
+        self.last_step_stats = stats
+        return self.from_device(x, like=state), ok, its

@@ -21,6 +21,12 @@ value distributions (all seeded with numpy's default_rng):
 * `ow_fluid()`: Corey n = 2 with Swc = Sor = 0.1, mu_w = 1 cP, mu_o = 5 cP,
   rho 1000 / 800 kg/m^3, compressibility 1e-5 / bar for both phases,
   p_ref = 200 bar.
+* `synthetic_blackoil_deck()`: a live-oil / dry-gas black-oil description in
+  the layout of a parsed deck (PVTW, ROCK, PVDG, PVTO, SWOF, SGOF, surface
+  densities; SI units), with smooth analytic tables of the usual shapes: six
+  PVTO keys (Rs 10 .. 160 sm^3/sm^3, bubble points 15 .. 240 bar), each with
+  an undersaturated branch of four rows; gas FVF ~ 1/p; Corey-like relative
+  permeabilities with Swc = 0.15 and small capillary pressures.
 """
 
 from __future__ import annotations
@@ -187,3 +193,33 @@ def incompressible_quarter_five_spot(dims=(64, 64, 8), cell_size=(10.0, 10.0, 2.
     wells = add_well(wells, g, rock, cell_index(g, nx - 1, ny - 1, k), well_type="bhp", val=100 * BARSA,
                      radius=0.1, compi=np.array([1.0]))
     return IncompCase(f"incomp_{nx}x{ny}x{nz}", g, rock, wells, 1 * CENTI * POISE, 1000.0)
+
+
+def synthetic_blackoil_deck() -> dict:
+    """Black-oil tables in the layout of a parsed deck (SI units): keys
+    pvtw, rock_cp, pvdg, pvto (list of (Rs, rows [p, Bo, mu_o])), swof
+    (sw, krw, krow, pcow), sgof (sg, krg, krog, pcog) and rhoS (water, oil,
+    gas).  Analytic, smooth and monotone; no field data."""
+    bar, cp = BARSA, CENTI * POISE
+    pg = np.array([10.0, 30.0, 60.0, 100.0, 150.0, 200.0, 260.0, 330.0, 400.0])
+    pvdg = np.column_stack([pg * bar, (0.95 + 3e-4 * pg) / pg, (0.012 + 4.5e-5 * pg) * cp])
+    keys = np.array([10.0, 40.0, 70.0, 100.0, 130.0, 160.0])
+    p_bub = np.array([15.0, 60.0, 105.0, 150.0, 195.0, 240.0])
+    pvto = []
+    for rs, pb in zip(keys, p_bub):
+        dp = np.array([0.0, 80.0, 160.0, 240.0])
+        bo_sat, mu_sat = 1.05 + 0.0025 * rs, 1.6 - 0.006 * rs
+        rows = np.column_stack([(pb + dp) * bar, bo_sat * np.exp(-1.5e-4 * dp), mu_sat * (1.0 + 1e-3 * dp) * cp])
+        pvto.append((float(rs), rows))
+    sw = np.linspace(0.15, 1.0, 12)
+    u = (sw - 0.15) / 0.85
+    swof = np.column_stack([sw, 0.6 * u ** 2.5, (1.0 - u) ** 2, 0.2 * bar * (1.0 - u) ** 2])
+    sg = np.linspace(0.0, 0.85, 12)
+    v = sg / 0.85
+    sgof = np.column_stack([sg, 0.8 * v ** 2, (1.0 - v) ** 3, 0.05 * bar * v])
+    return dict(
+        pvtw=dict(p_ref=250.0 * bar, b_ref=1.03, c=4.5e-10, mu_ref=0.4 * cp, viscosibility=0.0),
+        rock_cp=dict(p_ref=250.0 * bar, c=6e-10),
+        pvdg=pvdg, pvto=pvto, swof=swof, sgof=sgof,
+        rhoS=np.array([1020.0, 840.0, 0.95]),
+    )

@@ -544,7 +544,8 @@ class GpuOilWaterModel:
         d = self.pack(OWState(pressure=dx[:nc], sW=dx[nc:2 * nc], qWs=dx[2 * nc:2 * nc + nw],
                               qOs=dx[2 * nc + nw:2 * nc + 2 * nw], bhp=dx[2 * nc + 2 * nw:]))
         x = self.to_device(state)
-        N.check(N.lib().pmb_ow_update(self._handle, N.ptr(x), N.ptr(torch.as_tensor(d, device="cuda")), 1.0))
+        dd = torch.as_tensor(d, device="cuda")  # held until the update kernel has run
+        N.check(N.lib().pmb_ow_update(self._handle, N.ptr(x), N.ptr(dd), 1.0))
         return self.from_device(x)
 
     def cpr_levels(self):

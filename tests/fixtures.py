@@ -42,3 +42,29 @@ def ow_case(d):
     rock = make_rock(g, d["perm"][:, None], float(d["poro"]))
     fluid = ow_fluid(d["fluid_kind"])
     return g, rock, fluid, wells_from(d)
+
+
+def bo_deck(d):
+    """The synthetic deck stored in a black-oil fixture, in the parsed-deck
+    layout (pvtw, rock_cp, pvdg, pvto, swof, sgof, rhoS)."""
+    w, r = d["pvtw"], d["rock_cp"]
+    rows, nrows, keys = d["pvto_rows"], d["pvto_nrows"], d["pvto_keys"]
+    starts = np.concatenate([[0], np.cumsum(nrows)])
+    pvto = [(float(k), rows[starts[i]:starts[i + 1]]) for i, k in enumerate(keys)]
+    return dict(pvtw=dict(p_ref=w[0], b_ref=w[1], c=w[2], mu_ref=w[3], viscosibility=w[4]),
+                rock_cp=dict(p_ref=r[0], c=r[1]), pvdg=d["pvdg"], pvto=pvto, swof=d["swof"], sgof=d["sgof"],
+                rhoS=d["rhoS"])
+
+
+def bo_case(d):
+    """Grid, rock, deck and wells of a black-oil fixture."""
+    g = cartesian_grid(d["dims"], d["phys"])
+    rock = make_rock(g, d["perm"][:, None], float(d["poro"]))
+    return g, rock, bo_deck(d), wells_from(d)
+
+
+def bo_state(d, prefix):
+    from pymrst_b200.blackoil import BOState
+    return BOState(pressure=d[prefix + "p"].copy(), s=d[prefix + "s"].copy(), rs=d[prefix + "rs"].copy(),
+                   status=d[prefix + "status"].copy(), qWs=d[prefix + "qWs"].copy(), qOs=d[prefix + "qOs"].copy(),
+                   qGs=d[prefix + "qGs"].copy(), bhp=d[prefix + "bhp"].copy())

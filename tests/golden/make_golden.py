@@ -6,7 +6,9 @@ Run once, where the reference's Python package is importable:
 
 NAME selects fixture groups: small (the toy-grid fixtures), cfg0 (incomp_tpfa
 at 64x64x8), cfg1 (the first oil-water steps at 100x100x10), cfg4 (the
-adjoint at 64x64x4).  Without --only every group is written.
+adjoint at 64x64x4), bo (the three-phase black-oil model on a synthetic
+deck: residuals and Jacobians, and Newton histories).  Without --only every
+group is written.
 
 It writes small .npz files holding inputs and the reference's own outputs
 (grid arrays, transmissibilities, oil-water residuals and Jacobians, Newton
@@ -368,6 +370,152 @@ def cfg4_fixture(nsteps=30):
 
 
 
+def _bo_deck_arrays(deck):
+    """The deck's tables as flat arrays (pvto rows stacked with their key)."""
+    keys = np.array([k for k, _ in deck["pvto"]])
+    nrows = np.array([len(r) for _, r in deck["pvto"]])
+    rows = np.vstack([r for _, r in deck["pvto"]])
+    w, r = deck["pvtw"], deck["rock_cp"]
+    return dict(pvtw=np.array([w["p_ref"], w["b_ref"], w["c"], w["mu_ref"], w["viscosibility"]]),
+                rock_cp=np.array([r["p_ref"], r["c"]]), pvdg=deck["pvdg"], pvto_keys=keys,
+                pvto_nrows=nrows, pvto_rows=rows, swof=deck["swof"], sgof=deck["sgof"], rhoS=deck["rhoS"])
+
+
+def _bo_model(dims, phys, seed, wells_spec):
+    """The reference's ThreePhaseBlackOilModelAD on a box grid with the
+    synthetic deck; layered lognormal permeability."""
+    from pymrst.modules.ad_blackoil.models.three_phase_black_oil_model import ThreePhaseBlackOilModelAD
+    from pymrst.modules.ad_props.props.init_deck_adi_fluid import init_deck_blackoil_fluid
+    from pymrst_b200.cases import synthetic_blackoil_deck
+    deck = synthetic_blackoil_deck()
+    g = compute_geometry(cart_grid(dims, phys))
+    layer = np.array([500.0, 50.0, 200.0, 120.0])[np.arange(dims[2]) % 4]
+    perm = lognormal_perm(dims, seed, sigma=0.5, mean_md=1.0) * np.repeat(layer, dims[0] * dims[1])
+    rock = make_rock(g, perm[:, None], 0.3)
+    fluid = init_deck_blackoil_fluid(deck)
+    nx, ny = dims[0], dims[1]
+    wells = None
+    for (i, j, ks, wtype, val, compi) in wells_spec:
+        cells = np.array([i + nx * (j + ny * k) for k in ks])
+        wells = add_well(wells, g, rock, cells, well_type=wtype, val=val, radius=0.1,
+                         compi=np.asarray(compi, float), sign=1 if compi[2] > 0 or compi[0] > 0 else -1)
+    model = ThreePhaseBlackOilModelAD(g, rock, fluid, wells)
+    return deck, g, rock, perm, model
+
+
+def _bo_initial_state(model, g, p_top=300.0 * BARSA, sw=0.2, rs=120.0):
+    from pymrst.modules.ad_blackoil.models.three_phase_black_oil_model import BOState
+    nc, nw = g.cells.num, len(model.wells)
+    z = g.cells.centroids[:, 2]
+    p = p_top + 840.0 * 1.1 * 9.80665 * z
+    s = np.column_stack([np.full(nc, sw), np.full(nc, 1.0 - sw), np.zeros(nc)])
+    qws, qos, qgs, bhp = np.zeros(nw), np.zeros(nw), np.zeros(nw), np.zeros(nw)
+    for k, w in enumerate(model.wells):
+        if w.type == "orat":
+            qos[k], bhp[k] = w.val, p.mean() - 10 * BARSA
+        elif w.type == "rate":
+            qws[k], qgs[k], bhp[k] = w.val * w.compi[0], w.val * w.compi[2], p.mean() + 10 * BARSA
+        else:
+            bhp[k] = w.val
+    return BOState(pressure=p, s=s, rs=np.full(nc, rs), status=np.ones(nc, dtype=np.int64),
+                   qWs=qws, qOs=qos, qGs=qgs, bhp=bhp)
+
+
+def _bo_save_common(out, deck, dims, phys, perm, model):
+    out.update(_bo_deck_arrays(deck))
+    out.update(dims=np.array(dims), phys=np.array(phys), perm=perm, poro=np.array(0.3))
+    out.update(wells_arrays("w", model.wells))
+    return out
+
+
+def _bo_state_arrays(prefix, st):
+    return {prefix + "p": st.pressure, prefix + "s": st.s, prefix + "rs": st.rs, prefix + "status": st.status,
+            prefix + "qWs": st.qWs, prefix + "qOs": st.qOs, prefix + "qGs": st.qGs, prefix + "bhp": st.bhp}
+
+
+BO_WELLS = [(0, 0, (0, 1), "rate", 5.0, (0.0, 0.0, 1.0)),
+            (9, 9, (1, 2), "orat", -0.012, (0.0, 1.0, 0.0)),
+            (9, 0, (2,), "bhp", 250.0 * BARSA, (0.0, 1.0, 0.0))]
+
+
+def bo_assemble_fixture():
+    """Residual and Jacobian of the reference's assemble at an iterate with
+    saturated and undersaturated cells, a cross-flowing bhp well (its top
+    perforation injects, its bottom one produces) and every control type."""
+    from pymrst.modules.ad_blackoil.models.three_phase_black_oil_model import BOState
+    dims, phys = [6, 5, 4], [180.0, 150.0, 40.0]
+    spec = [(0, 0, (0, 1), "rate", 5.0, (0.0, 0.0, 1.0)),
+            (5, 4, (2, 3), "orat", -0.012, (0.0, 1.0, 0.0)),
+            (5, 0, (0, 1, 2, 3), "bhp", 0.0, (0.0, 1.0, 0.0))]
+    deck, g, rock, perm, model = _bo_model(dims, phys, 21, spec)
+    st0 = _bo_initial_state(model, g)
+    rng = np.random.default_rng(22)
+    nc = g.cells.num
+    xf = model.wells[2]
+    pw = st0.pressure[xf.cells]
+    xf.val = float(0.5 * (pw[1] + pw[2]))      # between the 2nd and 3rd perforation pressures
+    st0.bhp[2] = xf.val
+    st = st0.copy()
+    st.pressure = st.pressure + rng.uniform(-2, 2, nc) * BARSA
+    sat = rng.random(nc) < 0.4
+    st.status = np.where(sat, 3, 1).astype(np.int64)
+    sg = np.where(sat, rng.uniform(0.01, 0.2, nc), 0.0)
+    swv = st.s[:, 0] + rng.uniform(-0.03, 0.05, nc)
+    st.s = np.column_stack([swv, 1.0 - swv - sg, sg])
+    rs_sat = np.asarray(model.fluid.rs_sat(st.pressure))
+    st.rs = np.where(sat, rs_sat, 120.0 + rng.uniform(-20, 5, nc))
+    bub = ~sat & (rng.random(nc) < 0.4)           # undersaturated cells at their bubble point
+    st.rs[bub] = rs_sat[bub]
+    st.qWs = np.array([0.0, 0.0, 0.0])
+    st.qOs = np.array([0.0, -0.011, -0.004])
+    st.qGs = np.array([4.8, -0.9, -0.3])
+    st.bhp = np.array([st0.pressure.mean() + 12 * BARSA, st0.pressure.mean() - 9 * BARSA, xf.val])
+    out = _bo_save_common({}, deck, dims, phys, perm, model)
+    for tag, (a, b, dt) in {"a": (st0, st, 5 * DAY), "b": (st, st0, 2 * DAY)}.items():
+        x_val = np.where(b.status == 1, b.rs, b.s[:, 2])
+        ad = init_variables_adi(b.pressure, b.s[:, 0], x_val, b.qWs, b.qOs, b.qGs, b.bhp)
+        eqs = model.assemble(a, b, *ad, dt)
+        eq = combine_equations(*eqs)
+        jac = eq.jac[0].tocsr()
+        jac.sort_indices()
+        out.update(_bo_state_arrays(tag + "0_", a))
+        out.update(_bo_state_arrays(tag + "_", b))
+        out[tag + "_dt"] = np.array(dt)
+        out[tag + "_res"] = np.asarray(eq.val)
+        out[tag + "_jac_data"], out[tag + "_jac_indices"], out[tag + "_jac_indptr"] = jac.data, jac.indices, jac.indptr
+        out[tag + "_converged"] = np.array(model._converged(eqs, dt, b))
+        upd = np.linspace(-1.0, 1.0, jac.shape[0]) * np.concatenate(
+            [np.full(nc, 3 * BARSA), np.full(nc, 0.05), np.where(b.status == 1, 5.0, 0.04),
+             np.full(4 * len(model.wells), 0.01)])
+        new = model.update_state(b, upd)
+        out[tag + "_upd"] = upd
+        out.update(_bo_state_arrays(tag + "_new_", new))
+    save("bo_assemble.npz", **out)
+
+
+def bo_newton_fixture(nsteps_days=(0.5, 1.0, 2.0, 5.0, 10.0, 10.0, 20.0)):
+    """Newton histories of the reference's step on a 10x10x3 box with a gas
+    injector (rate), an oil-rate producer (orat) and a bhp producer."""
+    dims, phys = [10, 10, 3], [300.0, 300.0, 30.0]
+    deck, g, rock, perm, model = _bo_model(dims, phys, 23, BO_WELLS)
+    st = _bo_initial_state(model, g)
+    out = _bo_save_common({}, deck, dims, phys, perm, model)
+    out.update(_bo_state_arrays("init_", st))
+    its, hist = [], []
+    for dt in np.asarray(nsteps_days) * DAY:
+        st, ok, it = model.step(st, float(dt))
+        assert ok, "reference step did not converge"
+        its.append(it)
+        hist.append(st.copy())
+    out["dts"] = np.asarray(nsteps_days) * DAY
+    out["its"] = np.array(its)
+    for name in ("pressure", "rs", "qWs", "qOs", "qGs", "bhp"):
+        out["hist_" + name] = np.array([getattr(h, name) for h in hist])
+    out["hist_s"] = np.array([h.s for h in hist])
+    out["hist_status"] = np.array([h.status for h in hist])
+    save("bo_newton.npz", **out)
+
+
 if __name__ == "__main__":
     def want(name):
         return ONLY is None or name in ONLY
@@ -389,3 +537,6 @@ if __name__ == "__main__":
         cfg4_fixture()
     if want("cfg1"):
         cfg1_fixture()
+    if want("bo"):
+        bo_assemble_fixture()
+        bo_newton_fixture()

@@ -164,9 +164,9 @@ def test_device_csr_jacobian_equals_the_exported_one(transpose):
     d, m, st, st0, x, x0, jac, well = _xflow_model_and_jacobian()
     rp, ci, ptr, terms = jacobian_terms(m, transpose=transpose)
     vals = torch.empty(ci.size, dtype=torch.float64, device="cuda")
-    N.check(N.lib().pmb_ow_csr_values(m._handle, N.ptr(jac), N.ptr(well), ci.size,
-                                      N.ptr(torch.as_tensor(ptr, device="cuda")),
-                                      N.ptr(torch.as_tensor(terms, device="cuda")), N.ptr(vals)))
+    d_ptr, d_terms = torch.as_tensor(ptr, device="cuda"), torch.as_tensor(terms, device="cuda")
+    N.check(N.lib().pmb_ow_csr_values(m._handle, N.ptr(jac), N.ptr(well), ci.size, N.ptr(d_ptr), N.ptr(d_terms),
+                                      N.ptr(vals)))
     n = rp.size - 1
     A = sp.csr_array((vals.cpu().numpy(), ci, rp), shape=(n, n))
     J = m.export_jacobian(jac.cpu().numpy(), well.cpu().numpy())
@@ -186,7 +186,8 @@ def test_previous_step_coupling_equals_the_oracle():
     lam = np.random.default_rng(3).normal(size=2 * m.nc + 3 * m.nw)
     y = torch.empty(lam.size, dtype=torch.float64, device="cuda")
     dt = float(d["dt"])
-    N.check(N.lib().pmb_ow_prev_jacobian_tmul(m._handle, N.ptr(x0), dt, N.ptr(torch.as_tensor(lam, device="cuda")),
+    d_lam = torch.as_tensor(lam, device="cuda")
+    N.check(N.lib().pmb_ow_prev_jacobian_tmul(m._handle, N.ptr(x0), dt, N.ptr(d_lam),
                                               N.ptr(y)))
     st0o = oow.State(pressure=d["p0"].copy(), sW=d["sw0"].copy(), qWs=d["qws0"].copy(), qOs=d["qos0"].copy(),
                      bhp=d["bhp0"].copy())

@@ -81,8 +81,8 @@ def test_assembly_is_bit_reproducible_and_spmv_matches_the_exported_matrix():
     v = rng.standard_normal(m.sizes["nvec"])
     y = torch.empty_like(x)
     from pymrst_b200 import _native as N
-    N.check(N.lib().pmb_ow_spmv(m._handle, N.ptr(j1), N.ptr(w1), N.ptr(torch.as_tensor(v, device="cuda")),
-                                N.ptr(y)))
+    dv = torch.as_tensor(v, device="cuda")
+    N.check(N.lib().pmb_ow_spmv(m._handle, N.ptr(j1), N.ptr(w1), N.ptr(dv), N.ptr(y)))
     # export is in the reference layout: permute v and y
     vref = m.export_residual(v)
     yref = J @ vref
