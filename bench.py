@@ -26,6 +26,7 @@ import subprocess
 import sys
 import threading
 import time
+from pathlib import Path
 
 import numpy as np
 
@@ -434,6 +435,76 @@ def measure_adjoint(torch, GpuOilWaterModel, cpu_steps=3):
             "cpu": f"oracle forward + adjoint (numpy, SuperLU) over the first {cpu_steps} steps, one core"}
 
 
+def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budget=30.0):
+    """The three-phase black-oil model with dissolved gas (the seeded
+    lattice case of cases.blackoil_box: gas injectors, bhp producers, one
+    oil-rate producer) over its seven steps (0.5 to 20 days), the whole
+    schedule CUDA-event timed after a warm-up run on a copy of the state.
+    CPU: the reference's own ThreePhaseBlackOilModelAD (its installed
+    package, SuperLU) on the same generator at cpu_dims, steps until the
+    budget is spent, one core."""
+    from pymrst_b200 import cases
+    from pymrst_b200.blackoil import GpuBlackOilModel
+    case = cases.blackoil_box(dims=dims)
+    model = GpuBlackOilModel(case.grid, case.rock, case.deck, case.wells)
+    x0 = model.to_device(case.state)
+    warm = x0.clone()
+    for dt in case.dts[:2]:
+        model.step_device(warm, float(dt))
+    x = x0.clone()
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    its, krylov, failed = 0, 0, 0
+    e0.record()
+    for dt in case.dts:
+        ok, nit, st = model.step_device(x, float(dt))
+        its += nit
+        krylov += int(st[2])
+        failed += 0 if ok else 1
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) * 1e-3
+    out = {"workload": f"black-oil (live oil, dry gas, switching) {dims[0]}x{dims[1]}x{dims[2]} "
+                       f"({model.nc:,} cells, {model.nw} wells), steps of 0.5 to 20 days, FP64",
+           "value": model.nc * its / sec, "unit": UNIT, "ms_per_step": sec / len(case.dts) * 1e3,
+           "newton_iterations": its, "krylov_iterations": krylov, "failed_steps": failed,
+           "saturated_cells_at_end": int((model.from_device(x).status == 3).sum())}
+    ref = Path(__file__).resolve().parent / "baseline" / "_ref"
+    if not (ref / "pymrst").is_dir():
+        out["cpu"] = "the reference package is not installed under baseline/_ref"
+        return out
+    sys.path.insert(0, str(ref))
+    from pymrst.gridprocessing import cart_grid, compute_geometry
+    from pymrst.modules.ad_blackoil.models.three_phase_black_oil_model import BOState, ThreePhaseBlackOilModelAD
+    from pymrst.modules.ad_props.props.init_deck_adi_fluid import init_deck_blackoil_fluid
+    from pymrst.params import add_well, make_rock
+    small = cases.blackoil_box(dims=cpu_dims)
+    g = compute_geometry(cart_grid(list(cpu_dims), [d * 30.0 if i < 2 else d * 10.0 for i, d in enumerate(cpu_dims)]))
+    rock = make_rock(g, np.asarray(small.rock.perm)[:, :1], 0.3)
+    wells = None
+    for w in small.wells:
+        wells = add_well(wells, g, rock, w.cells, well_type=w.type, val=w.val, radius=0.1, compi=w.compi)
+    rmodel = ThreePhaseBlackOilModelAD(g, rock, init_deck_blackoil_fluid(small.deck), wells)
+    s0 = small.state
+    st = BOState(pressure=s0.pressure.copy(), s=s0.s.copy(), rs=s0.rs.copy(), status=s0.status.copy(),
+                 qWs=s0.qWs.copy(), qOs=s0.qOs.copy(), qGs=s0.qGs.copy(), bhp=s0.bhp.copy())
+    t0 = time.perf_counter()
+    cits, nsteps = 0, 0
+    for dt in small.dts:
+        st, ok, it = rmodel.step(st, float(dt))
+        cits += it
+        nsteps += 1
+        if time.perf_counter() - t0 >= cpu_budget:
+            break
+    csec = time.perf_counter() - t0
+    out.update(cpu_value=g.cells.num * cits / csec,
+               cpu=f"the reference's ThreePhaseBlackOilModelAD (installed package, SuperLU) on the same generator "
+                   f"at {cpu_dims[0]}x{cpu_dims[1]}x{cpu_dims[2]} ({g.cells.num} cells): {nsteps} step(s), {cits} "
+                   f"Newton iterations in {csec:.1f} s, one core")
+    out["speedup"] = out["value"] / out["cpu_value"]
+    return out
+
+
 def run_ensemble_workload(args):
     """Config 3 (`--workload ensemble`): the seeded realisations (nx, ny in
     16..64, nz in 2..8, an independent lognormal permeability and a five-spot
@@ -694,7 +765,8 @@ def run_ours(args):
         for name, fn in (("incomp_64x64x8", lambda: measure_incomp(torch)),
                          ("ow_fp64_100x100x10", lambda: measure_ow_fp64(torch, N, GpuOilWaterModel, run_report_step,
                                                                         args.cpu_budget)),
-                         ("adjoint_64x64x4", lambda: measure_adjoint(torch, GpuOilWaterModel))):
+                         ("adjoint_64x64x4", lambda: measure_adjoint(torch, GpuOilWaterModel)),
+                         ("blackoil_100x100x10", lambda: measure_blackoil(torch))):
             try:
                 configs[name] = fn()
             except Exception as e:  # a secondary measurement must not hide the headline line

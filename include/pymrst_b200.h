@@ -282,7 +282,10 @@ int pmb_ow_step_members(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t m
  * (pymrst/modules/ad_core/solvers/linear_solvers.py:426-545).
  * The n x n matrix is in the reference's variable-blocked ordering: nph
  * blocks of nc cell unknowns (pressure first), then n - nph*nc facility
- * unknowns (at most 4096).  h_row_ptr / h_col: canonical CSR (columns
+ * unknowns.  The second stage inverts the facility block group by group, a
+ * group being a connected component of the facility block's own pattern
+ * (one well's unknowns where wells do not couple), of at most 4096
+ * unknowns each.  h_row_ptr / h_col: canonical CSR (columns
  * strictly increasing in a row), fixed for the handle's life; values are
  * given per setup.  opts as for pmb_cpr_create; local_sweeps counts
  * block-Jacobi sweeps of the second stage (1 = the reference's single

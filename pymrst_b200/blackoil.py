@@ -243,7 +243,7 @@ class GpuBlackOilModel:
         self.pv_ref = pore_volume(g, rock)
         self.nc = int(g.cells.num)
         self.nw = len(self.wells)
-        self.cpr_options = default_cpr_options(**({"rtol": 1e-10, "maxiter": 400, "amg_rebuild_interval": 1}
+        self.cpr_options = default_cpr_options(**({"rtol": 1e-10, "maxiter": 400}
                                                   | dict(cpr_options or {})))
         self._stream = torch.cuda.current_stream()
         self._build()

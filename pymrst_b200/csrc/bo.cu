@@ -965,7 +965,6 @@ BOModel::BOModel(const pmb_bo_desc& d, cudaStream_t s) : s_(s) {
   PMB_REQUIRE(d.nc > 0 && d.nf >= 0 && d.nw >= 0, "bo: sizes must be nc > 0, nf >= 0, nw >= 0");
   PMB_REQUIRE(d.h_N && d.h_T && d.h_gdz && d.h_pv, "bo: grid arrays must not be NULL");
   const int nc = d.nc, nf = d.nf, nw = d.nw;
-  PMB_REQUIRE(4LL * nw <= 4096, "bo: at most 1024 wells");
   // ---- fluid tables into one device buffer
   std::vector<double> tab;
   auto put = [&](const double* p, int n, const char* what) -> int64_t {

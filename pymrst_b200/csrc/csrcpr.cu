@@ -11,8 +11,10 @@
 // :155-190), P the injection of the first nc columns (pressure), solve_p an
 // aggregation-AMG cycle on A_p = W A P (:471-473), and local() the
 // block-Jacobi stage (:316-363): each cell's nph x nph block inverted, the
-// facility block inverted as a whole (regularised by sqrt(eps) where it is
-// exactly singular, as the reference does after equilibration, :345-357).
+// facility block inverted group by group, a group being a connected component
+// of the facility block's own pattern (a well's unknowns, where wells do not
+// couple one another), each regularised by sqrt(eps) where it is exactly
+// singular, as the reference does after equilibration, :345-357).
 // In transposed mode the caller passes A' = J^T (the adjoint system,
 // optimization/adjoint.py:209) and the transfer operators are the
 // transposes of the forward ones: restriction P^T (the pressure rows of r),
@@ -24,7 +26,9 @@
 // row scaling of A_p.
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <memory>
+#include <numeric>
 #include <type_traits>
 #include <vector>
 
@@ -105,35 +109,44 @@ __global__ void csr_block_inv_kernel(int nc, int nph, const int* __restrict__ bl
     for (int j = 0; j < nph; ++j) inv[(long long)c * m2 + i * nph + j] = ok ? I[i][j] : 0.0;
 }
 
-// Facility block, dense: scatter, then scale each row to unit max norm
-// (rs[r] = 1 / max|row|).  One CTA.
-__global__ void csr_tail_assemble_kernel(int nt, int cnt, const int* __restrict__ pos, const int* __restrict__ rc,
-                                         const double* __restrict__ a, double* __restrict__ M,
-                                         double* __restrict__ rs) {
-  for (int e = threadIdx.x; e < nt * nt; e += blockDim.x) M[e] = 0.0;
-  __syncthreads();
-  for (int e = threadIdx.x; e < cnt; e += blockDim.x) M[rc[e]] = a[pos[e]];
-  __syncthreads();
-  for (int r = threadIdx.x; r < nt; r += blockDim.x) {
-    double m = 0.0;
-    for (int j = 0; j < nt; ++j) m = fmax(m, fabs(M[(long long)r * nt + j]));
-    const double s = m > 0.0 && isfinite(m) ? 1.0 / m : 1.0;
-    rs[r] = s;
-    for (int j = 0; j < nt; ++j) M[(long long)r * nt + j] *= s;
-  }
+// Facility block.  Its unknowns fall into independent groups (the connected
+// components of its own pattern: one group per well when wells do not couple
+// one another); group g has m_g unknowns, listed ascending at
+// gmem[gptr[g] ..), and a dense m_g x m_g block at goff[g] in tM / tInv.
+__global__ void csr_tail_zero_kernel(long long n, double* __restrict__ M) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+    M[e] = 0.0;
 }
 
-// Gauss-Jordan inverse of the row-scaled facility block in one CTA; an exactly
-// zero pivot column is replaced by sqrt(eps) on the diagonal.  Finally
+__global__ void csr_tail_scatter_kernel(int cnt, const int* __restrict__ pos, const long long* __restrict__ dst,
+                                        const double* __restrict__ a, double* __restrict__ M) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) M[dst[e]] = a[pos[e]];
+}
+
+// One CTA per group: scale each row of the group's block to unit max norm
+// (rs = 1 / max|row|), Gauss-Jordan inverse with row pivoting, an exactly
+// zero pivot column replaced by sqrt(eps) on the diagonal, and finally
 // Inv <- Inv diag(rs), the inverse of the unscaled block.
-__global__ void __launch_bounds__(256) csr_tail_invert_kernel(int nt, double* __restrict__ M,
-                                                              double* __restrict__ Inv,
-                                                              const double* __restrict__ rs,
-                                                              int* __restrict__ status) {
+__global__ void __launch_bounds__(128) csr_tail_invert_kernel(const int* __restrict__ gptr,
+                                                              const long long* __restrict__ goff,
+                                                              double* __restrict__ Mall, double* __restrict__ Invall,
+                                                              double* __restrict__ rsall, int* __restrict__ status) {
   __shared__ int piv;
   __shared__ double pval;
+  const int g = blockIdx.x;
+  const int nt = gptr[g + 1] - gptr[g];
+  double* M = Mall + goff[g];
+  double* Inv = Invall + goff[g];
+  double* rs = rsall + gptr[g];
   const int t = threadIdx.x, nthr = blockDim.x;
   const double shift = 1.4901161193847656e-08;  // sqrt(2^-52)
+  for (int r = t; r < nt; r += nthr) {
+    double m = 0.0;
+    for (int j = 0; j < nt; ++j) m = fmax(m, fabs(M[(long long)r * nt + j]));
+    const double sc = m > 0.0 && isfinite(m) ? 1.0 / m : 1.0;
+    rs[r] = sc;
+    for (int j = 0; j < nt; ++j) M[(long long)r * nt + j] *= sc;
+  }
   for (int idx = t; idx < nt * nt; idx += nthr) Inv[idx] = (idx / nt == idx % nt) ? 1.0 : 0.0;
   __syncthreads();
   for (int c = 0; c < nt; ++c) {
@@ -242,33 +255,36 @@ __global__ void __launch_bounds__(256) csr_local_cells_kernel(int nc, int nph, c
   }
 }
 
-// Facility rows of the second stage (one CTA): t = r - A x over the nt rows,
-// z = Inv t (x is zero there).
+// Facility rows of the second stage, one CTA per facility group: t = r - A x
+// over the group's rows, z = Inv_g t (x is zero there).
 template <bool TR, class T>
-__global__ void __launch_bounds__(256) csr_local_tail_kernel(int nc, int nph, int nt, const int* __restrict__ rp,
+__global__ void __launch_bounds__(128) csr_local_tail_kernel(int nc, int nph, const int* __restrict__ gptr,
+                                                             const int* __restrict__ gmem,
+                                                             const long long* __restrict__ goff,
+                                                             const int* __restrict__ rp,
                                                              const int* __restrict__ ci,
                                                              const double* __restrict__ a,
                                                              const double* __restrict__ r,
                                                              const T* __restrict__ xp,
                                                              const double* __restrict__ pw,
-                                                             const double* __restrict__ Inv,
+                                                             const double* __restrict__ Invall,
                                                              double* __restrict__ z) {
   extern __shared__ double ts[];
   const int base = nph * nc;
-  for (int q = threadIdx.x; q < nt; q += blockDim.x) {
-    const int row = base + q;
+  const int g = blockIdx.x, g0 = gptr[g], m = gptr[g + 1] - g0;
+  const double* Inv = Invall + goff[g];
+  for (int q = threadIdx.x; q < m; q += blockDim.x) {
+    const int row = base + gmem[g0 + q];
     double s = r[row];
     if (xp)
       for (int k = rp[row]; k < rp[row + 1]; ++k) s -= a[k] * prolonged<TR>(ci[k], nc, nph, xp, pw);
     ts[q] = s;
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  for (int q = warp; q < nt; q += nwarp) {
+  for (int q = threadIdx.x; q < m; q += blockDim.x) {
     double s = 0.0;
-    for (int j = lane; j < nt; j += 32) s += Inv[(long long)q * nt + j] * ts[j];
-    s = warp_sum(s);
-    if (lane == 0) z[base + q] = s;
+    for (int j = 0; j < m; ++j) s += Inv[(long long)q * m + j] * ts[j];
+    z[base + gmem[g0 + q]] = s;
   }
 }
 
@@ -292,19 +308,25 @@ __global__ void __launch_bounds__(256) csr_jacobi_cells_kernel(int nc, int nph, 
   }
 }
 
-__global__ void __launch_bounds__(256) csr_jacobi_tail_kernel(int base, int nt, const double* __restrict__ r,
+__global__ void __launch_bounds__(128) csr_jacobi_tail_kernel(int base, const int* __restrict__ gptr,
+                                                              const int* __restrict__ gmem,
+                                                              const long long* __restrict__ goff,
+                                                              const double* __restrict__ r,
                                                               const double* __restrict__ y,
-                                                              const double* __restrict__ Inv,
+                                                              const double* __restrict__ Invall,
                                                               double* __restrict__ z) {
   extern __shared__ double ts[];
-  for (int q = threadIdx.x; q < nt; q += blockDim.x) ts[q] = r[base + q] - y[base + q];
+  const int g = blockIdx.x, g0 = gptr[g], m = gptr[g + 1] - g0;
+  const double* Inv = Invall + goff[g];
+  for (int q = threadIdx.x; q < m; q += blockDim.x) {
+    const int row = base + gmem[g0 + q];
+    ts[q] = r[row] - y[row];
+  }
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  for (int q = warp; q < nt; q += nwarp) {
+  for (int q = threadIdx.x; q < m; q += blockDim.x) {
     double s = 0.0;
-    for (int j = lane; j < nt; j += 32) s += Inv[(long long)q * nt + j] * ts[j];
-    s = warp_sum(s);
-    if (lane == 0) z[base + q] += s;
+    for (int j = 0; j < m; ++j) s += Inv[(long long)q * m + j] * ts[j];
+    z[base + gmem[g0 + q]] += s;
   }
 }
 
@@ -344,8 +366,10 @@ class CsrCPR {
   int since_build_ = 0;
   std::vector<double> h_ap_;
   // local stage
-  DArray<int> blk_pos_, tail_pos_, tail_rc_;
-  int tail_cnt_ = 0;
+  DArray<int> blk_pos_, tail_pos_, tg_ptr_, tg_mem_;
+  DArray<long long> tail_dst_, tg_off_;
+  int tail_cnt_ = 0, ngroups_ = 0, max_group_ = 0;
+  long long tail_dense_ = 0;
   DArray<double> inv_, tM_, tInv_, trs_, ytmp_;
   DArray<int> status_;
   PinnedArray<int> st_pin_;
@@ -362,7 +386,6 @@ CsrCPR::CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, bool t
   PMB_REQUIRE(nph >= 1 && nph <= kMaxPhases, "nph must be 1, 2 or 3");
   PMB_REQUIRE(nc >= 1 && (long long)nph * nc <= n, "need 1 <= nc and nph * nc <= n");
   nt_ = n - nph * nc;
-  PMB_REQUIRE(nt_ <= kMaxTail, "at most 4096 facility unknowns");
   PMB_REQUIRE(o_.restart >= 1 && o_.restart <= kMaxRestart, "restart must be in 1..60");
   PMB_REQUIRE(o_.maxiter >= 1, "maxiter must be positive");
   PMB_REQUIRE(o_.rtol > 0.0, "rtol must be positive");
@@ -421,15 +444,52 @@ CsrCPR::CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, bool t
   for (int c = 0; c < nc; ++c)
     for (int i = 0; i < nph; ++i)
       for (int j = 0; j < nph; ++j) blk[(size_t)c * nph * nph + i * nph + j] = find(i * nc + c, j * nc + c);
-  std::vector<int> tp, trc;
+  // facility groups: connected components of the facility-facility pattern
+  std::vector<int> tp, tgp(1, 0), tgm;
+  std::vector<long long> tdst, tgo(1, 0);
   if (nt_ > 0) {
     const int base = nph * nc;
+    std::vector<int> parent(nt_);
+    std::iota(parent.begin(), parent.end(), 0);
+    std::function<int(int)> root = [&](int q) {
+      while (parent[q] != q) q = parent[q] = parent[parent[q]];
+      return q;
+    };
     for (int q = 0; q < nt_; ++q)
       for (int k = h_rp[base + q]; k < h_rp[base + q + 1]; ++k)
         if (h_col[k] >= base) {
-          tp.push_back(k);
-          trc.push_back(q * nt_ + (h_col[k] - base));
+          const int a = root(q), b = root(h_col[k] - base);
+          if (a != b) parent[std::max(a, b)] = std::min(a, b);
         }
+    std::vector<int> gid(nt_, -1), lid(nt_), gsize;
+    std::vector<int> rid(nt_, -1);
+    for (int q = 0; q < nt_; ++q) {
+      const int r0 = root(q);
+      if (rid[r0] < 0) {
+        rid[r0] = (int)gsize.size();
+        gsize.push_back(0);
+      }
+      gid[q] = rid[r0];
+      lid[q] = gsize[gid[q]]++;
+    }
+    ngroups_ = (int)gsize.size();
+    std::vector<int> fill(ngroups_, 0);
+    for (int g = 0; g < ngroups_; ++g) {
+      tgp.push_back(tgp.back() + gsize[g]);
+      tgo.push_back(tgo.back() + (long long)gsize[g] * gsize[g]);
+      max_group_ = std::max(max_group_, gsize[g]);
+    }
+    tgm.assign(nt_, 0);
+    for (int q = 0; q < nt_; ++q) tgm[tgp[gid[q]] + fill[gid[q]]++] = q;  // ascending within a group
+    for (int q = 0; q < nt_; ++q)
+      for (int k = h_rp[base + q]; k < h_rp[base + q + 1]; ++k)
+        if (h_col[k] >= base) {
+          const int j = h_col[k] - base, g = gid[q];
+          tp.push_back(k);
+          tdst.push_back(tgo[g] + (long long)lid[q] * gsize[g] + lid[j]);
+        }
+    tail_dense_ = tgo.back();
+    PMB_REQUIRE(max_group_ <= kMaxTail, "at most 4096 coupled facility unknowns in one group");
   }
   // device arrays (everything above is host-only validation and analysis)
   rp_.upload(h_rp, n + 1, s_);
@@ -445,9 +505,12 @@ CsrCPR::CsrCPR(int n, int nc, int nph, const int* h_rp, const int* h_col, bool t
   if (nt_ > 0) {
     tail_cnt_ = (int)tp.size();
     tail_pos_.upload(tp.empty() ? std::vector<int>{0} : tp, s_);
-    tail_rc_.upload(trc.empty() ? std::vector<int>{0} : trc, s_);
-    tM_.resize((size_t)nt_ * nt_);
-    tInv_.resize((size_t)nt_ * nt_);
+    tail_dst_.upload(tdst.empty() ? std::vector<long long>{0} : tdst, s_);
+    tg_ptr_.upload(tgp, s_);
+    tg_mem_.upload(tgm, s_);
+    tg_off_.upload(tgo, s_);
+    tM_.resize((size_t)tail_dense_);
+    tInv_.resize((size_t)tail_dense_);
     trs_.resize(nt_);
   }
   w_.resize(nph);
@@ -498,10 +561,16 @@ void CsrCPR::setup(const double* d_val, const double* h_w) {
                                                             status_.get());
   PMB_CHECK_LAUNCH();
   if (nt_ > 0) {
-    csr_tail_assemble_kernel<<<1, 256, 0, s_>>>(nt_, tail_cnt_, tail_pos_.get(), tail_rc_.get(), val_, tM_.get(),
-                                                trs_.get());
+    const int zb = (int)std::min<long long>(2LL * kNumSM, (tail_dense_ + 255) / 256);
+    csr_tail_zero_kernel<<<std::max(zb, 1), 256, 0, s_>>>(tail_dense_, tM_.get());
     PMB_CHECK_LAUNCH();
-    csr_tail_invert_kernel<<<1, 256, 0, s_>>>(nt_, tM_.get(), tInv_.get(), trs_.get(), status_.get());
+    if (tail_cnt_ > 0) {
+      csr_tail_scatter_kernel<<<std::min(2 * kNumSM, (tail_cnt_ + 255) / 256), 256, 0, s_>>>(
+          tail_cnt_, tail_pos_.get(), tail_dst_.get(), val_, tM_.get());
+      PMB_CHECK_LAUNCH();
+    }
+    csr_tail_invert_kernel<<<ngroups_, 128, 0, s_>>>(tg_ptr_.get(), tg_off_.get(), tM_.get(), tInv_.get(),
+                                                     trs_.get(), status_.get());
     PMB_CHECK_LAUNCH();
   }
   if (o_.use_pressure_stage) {
@@ -560,8 +629,9 @@ void CsrCPR::precond_body(const double* r, double* z) {
                                                                         xp, pw_.get(), inv_.get(), z);
       PMB_CHECK_LAUNCH();
       if (nt_ > 0) {
-        csr_local_tail_kernel<TR, T><<<1, 256, sizeof(double) * nt_, s_>>>(nc_, nph_, nt_, rp_.get(), col_.get(),
-                                                                           val_, r, xp, pw_.get(), tInv_.get(), z);
+        csr_local_tail_kernel<TR, T><<<ngroups_, 128, sizeof(double) * max_group_, s_>>>(
+            nc_, nph_, tg_ptr_.get(), tg_mem_.get(), tg_off_.get(), rp_.get(), col_.get(), val_, r, xp, pw_.get(),
+            tInv_.get(), z);
         PMB_CHECK_LAUNCH();
       }
     };
@@ -593,7 +663,8 @@ void CsrCPR::precond_body(const double* r, double* z) {
     csr_jacobi_cells_kernel<<<grid_for(nc_, 256), 256, 0, s_>>>(nc_, nph_, r, ytmp_.get(), inv_.get(), z);
     PMB_CHECK_LAUNCH();
     if (nt_ > 0) {
-      csr_jacobi_tail_kernel<<<1, 256, sizeof(double) * nt_, s_>>>(nph_ * nc_, nt_, r, ytmp_.get(), tInv_.get(), z);
+      csr_jacobi_tail_kernel<<<ngroups_, 128, sizeof(double) * max_group_, s_>>>(
+          nph_ * nc_, tg_ptr_.get(), tg_mem_.get(), tg_off_.get(), r, ytmp_.get(), tInv_.get(), z);
       PMB_CHECK_LAUNCH();
     }
   }

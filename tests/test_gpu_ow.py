@@ -174,3 +174,23 @@ def test_nonfinite_state_fails_the_step_without_a_device_fault():
     # the handle is still usable afterwards
     new, ok, its = m.step(m.initial_state(case.p0, case.sw0), case.dt)
     assert ok
+
+
+def test_config1_first_step_matches_reference_at_100x100x10():
+    """Benchmark config 1 at its own size: the 100,000-cell five-spot with
+    gravity, the first 10-day report step under the schedule driver (with
+    the reference's timestep cuts), against the reference's own
+    simulate_schedule_ad with its direct solver (cfg1_ow_100x100x10.npz):
+    the same Newton iteration count, p <= 1e-8 relative and sW <= 1e-7."""
+    d = load("cfg1_ow_100x100x10.npz")
+    c = cases.five_spot(dims=(100, 100, 10), seed=1)
+    assert np.isclose(np.sum(c.rock.perm), float(d["perm_sum"]), rtol=1e-14)
+    assert np.isclose(sum(np.sum(w.WI) for w in c.wells), float(d["wi_sum"]), rtol=1e-12)
+    m = GpuOilWaterModel(c.grid, c.rock, c.fluid, c.wells, gravity=c.gravity,
+                         cpr_options=dict(rtol=1e-12, maxiter=600, amg_rebuild_interval=1_000_000))
+    states, its = simulate_schedule_ad(m.initial_state(c.p0, c.sw0), m, [c.dt], verbose=False)
+    assert list(its) == list(d["its"])
+    p_ref = d["p_hist"][0]
+    assert np.abs(states[0].pressure - p_ref).max() <= 1e-8 * np.abs(p_ref).max()
+    assert np.abs(states[0].sW - d["sw_hist"][0]).max() <= 1e-7
+    assert np.abs(states[0].bhp - d["bhp_hist"][0]).max() <= 1e-8 * np.abs(d["bhp_hist"][0]).max()
