@@ -6,7 +6,7 @@ Run once, where the reference's Python package is importable:
 
 NAME selects fixture groups: small (the toy-grid fixtures), cfg0 (incomp_tpfa
 at 64x64x8), cfg1 (the first oil-water steps at 100x100x10), cfg4 (the
-adjoint at 64x64x4), bo (the three-phase black-oil model on a synthetic
+adjoint at 64x64x4), transport (the phase-3 transport cases), bo (the three-phase black-oil model on a synthetic
 deck: residuals and Jacobians, and Newton histories).  Without --only every
 group is written.
 
@@ -516,6 +516,63 @@ def bo_newton_fixture(nsteps_days=(0.5, 1.0, 2.0, 5.0, 10.0, 10.0, 20.0)):
     save("bo_newton.npz", **out)
 
 
+def transport_fixture():
+    """validate_phase3.py's three cases (Buckley-Leverett 100x1x1 with fixed
+    and computed explicit substeps and implicit transport; two sequential
+    incomp_tpfa + implicit cycles on a 32x32 quarter five-spot; gravity
+    segregation in a 20-cell column) run by the reference, with the MATLAB
+    arrays (ref_p3_bl.mat, ref_p3_qfs.mat, ref_p3_gravity.mat)."""
+    from pymrst.modules.incomp import explicit_transport, implicit_transport, incomp_tpfa_ad, init_simple_fluid
+    from pymrst.params import add_source, gravity_vector, pore_volume
+    from pymrst.solvers import init_res_sol
+    fluid = init_simple_fluid(mu=np.array([1.0, 10.0]) * CENTI * POISE, rho=[1000.0, 700.0], n=[2.0, 2.0])
+    out = {}
+    # Buckley-Leverett
+    mb = scipy.io.loadmat(REF / "examples/validation/ref_p3_bl.mat", squeeze_me=True)
+    g = compute_geometry(cart_grid([100, 1, 1], [100.0, 1.0, 1.0]))
+    rock = make_rock(g, 100 * MILLI * DARCY, 0.2)
+    ht = compute_trans(g, rock)
+    rate = float(pore_volume(g, rock).sum()) / (100 * DAY)
+    src = add_source(None, np.array([0]), rate, sat=np.array([[1.0, 0.0]]))
+    src = add_source(src, np.array([99]), -rate, sat=np.array([[0.0, 1.0]]))
+    new = lambda: incomp_tpfa_ad(init_res_sol(g, 0.0, s0=np.array([[0.0, 1.0]])), g, ht, fluid, src=src)
+    st = new()
+    out.update(bl_rate=np.array(rate), bl_p0=st.pressure, bl_flux0=st.flux)
+    out["bl_sE"] = explicit_transport(new(), g, 30 * DAY, rock, fluid, src=src, dt=0.25 * DAY).s[:, 0]
+    out["bl_sE_auto"] = explicit_transport(new(), g, 30 * DAY, rock, fluid, src=src).s[:, 0]
+    out["bl_sI"] = implicit_transport(new(), g, 30 * DAY, rock, fluid, src=src).s[:, 0]
+    for k in ("p0", "flux0", "sE", "sI"):
+        out["bl_mat_" + k] = np.asarray(mb[k], float).ravel()
+    # quarter five-spot, two sequential cycles
+    mq = scipy.io.loadmat(REF / "examples/validation/ref_p3_qfs.mat", squeeze_me=True)
+    g = compute_geometry(cart_grid([32, 32, 1], [500.0, 500.0, 10.0]))
+    kvals = (10 + (7 * np.arange(g.cells.num)) % 100) * MILLI * DARCY
+    rock = make_rock(g, kvals[:, None], 0.2)
+    ht = compute_trans(g, rock)
+    src = add_source(None, np.array([0]), 5e-3, sat=np.array([[1.0, 0.0]]))
+    src = add_source(src, np.array([g.cells.num - 1]), -5e-3, sat=np.array([[0.0, 1.0]]))
+    st = init_res_sol(g, 0.0, s0=np.array([[0.0, 1.0]]))
+    for _ in range(2):
+        st = incomp_tpfa_ad(st, g, ht, fluid, src=src)
+        st = implicit_transport(st, g, 100 * DAY, rock, fluid, src=src)
+    out.update(qfs_sQ=st.s[:, 0], qfs_pQ=st.pressure, qfs_mat_sQ=np.asarray(mq["sQ"], float).ravel(),
+               qfs_mat_pQ=np.asarray(mq["pQ"], float).ravel())
+    # gravity segregation, implicit (the MATLAB case) and explicit with computed substeps
+    mg = scipy.io.loadmat(REF / "examples/validation/ref_p3_gravity.mat", squeeze_me=True)
+    g = compute_geometry(cart_grid([1, 1, 20], [1.0, 1.0, 20.0]))
+    rock = make_rock(g, 1000 * MILLI * DARCY, 0.3)
+    gfluid = init_simple_fluid(mu=[1e-3, 1e-3], rho=[1000.0, 700.0], n=[2.0, 2.0])
+
+    def col():
+        s0 = init_res_sol(g, 0.0, s0=np.array([[0.5, 0.5]]))
+        s0.flux = np.zeros(g.faces.num)
+        return s0
+    out["grav_sG"] = implicit_transport(col(), g, 50 * DAY, rock, gfluid, gravity=gravity_vector(3)).s[:, 0]
+    out["grav_sE_auto"] = explicit_transport(col(), g, 5 * DAY, rock, gfluid, gravity=gravity_vector(3)).s[:, 0]
+    out["grav_mat_sG"] = np.asarray(mg["sG"], float).ravel()
+    save("transport_phase3.npz", **out)
+
+
 if __name__ == "__main__":
     def want(name):
         return ONLY is None or name in ONLY
@@ -537,6 +594,8 @@ if __name__ == "__main__":
         cfg4_fixture()
     if want("cfg1"):
         cfg1_fixture()
+    if want("transport"):
+        transport_fixture()
     if want("bo"):
         bo_assemble_fixture()
         bo_newton_fixture()

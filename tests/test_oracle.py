@@ -273,3 +273,97 @@ def test_blackoil_fixture_exercises_switching_and_crossflow():
     assert (p[xf] < d["a_bhp"][2]).any() and (p[xf] > d["a_bhp"][2]).any()
     n = load("bo_newton.npz")
     assert (n["hist_status"][-1] == 3).sum() > (n["init_status"] == 3).sum()
+
+
+# ---- incompressible transport ------------------------------------------------------------------
+
+def transport_problem(case, flux=None):
+    """The phase-3 transport cases: (problem, initial s, gravity-estimate
+    flux) for the oracle, from the grid, rock, sources and flux of
+    validate_phase3's setups."""
+    from oracle import transport as otr
+    from pymrst_b200.params import CENTI, DARCY, DAY, MILLI, POISE
+    d = load("transport_phase3.npz")
+    if case == "bl":
+        g = cartesian_grid([100, 1, 1], [100.0, 1.0, 1.0])
+        k, poro, fl = 100 * MILLI * DARCY, 0.2, otr.Corey(np.array([1.0, 10.0]) * CENTI * POISE, [1000.0, 700.0], [2, 2])
+        rate = float(d["bl_rate"])
+        srcs = ([0, 99], [rate, -rate], [[1.0, 0.0], [0.0, 1.0]])
+        gvec = np.zeros(3)
+        flux = d["bl_flux0"] if flux is None else flux
+        s0 = np.zeros(g.cells.num)
+    elif case == "qfs":
+        g = cartesian_grid([32, 32, 1], [500.0, 500.0, 10.0])
+        k = ((10 + (7 * np.arange(g.cells.num)) % 100) * MILLI * DARCY)
+        poro, fl = 0.2, otr.Corey(np.array([1.0, 10.0]) * CENTI * POISE, [1000.0, 700.0], [2, 2])
+        srcs = ([0, g.cells.num - 1], [5e-3, -5e-3], [[1.0, 0.0], [0.0, 1.0]])
+        gvec = np.zeros(3)
+        s0 = np.zeros(g.cells.num)
+    else:
+        g = cartesian_grid([1, 1, 20], [1.0, 1.0, 20.0])
+        k, poro, fl = 1000 * MILLI * DARCY, 0.3, otr.Corey([1e-3, 1e-3], [1000.0, 700.0], [2, 2])
+        srcs = ([], [], np.zeros((0, 2)))
+        gvec = np.array([0.0, 0.0, 9.80665])
+        flux = np.zeros(g.faces.num)
+        s0 = np.full(g.cells.num, 0.5)
+    nc = g.cells.num
+    Nall = np.asarray(g.faces.neighbors)
+    internal = np.all(Nall >= 0, axis=1)
+    cf = np.asarray(g.cells.faces)
+    cell_no = np.repeat(np.arange(nc), np.diff(g.cells.facePos))
+    K = np.zeros((nc, 3, 3))
+    K[:, 0, 0] = K[:, 1, 1] = K[:, 2, 2] = k
+    normals = np.asarray(g.faces.normals)
+    gf = otr.gravity_flux(normals, cf, cell_no, K, gvec * (fl.rho[0] - fl.rho[1]), g.faces.num)[internal]
+    gf_est = otr.gravity_flux(normals, cf, cell_no, K, -gvec, g.faces.num)[internal]
+    q = otr.source(nc, fl, *srcs)
+    pv = poro * np.asarray(g.cells.volumes)
+    prob = otr.Problem(fl, Nall[internal], None if flux is None else np.asarray(flux)[internal], gf, q, pv)
+    return prob, s0, gf_est, g, internal
+
+
+def test_oracle_explicit_transport_matches_reference_and_matlab():
+    d = load("transport_phase3.npz")
+    DAY = 86400.0
+    prob, s0, gf_est, _, _ = transport_problem("bl")
+    s, nsub = prob.explicit(s0, 30 * DAY, gf_est, dt=0.25 * DAY)
+    assert nsub == 120
+    np.testing.assert_allclose(s, d["bl_sE"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(s, d["bl_mat_sE"], rtol=0, atol=1e-10)
+    s, _ = prob.explicit(s0, 30 * DAY, gf_est)
+    np.testing.assert_allclose(s, d["bl_sE_auto"], rtol=0, atol=1e-12)
+    prob, s0, gf_est, _, _ = transport_problem("grav")
+    s, _ = prob.explicit(s0, 5 * DAY, gf_est)
+    np.testing.assert_allclose(s, d["grav_sE_auto"], rtol=0, atol=1e-12)
+
+
+def test_oracle_implicit_transport_matches_reference_and_matlab():
+    d = load("transport_phase3.npz")
+    DAY = 86400.0
+    prob, s0, _, _, _ = transport_problem("bl")
+    s = prob.implicit(s0, 30 * DAY)
+    np.testing.assert_allclose(s, d["bl_sI"], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(s, d["bl_mat_sI"], rtol=0, atol=5e-6)
+    prob, s0, _, _, _ = transport_problem("grav")
+    s = prob.implicit(s0, 50 * DAY)
+    np.testing.assert_allclose(s, d["grav_sG"], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(s, d["grav_mat_sG"], rtol=0, atol=5e-6)
+
+
+def test_oracle_sequential_quarter_five_spot_matches_reference_and_matlab():
+    """Two incomp_tpfa + implicit transport cycles (validate_phase3's qfs)."""
+    from oracle import incomp as oinc
+    from pymrst_b200.params import DARCY, MILLI, add_source
+    d = load("transport_phase3.npz")
+    prob, s, _, g, internal = transport_problem("qfs")
+    rock = make_rock(g, ((10 + (7 * np.arange(g.cells.num)) % 100) * MILLI * DARCY)[:, None], 0.2)
+    ht = otrans.compute_trans(g, rock)
+    src = add_source(add_source(None, [0], 5e-3, sat=[[1.0, 0.0]]), [g.cells.num - 1], -5e-3, sat=[[0.0, 1.0]])
+    for _ in range(2):
+        mob = prob.fluid.mobility(np.column_stack([s, 1.0 - s]))
+        p, _, _, flux, _ = oinc.incomp_tpfa(g, ht, mob, [1000.0, 700.0], None, None, src, [])
+        prob.v = np.asarray(flux)[internal]
+        s = prob.implicit(s, 100 * 86400.0)
+    np.testing.assert_allclose(s, d["qfs_sQ"], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(p, d["qfs_pQ"], rtol=1e-9)
+    np.testing.assert_allclose(s, d["qfs_mat_sQ"], rtol=0, atol=2e-5)
