@@ -423,6 +423,48 @@ int pmb_tpfa_reconstruct(pmb_tpfa* h, const double* d_p, double* d_flux, double*
 int pmb_tpfa_levels(const pmb_tpfa* h, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);
 
 /* ------------------------------------------------------------------------
+ * Two-phase incompressible transport (explicit_transport and
+ * implicit_transport, pymrst/modules/incomp/transport/__init__.py:152-402)
+ * for a Corey fluid.  The handle holds the interior interfaces (h_N, nf x 2)
+ * and the pore volumes; pmb_transport_set_flow copies the frozen Darcy flux
+ * and gravity flux of each interior interface (d_flux, d_gflux, nf each) and
+ * the water source of each cell (d_q, nc; transport_source, :33-93) and takes
+ * h_fluid4 = [mu_w, mu_o, n_w, n_o].  Saturations d_s are the water
+ * saturations (nc), updated in place.
+ *
+ * pmb_transport_explicit: forward-Euler substeps over tf seconds, every
+ *   substep dt (dt > 0) or min(max_dt, dt_factor * the reference's stable-step
+ *   estimate, _estimate_dt :232-282) whose constant gravity part
+ *   max |dg gflux_est drho| the caller passes as gravity_wave; the substep
+ *   clock runs on the device.  Stops at the first substep that leaves
+ *   [-satwarn, 1 + satwarn] or produces NaN.  h_out4 = [substeps, time
+ *   reached, out-of-range flag, NaN flag].
+ * pmb_transport_implicit: backward Euler with Newton, bisection line search
+ *   and the substep control of newtonRaphson2ph; linear systems by the CSR
+ *   CPR-GMRES with one unknown per cell (opts as pmb_csr_cpr_create).
+ *   h_out6 = [time reached, substeps, Newton iterations, Krylov iterations,
+ *   linear solves that missed their tolerance, last substep length]; the
+ *   time reached is below tf when the minimum substep tf 2^-tsref failed.
+ * pmb_transport_residual / _jacobian: r(s, s0, dt) and dr/ds on the fixed
+ *   pattern of pmb_transport_pattern (each cell and its neighbours). */
+typedef struct pmb_transport pmb_transport;
+int pmb_transport_create(int32_t nc, int32_t nf, const int32_t* h_N, const double* h_pv, void* stream,
+                         pmb_transport** out);
+int pmb_transport_destroy(pmb_transport* h);
+/* *h_nnz = nonzeros; h_row_ptr (nc + 1) and h_col (nnz) may be NULL. */
+int pmb_transport_pattern(const pmb_transport* h, int64_t* h_nnz, int32_t* h_row_ptr, int32_t* h_col);
+int pmb_transport_set_flow(pmb_transport* h, const double* d_flux, const double* d_gflux, const double* d_q,
+                           const double* h_fluid4);
+/* *h_absmax (may be NULL) receives max |r|; synchronises when given. */
+int pmb_transport_residual(pmb_transport* h, const double* d_s, const double* d_s0, double dt, double* d_res,
+                           double* h_absmax);
+int pmb_transport_jacobian(pmb_transport* h, const double* d_s, double dt, double* d_vals);
+int pmb_transport_explicit(pmb_transport* h, double* d_s, double tf, double dt, double max_dt, double dt_factor,
+                           double satwarn, double gravity_wave, double* h_out4);
+int pmb_transport_implicit(pmb_transport* h, double* d_s, double tf, double nltol, int32_t lstrials,
+                           int32_t maxnewt, int32_t tsref, double resred, const pmb_cpr_opts* opts, double* h_out6);
+
+/* ------------------------------------------------------------------------
  * Three-phase black-oil model with dissolved gas (ThreePhaseBlackOilModelAD,
  * pymrst/modules/ad_blackoil/models/three_phase_black_oil_model.py:93-565)
  * and the deck-table fluid of init_deck_blackoil_fluid

@@ -148,6 +148,15 @@ SIGNATURES = {
     "pmb_tpfa_solve": (c_int, [c_vp, c_vp, c_vp, c_vp, c_dbl, c_int, P_dbl]),
     "pmb_tpfa_reconstruct": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_tpfa_levels": (c_int, [c_vp, c_int, P_i64, P_i32]),
+    "pmb_transport_create": (c_int, [c_int, c_int, P_i32, P_dbl, c_vp, C.POINTER(c_vp)]),
+    "pmb_transport_destroy": (c_int, [c_vp]),
+    "pmb_transport_pattern": (c_int, [c_vp, P_i64, P_i32, P_i32]),
+    "pmb_transport_set_flow": (c_int, [c_vp, c_vp, c_vp, c_vp, P_dbl]),
+    "pmb_transport_residual": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, P_dbl]),
+    "pmb_transport_jacobian": (c_int, [c_vp, c_vp, c_dbl, c_vp]),
+    "pmb_transport_explicit": (c_int, [c_vp, c_vp, c_dbl, c_dbl, c_dbl, c_dbl, c_dbl, c_dbl, P_dbl]),
+    "pmb_transport_implicit": (c_int, [c_vp, c_vp, c_dbl, c_dbl, c_int, c_int, c_int, c_dbl,
+                                       C.POINTER(CPROpts), P_dbl]),
     "pmb_bo_create": (c_int, [C.POINTER(BODesc), c_vp, C.POINTER(c_vp)]),
     "pmb_bo_destroy": (c_int, [c_vp]),
     "pmb_bo_sizes": (c_int, [c_vp, P_i64]),
