@@ -505,6 +505,72 @@ def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budge
     return out
 
 
+def measure_transport(torch, n=256, cpu_budget=20.0):
+    """Sequential incompressible transport on an n x n quarter five-spot
+    (rate injector and producer at opposite corners, the phase-3 Corey fluid,
+    the permeability pattern of validate_phase3's qfs case): one device
+    pressure solve, then implicit transport over 100 days and explicit
+    transport with the stable-step estimate over 2 days, each CUDA-event
+    timed after a warm-up call.  CPU: the oracle (numpy, SuperLU) on the same
+    flux, implicit and explicit, bounded by the budget, one core."""
+    from oracle import transport as otr
+    from pymrst_b200.grid import cartesian_grid
+    from pymrst_b200.incomp import State, incomp_tpfa
+    from pymrst_b200.ow_model import face_transmissibility_device
+    from pymrst_b200.params import CENTI, DARCY, DAY, MILLI, POISE, add_source, make_rock, pore_volume
+    from pymrst_b200.transport import explicit_transport, implicit_transport, init_simple_fluid, transport_source
+    g = cartesian_grid([n, n, 1], [500.0 * n / 32, 500.0 * n / 32, 10.0])
+    nc = g.cells.num
+    rock = make_rock(g, ((10 + (7 * np.arange(nc)) % 100) * MILLI * DARCY)[:, None], 0.2)
+    fluid = init_simple_fluid(mu=np.array([1.0, 10.0]) * CENTI * POISE, rho=[1000.0, 700.0], n=[2.0, 2.0])
+    rate = 5e-3 * (n / 32) ** 2
+    src = add_source(add_source(None, [0], rate, sat=[[1.0, 0.0]]), [nc - 1], -rate, sat=[[0.0, 1.0]])
+    new = lambda: State(pressure=np.zeros(nc), flux=np.zeros(g.faces.num),
+                        s=np.column_stack([np.zeros(nc), np.ones(nc)]))
+    st = incomp_tpfa(new(), g, face_transmissibility_device(g, rock)[1], fluid, src=src)
+    flux = st.flux.copy()
+
+    def run(kind, tf):
+        s = new()
+        s.flux = flux.copy()
+        e0, e1 = _events(torch)
+        torch.cuda.synchronize()
+        e0.record()
+        if kind == "implicit":
+            implicit_transport(s, g, tf, rock, fluid, src=src)
+        else:
+            explicit_transport(s, g, tf, rock, fluid, src=src)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3, s.s[:, 0]
+
+    run("implicit", 100 * DAY)
+    t_imp, s_imp = run("implicit", 100 * DAY)
+    stats = dict(implicit_transport.last_stats)
+    run("explicit", 2 * DAY)
+    t_exp, s_exp = run("explicit", 2 * DAY)
+    # the oracle on the same flux
+    Nall = np.asarray(g.faces.neighbors)
+    internal = np.all(Nall >= 0, axis=1)
+    q = transport_source(st, g, fluid, src=src)
+    prob = otr.Problem(otr.Corey(fluid.mu, fluid.rho, fluid.n), Nall[internal], flux[internal],
+                       np.zeros(int(internal.sum())), q, pore_volume(g, rock))
+    t0 = time.perf_counter()
+    s_cpu, nsub = prob.explicit(np.zeros(nc), 2 * DAY, np.zeros(int(internal.sum())))
+    t_cpu_exp = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    s_cpu_imp = prob.implicit(np.zeros(nc), 100 * DAY)
+    t_cpu_imp = time.perf_counter() - t0
+    return {"workload": f"incompressible transport, quarter five-spot {n}x{n} ({nc:,} cells), Corey n = 2, "
+                        f"mu 1 / 10 cP",
+            "implicit_100_days": {"gpu_s": t_imp, "cpu_s": t_cpu_imp, "speedup": t_cpu_imp / t_imp,
+                                  "max_abs_ds_vs_cpu": float(np.abs(s_imp - s_cpu_imp).max()), **stats},
+            "explicit_2_days": {"gpu_s": t_exp, "cpu_s": t_cpu_exp, "speedup": t_cpu_exp / t_exp, "substeps": nsub,
+                                 "cell_substeps_per_s": nc * nsub / t_exp,
+                                 "max_abs_ds_vs_cpu": float(np.abs(s_exp - s_cpu).max())},
+            "cpu": "oracle (numpy; SuperLU for the implicit systems) on the same flux, one core"}
+
+
 def run_ensemble_workload(args):
     """Config 3 (`--workload ensemble`): the seeded realisations (nx, ny in
     16..64, nz in 2..8, an independent lognormal permeability and a five-spot
@@ -766,7 +832,8 @@ def run_ours(args):
                          ("ow_fp64_100x100x10", lambda: measure_ow_fp64(torch, N, GpuOilWaterModel, run_report_step,
                                                                         args.cpu_budget)),
                          ("adjoint_64x64x4", lambda: measure_adjoint(torch, GpuOilWaterModel)),
-                         ("blackoil_100x100x10", lambda: measure_blackoil(torch))):
+                         ("blackoil_100x100x10", lambda: measure_blackoil(torch)),
+                         ("transport_256x256", lambda: measure_transport(torch))):
             try:
                 configs[name] = fn()
             except Exception as e:  # a secondary measurement must not hide the headline line
