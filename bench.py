@@ -56,8 +56,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="channelised", choices=["channelised", "ensemble"],
-                    help="channelised: the headline benchmark; ensemble: config 3 on its own line")
+    ap.add_argument("--workload", default="channelised", choices=["channelised", "ensemble", "blackoil", "transport"],
+                    help="channelised: the headline benchmark; ensemble: config 3 on its own line; blackoil / "
+                         "transport: those measurements of the other configurations on their own line "
+                         "(--dims sets the grid)")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (--workload ensemble)")
     ap.add_argument("--ens-graph", type=int, default=1, help="ensemble: replay each member's preconditioner as a graph")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
@@ -435,7 +437,7 @@ def measure_adjoint(torch, GpuOilWaterModel, cpu_steps=3):
             "cpu": f"oracle forward + adjoint (numpy, SuperLU) over the first {cpu_steps} steps, one core"}
 
 
-def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budget=30.0):
+def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budget=30.0, cpu=True):
     """The three-phase black-oil model with dissolved gas (the seeded
     lattice case of cases.blackoil_box: gas injectors, bhp producers, one
     oil-rate producer) over its seven steps (0.5 to 20 days), the whole
@@ -470,6 +472,8 @@ def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budge
            "newton_iterations": its, "krylov_iterations": krylov, "failed_steps": failed,
            "saturated_cells_at_end": int((model.from_device(x).status == 3).sum())}
     ref = Path(__file__).resolve().parent / "baseline" / "_ref"
+    if not cpu:
+        return out
     if not (ref / "pymrst").is_dir():
         out["cpu"] = "the reference package is not installed under baseline/_ref"
         return out
@@ -505,7 +509,7 @@ def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budge
     return out
 
 
-def measure_transport(torch, n=256, cpu_budget=20.0):
+def measure_transport(torch, n=256, cpu=True):
     """Sequential incompressible transport on an n x n quarter five-spot
     (rate injector and producer at opposite corners, the phase-3 Corey fluid,
     the permeability pattern of validate_phase3's qfs case): one device
@@ -549,6 +553,13 @@ def measure_transport(torch, n=256, cpu_budget=20.0):
     stats = dict(implicit_transport.last_stats)
     run("explicit", 2 * DAY)
     t_exp, s_exp = run("explicit", 2 * DAY)
+    nsub_gpu = explicit_transport.last_stats["substeps"]
+    out = {"workload": f"incompressible transport, quarter five-spot {n}x{n} ({nc:,} cells), Corey n = 2, "
+                       f"mu 1 / 10 cP",
+           "implicit_100_days": {"gpu_s": t_imp, **stats},
+           "explicit_2_days": {"gpu_s": t_exp, "substeps": nsub_gpu, "cell_substeps_per_s": nc * nsub_gpu / t_exp}}
+    if not cpu:
+        return out
     # the oracle on the same flux
     Nall = np.asarray(g.faces.neighbors)
     internal = np.all(Nall >= 0, axis=1)
@@ -565,10 +576,22 @@ def measure_transport(torch, n=256, cpu_budget=20.0):
                         f"mu 1 / 10 cP",
             "implicit_100_days": {"gpu_s": t_imp, "cpu_s": t_cpu_imp, "speedup": t_cpu_imp / t_imp,
                                   "max_abs_ds_vs_cpu": float(np.abs(s_imp - s_cpu_imp).max()), **stats},
-            "explicit_2_days": {"gpu_s": t_exp, "cpu_s": t_cpu_exp, "speedup": t_cpu_exp / t_exp, "substeps": nsub,
-                                 "cell_substeps_per_s": nc * nsub / t_exp,
+            "explicit_2_days": {"gpu_s": t_exp, "cpu_s": t_cpu_exp, "speedup": t_cpu_exp / t_exp, "substeps": nsub_gpu,
+                                 "cpu_substeps": nsub, "cell_substeps_per_s": nc * nsub_gpu / t_exp,
                                  "max_abs_ds_vs_cpu": float(np.abs(s_exp - s_cpu).max())},
             "cpu": "oracle (numpy; SuperLU for the implicit systems) on the same flux, one core"}
+
+
+def run_side_workload(args):
+    """One of the other configurations' measurements as its own JSON line
+    (rank 0, one GPU)."""
+    import torch
+    dims = tuple(int(v) for v in args.dims.split(",")) if args.dims else None
+    if args.workload == "blackoil":
+        out = measure_blackoil(torch, dims=dims or (100, 100, 10), cpu=not args.no_cpu_baseline)
+    else:
+        out = measure_transport(torch, n=dims[0] if dims else 256, cpu=not args.no_cpu_baseline)
+    print(json.dumps({"workload": args.workload, **out}), flush=True)
 
 
 def run_ensemble_workload(args):
@@ -910,6 +933,8 @@ def main():
         run_reference(args)
     elif args.workload == "ensemble":
         run_ensemble_workload(args)
+    elif args.workload in ("blackoil", "transport"):
+        run_side_workload(args)
     else:
         run_ours(args)
 

@@ -242,16 +242,16 @@ class BlackOilCase:
     dts: np.ndarray
 
 
-def blackoil_box(dims=(10, 10, 3), cell_size=(30.0, 30.0, 10.0), seed=23, spacing=10,
+def blackoil_box(dims=(10, 10, 3), cell_size=(30.0, 30.0, 10.0), seed=23, spacing=10, gas_rate=5.0,
                  dt_days=(0.5, 1.0, 2.0, 5.0, 10.0, 10.0, 20.0)) -> BlackOilCase:
     """Gas injection into an undersaturated live-oil box (see the module
     docstring).  Wells on a lattice: gas injectors (total surface rate) down
     the upper half of columns (s/2 + s a, s/2 + s b), bhp producers (250 bar)
     down the lower half of columns (s a, s b), s = `spacing`, and an oil-rate
     producer down the lower half of column (nx-1, ny-1).  Each injector takes
-    5 sm^3/s and the oil producer 0.012 sm^3/s per 5,400 m^3 of perforated
-    pore volume, which liberates gas around the injectors within a few
-    steps."""
+    `gas_rate` sm^3/s and the oil producer 0.012 sm^3/s per 5,400 m^3 of
+    perforated pore volume, which liberates gas around the injectors within
+    a few steps."""
     from .blackoil import BOState
     rng = np.random.default_rng(seed)
     dims = tuple(int(v) for v in dims)
@@ -270,7 +270,7 @@ def blackoil_box(dims=(10, 10, 3), cell_size=(30.0, 30.0, 10.0), seed=23, spacin
     for i in range(h, nx, spacing):
         for j in range(h, ny, spacing):
             cells = cell_index(g, i, j, top)
-            q = 5.0 * float(pv[cells].sum()) / 5400.0
+            q = gas_rate * float(pv[cells].sum()) / 5400.0
             wells = add_well(wells, g, rock, cells, well_type="rate", val=q, radius=0.1,
                              compi=np.array([0.0, 0.0, 1.0]))
             gas.append(q); oil.append(0.0); bhp_val.append(None)

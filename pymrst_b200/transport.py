@@ -260,6 +260,7 @@ def explicit_transport(state, g, tf: float, rock, fluid, wells: Optional[Sequenc
         raise AssertionError("explicit_transport: transport failed")
     sw = s.cpu().numpy()
     state.s = np.column_stack([sw, 1.0 - sw])
+    explicit_transport.last_stats = dict(substeps=int(out[0]))
     return state
 
 

@@ -337,10 +337,16 @@ def cfg1_fixture(nsteps=1):
     case = cases.five_spot(dims=(100, 100, 10), seed=1)
     g, rock, w, model = _five_spot_reference(case)
     st0 = model.initial_state(case.p0, case.sw0)
+    events = []
     t0 = time.perf_counter()
-    states, its = simulate_schedule_ad(st0, model, np.full(nsteps, case.dt), verbose=False)
+    states, its = simulate_schedule_ad(st0, model, np.full(nsteps, case.dt), verbose=False,
+                                       observer=lambda ev, p: events.append((ev, p.get("dt", 0.0),
+                                                                             p.get("iterations", -1))))
     el = time.perf_counter() - t0
+    ministeps = np.array([[dt, it, 1.0 if ev == "step_accepted" else 0.0] for ev, dt, it in events
+                          if ev in ("step_accepted", "step_rejected")])
     save("cfg1_ow_100x100x10.npz", dims=np.array(case.grid.cartDims), perm_sum=np.array(np.sum(rock.perm)),
+         ministeps=ministeps,
          wi_sum=np.array(sum(np.sum(x.WI) for x in w)), its=np.asarray(its),
          p_hist=np.vstack([s.pressure for s in states]), sw_hist=np.vstack([s.sW for s in states]),
          qws_hist=np.vstack([s.qWs for s in states]), qos_hist=np.vstack([s.qOs for s in states]),

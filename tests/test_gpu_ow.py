@@ -188,8 +188,12 @@ def test_config1_first_step_matches_reference_at_100x100x10():
     assert np.isclose(sum(np.sum(w.WI) for w in c.wells), float(d["wi_sum"]), rtol=1e-12)
     m = GpuOilWaterModel(c.grid, c.rock, c.fluid, c.wells, gravity=c.gravity,
                          cpr_options=dict(rtol=1e-12, maxiter=600, amg_rebuild_interval=1_000_000))
-    states, its = simulate_schedule_ad(m.initial_state(c.p0, c.sw0), m, [c.dt], verbose=False)
-    assert list(its) == list(d["its"])
+    events = []
+    states, its = simulate_schedule_ad(m.initial_state(c.p0, c.sw0), m, [c.dt], verbose=False,
+                                       observer=lambda ev, p: events.append((ev, p.get("dt"), p.get("iterations"))))
+    mine = [(round(dt), it, ev == "step_accepted") for ev, dt, it in events if ev in ("step_accepted", "step_rejected")]
+    ref = [(round(a), int(b), bool(c)) for a, b, c in d["ministeps"]] if "ministeps" in d else None
+    assert list(its) == list(d["its"]), (mine, ref)
     p_ref = d["p_hist"][0]
     assert np.abs(states[0].pressure - p_ref).max() <= 1e-8 * np.abs(p_ref).max()
     assert np.abs(states[0].sW - d["sw_hist"][0]).max() <= 1e-7
