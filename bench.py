@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the measurements of the other benchmark configurations")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--skip-implicit", action="store_true", help="transport workload: explicit transport only")
     ap.add_argument("--cpr", default="", help="CPR option overrides, e.g. amg_cycle=2,local_sweeps=1")
     ap.add_argument("--probe", type=int, default=0,
                     help="profiling probe: run this many Newton iterations of the first step and exit")
@@ -509,7 +510,7 @@ def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budge
     return out
 
 
-def measure_transport(torch, n=256, cpu=True):
+def measure_transport(torch, n=256, cpu=True, implicit=True):
     """Sequential incompressible transport on an n x n quarter five-spot
     (rate injector and producer at opposite corners, the phase-3 Corey fluid,
     the permeability pattern of validate_phase3's qfs case): one device
@@ -548,9 +549,11 @@ def measure_transport(torch, n=256, cpu=True):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) * 1e-3, s.s[:, 0]
 
-    run("implicit", 100 * DAY)
-    t_imp, s_imp = run("implicit", 100 * DAY)
-    stats = dict(implicit_transport.last_stats)
+    t_imp, s_imp, stats = float("nan"), None, {}
+    if implicit:
+        run("implicit", 100 * DAY)
+        t_imp, s_imp = run("implicit", 100 * DAY)
+        stats = dict(implicit_transport.last_stats)
     run("explicit", 2 * DAY)
     t_exp, s_exp = run("explicit", 2 * DAY)
     nsub_gpu = explicit_transport.last_stats["substeps"]
@@ -558,7 +561,7 @@ def measure_transport(torch, n=256, cpu=True):
                        f"mu 1 / 10 cP",
            "implicit_100_days": {"gpu_s": t_imp, **stats},
            "explicit_2_days": {"gpu_s": t_exp, "substeps": nsub_gpu, "cell_substeps_per_s": nc * nsub_gpu / t_exp}}
-    if not cpu:
+    if not cpu or not implicit:
         return out
     # the oracle on the same flux
     Nall = np.asarray(g.faces.neighbors)
@@ -590,7 +593,8 @@ def run_side_workload(args):
     if args.workload == "blackoil":
         out = measure_blackoil(torch, dims=dims or (100, 100, 10), cpu=not args.no_cpu_baseline)
     else:
-        out = measure_transport(torch, n=dims[0] if dims else 256, cpu=not args.no_cpu_baseline)
+        out = measure_transport(torch, n=dims[0] if dims else 256, cpu=not args.no_cpu_baseline,
+                                implicit=not args.skip_implicit)
     print(json.dumps({"workload": args.workload, **out}), flush=True)
 
 

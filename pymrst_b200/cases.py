@@ -242,7 +242,7 @@ class BlackOilCase:
     dts: np.ndarray
 
 
-def blackoil_box(dims=(10, 10, 3), cell_size=(30.0, 30.0, 10.0), seed=23, spacing=10, gas_rate=5.0,
+def blackoil_box(dims=(10, 10, 3), cell_size=(30.0, 30.0, 10.0), seed=23, spacing=10, gas_rate=1.0,
                  dt_days=(0.5, 1.0, 2.0, 5.0, 10.0, 10.0, 20.0)) -> BlackOilCase:
     """Gas injection into an undersaturated live-oil box (see the module
     docstring).  Wells on a lattice: gas injectors (total surface rate) down
