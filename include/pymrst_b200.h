@@ -326,9 +326,13 @@ int pmb_dense_inverse(int32_t n, const double* d_a, double* d_inv, void* stream)
  * One backward-Euler step solved by Newton on the device (step,
  * two_phase_oil_water_model.py:605-657): d_x holds the state at the start
  * of the step and receives the new state.  h_stats8 = [iterations,
- * converged, krylov_iterations, setups, cnv, mb, nonfinite, 0].  Returns
- * PMB_OK also when Newton did not converge (converged = 0); a linear-solver
- * failure returns PMB_ERR_NOCONV with d_x restored to the start state. */
+ * converged, krylov_iterations, setups, cnv, mb, nonfinite, linear solves
+ * that stopped above their tolerance but were used].  Returns PMB_OK also
+ * when Newton did not converge (converged = 0).  A linear solve that stops
+ * above rtol with a relative residual of at most 1e-6 still updates the
+ * iterate (the Newton test decides, as with an exact solve); a worse or
+ * non-finite one returns PMB_ERR_NOCONV with d_x restored to the start
+ * state. */
 int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_iterations,
                 double* h_stats8);
 
@@ -554,7 +558,9 @@ int pmb_bo_update(pmb_bo* h, double* d_state, const double* d_dx);
 /* One step by Newton (step, :541-565) with the CSR CPR-GMRES as the linear
  * solver; d_state holds the start state and receives the last iterate.
  * h_stats4 = [iterations, converged, Krylov iterations, linear solves that
- * missed their tolerance]. */
+ * missed their tolerance].  A solve that missed it with a relative residual
+ * of at most 1e-6 still updates the iterate; a worse one ends the step
+ * unconverged. */
 int pmb_bo_step(pmb_bo* h, double* d_state, double dt, int32_t max_iterations, const pmb_cpr_opts* opts,
                 double* h_stats4);
 /* The fluid at n points (tests and the host's fluid check): d_out7 =

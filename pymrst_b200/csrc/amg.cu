@@ -21,7 +21,11 @@ namespace pmb {
 // Rows without any negative coupling (possible after upwinding with gravity,
 // and on Galerkin coarse levels) use |a_ij| as strength instead.  With
 // `attach`, an unknown left alone joins the aggregate of its strongest
-// neighbour, so every connected unknown is coarsened.
+// neighbour, so every connected unknown is coarsened; a row whose couplings
+// are all exactly zero (a transport Jacobian where no phase is mobile) is
+// then paired with, or attached to, its first neighbour in the pattern, so
+// that the coarsening does not stall on it (the smoother solves such rows
+// exactly).
 static int pairwise_match(int n, const int* rp, const int* ci, const double* v, double theta,
                           std::vector<int>& agg, bool attach) {
   agg.assign(n, -1);
@@ -45,6 +49,9 @@ static int pairwise_match(int n, const int* rp, const int* ci, const double* v, 
         const double s = use_abs ? std::fabs(v[k]) : -v[k];
         if (s >= theta * mx && s > bv) { bv = s; best = j; }
       }
+    } else if (attach) {
+      for (int k = rp[i]; k < rp[i + 1] && best < 0; ++k)
+        if (ci[k] != i && agg[ci[k]] < 0) best = ci[k];
     }
     agg[i] = na;
     if (best >= 0) agg[best] = na;
@@ -62,6 +69,8 @@ static int pairwise_match(int n, const int* rp, const int* ci, const double* v, 
       const double s = std::fabs(v[k]);
       if (s > bv) { bv = s; best = j; }
     }
+    for (int k = rp[i]; k < rp[i + 1] && best < 0; ++k)
+      if (ci[k] != i) best = ci[k];
     if (best >= 0) agg[i] = agg[best];
   }
   std::vector<int> ren(na, -1);

@@ -1267,7 +1267,11 @@ void BOModel::step(double* x, double dt, int maxit, const pmb_cpr_opts& o, doubl
     rc = pmb_csr_cpr_solve(cpr_, rhs_.get(), dx_.get(), info);
     if (rc != PMB_OK && rc != PMB_ERR_NOCONV) throw Error(rc, std::string("bo: linear solve failed: ") + pmb_last_error());
     lin_its += info[0];
-    if (rc != PMB_OK || info[2] == 0.0) lin_fail += 1.0;
+    if (rc != PMB_OK || info[2] == 0.0) {
+      // a solve this close to exact still makes a Newton update; worse fails the step
+      lin_fail += 1.0;
+      if (!(std::isfinite(info[1]) && info[1] <= 1e-6)) break;
+    }
     update(x, dx_.get());
   }
   assemble(x, x0_.get(), dt, res_.get(), vals_.get());

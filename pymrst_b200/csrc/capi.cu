@@ -447,7 +447,10 @@ int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_itera
     for (int i = 0; i < 8; ++i) stats[i] = 0.0;
     PMB_CUDA(cudaMemcpyAsync(m.x0(), d_x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     m.compute_cdp(m.x0(), m.cdp());
-    double krylov = 0.0;
+    double krylov = 0.0, soft = 0.0;
+    // a solve that stopped above rtol but this close to exact still makes a
+    // Newton update
+    constexpr double kUsableRelres = 1e-6;
     auto evaluate = [&](bool want_jac) {
       {
         PhaseTimer pt("newton.assemble", st);
@@ -468,6 +471,7 @@ int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_itera
         stats[1] = 1.0;
         stats[2] = krylov;
         stats[3] = (double)cpr.setups();
+        stats[7] = soft;
         return;
       }
       if (h->conv[6] != 0.0) break;  // non-finite residual: the step fails
@@ -489,6 +493,10 @@ int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_itera
         std::fprintf(stderr, "# newton it=%d cnv=%.3e mb=%.3e well_w=%.3e well_o=%.3e ctrl_ok=%g krylov=%g relres=%.2e\n",
                      it, h->conv[0], h->conv[1], h->conv[2], h->conv[3], h->conv[4], info[0], info[1]);
       krylov += info[0];
+      if (!ok && std::isfinite(info[1]) && info[1] <= kUsableRelres) {
+        ok = true;  // close enough to an exact solve: let the Newton test decide
+        soft += 1.0;
+      }
       if (!ok) {
         PMB_CUDA(cudaMemcpyAsync(d_x, m.x0(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         PMB_CUDA(cudaStreamSynchronize(st));
@@ -508,6 +516,7 @@ int pmb_ow_step(pmb_ow* h, pmb_cpr* s, double* d_x, double dt, int32_t max_itera
     stats[4] = h->conv[0];
     stats[5] = h->conv[1];
     stats[6] = h->conv[6];
+    stats[7] = soft;
   });
 }
 
