@@ -303,6 +303,13 @@ int pmb_csr_cpr_create(int32_t n, int32_t nc, int32_t nph, const int32_t* h_row_
 int pmb_csr_cpr_destroy(pmb_csr_cpr* h);
 int pmb_csr_cpr_setup(pmb_csr_cpr* h, const double* d_values, const double* h_weights);
 int pmb_csr_cpr_solve(pmb_csr_cpr* h, const double* d_b, double* d_x, double* h_info4);
+/* on != 0: the pressure stage uses per-cell weights, row 0 of the inverse of
+ * each cell's diagonal nph x nph block (the weighted sum of the cell's rows
+ * then has a unit derivative in its own pressure and none in its other
+ * unknowns: true-IMPES on the full diagonal block), instead of the phase
+ * weights given to setup; non-transposed systems only.  No reference
+ * counterpart (its CPRSolver uses the quasi-IMPES phase weights). */
+int pmb_csr_cpr_set_cell_weights(pmb_csr_cpr* h, int32_t on);
 /* y = A x with the values d_values on the handle's pattern. */
 int pmb_csr_spmv(pmb_csr_cpr* h, const double* d_values, const double* d_x, double* d_y);
 int pmb_csr_cpr_levels(const pmb_csr_cpr* h, int32_t max_levels, int64_t* h_sizes, int32_t* n_levels);

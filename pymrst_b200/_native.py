@@ -132,6 +132,7 @@ SIGNATURES = {
     "pmb_csr_cpr_destroy": (c_int, [c_vp]),
     "pmb_csr_cpr_setup": (c_int, [c_vp, c_vp, P_dbl]),
     "pmb_csr_cpr_solve": (c_int, [c_vp, c_vp, c_vp, P_dbl]),
+    "pmb_csr_cpr_set_cell_weights": (c_int, [c_vp, c_int]),
     "pmb_csr_spmv": (c_int, [c_vp, c_vp, c_vp, c_vp]),
     "pmb_csr_row_scale": (c_int, [c_int, c_vp, c_vp, c_vp, c_vp]),
     "pmb_csr_cpr_levels": (c_int, [c_vp, c_int, P_i64, P_i32]),

@@ -27,6 +27,7 @@
 // (the Newton update with the reference's limits and the black-oil flash).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -952,6 +953,9 @@ class BOModel {
   PinnedArray<double> h_conv_;
   pmb_csr_cpr* cpr_ = nullptr;
   pmb_cpr_opts cpr_opts_{};
+
+ public:
+  bool cell_weights_ = true;
 };
 
 namespace {
@@ -1189,6 +1193,10 @@ BOModel::BOModel(const pmb_bo_desc& d, cudaStream_t s) : s_(s) {
   v_.tol_well = d.tol_well;
   v_.ds_max = d.ds_max;
   v_.pv_tot = pv_tot;
+  {
+    const char* e = std::getenv("PMB_BO_PHASE_WEIGHTS");  // A/B: the global quasi-IMPES weights instead
+    cell_weights_ = !(e && e[0] == '1');
+  }
   props_.resize((size_t)bo::kNumProps * nc);
   part_.resize((size_t)bo::kConvBlocks * (bo::kConvSums + bo::kConvMax));
   conv_out_.resize(bo::kConvOut);
@@ -1239,7 +1247,11 @@ void BOModel::step(double* x, double dt, int maxit, const pmb_cpr_opts& o, doubl
   if (!cpr_ || std::memcmp(&o, &cpr_opts_, sizeof(o)) != 0) {
     if (cpr_) pmb_csr_cpr_destroy(cpr_);
     cpr_ = nullptr;
-    const int rc = pmb_csr_cpr_create((int32_t)n, v_.nc, 3, h_row_ptr_.data(), h_col_.data(), 0, &o, s_, &cpr_);
+    int rc = pmb_csr_cpr_create((int32_t)n, v_.nc, 3, h_row_ptr_.data(), h_col_.data(), 0, &o, s_, &cpr_);
+    if (rc != PMB_OK) throw Error(rc, std::string("bo: CPR setup failed: ") + pmb_last_error());
+    // per-cell true-IMPES weights: in undersaturated cells the third unknown
+    // is Rs, which global phase weights at the mean pressure leave coupled
+    rc = pmb_csr_cpr_set_cell_weights(cpr_, cell_weights_ ? 1 : 0);
     if (rc != PMB_OK) throw Error(rc, std::string("bo: CPR setup failed: ") + pmb_last_error());
     cpr_opts_ = o;
   }

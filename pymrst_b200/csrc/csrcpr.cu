@@ -214,6 +214,44 @@ __global__ void csr_restrict_kernel(int nc, int nph, const double* __restrict__ 
   bp[c] = (T)s;
 }
 
+// Per-cell decoupling weights: row 0 of the inverse of the cell's diagonal
+// block, so that the weighted sum of the cell's rows has a unit derivative
+// with respect to its own pressure and none with respect to its other
+// unknowns (true-IMPES on the full diagonal block).
+__global__ void csr_cell_weights_kernel(int nc, int nph, const double* __restrict__ inv, double* __restrict__ wc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  for (int j = 0; j < nph; ++j) wc[(long long)c * nph + j] = inv[(long long)c * nph * nph + j];
+}
+
+// A_p values with per-cell weights: row c sums w_c[phase] * A over the
+// sources of each of its entries.
+template <class T>
+__global__ void csr_pressure_values_cell_kernel(int nc, int nph, const int* __restrict__ prp,
+                                                const int* __restrict__ gptr, const int* __restrict__ gsrc,
+                                                const unsigned char* __restrict__ gph, const double* __restrict__ a,
+                                                const double* __restrict__ wc, T* __restrict__ ap) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const double* w = wc + (long long)c * nph;
+  for (int e = prp[c]; e < prp[c + 1]; ++e) {
+    double s = 0.0;
+    for (int k = gptr[e]; k < gptr[e + 1]; ++k) s += w[gph[k]] * a[gsrc[k]];
+    ap[e] = (T)s;
+  }
+}
+
+// bp[c] = sum_i w_c[i] r[i*nc + c]
+template <class T>
+__global__ void csr_restrict_cell_kernel(int nc, int nph, const double* __restrict__ r, const double* __restrict__ wc,
+                                         T* __restrict__ bp) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double s = 0.0;
+  for (int i = 0; i < nph; ++i) s += wc[(long long)c * nph + i] * r[(long long)i * nc + c];
+  bp[c] = (T)s;
+}
+
 // x = Q xp evaluated at column j: the injection into the pressure block
 // (Q = P), or the weighted spread into every cell block (Q = W^T).
 template <bool TR, class T>
@@ -339,6 +377,14 @@ class CsrCPR {
   void setup(const double* d_val, const double* h_w);
   bool solve(const double* b, double* x, double* info);
   void spmv(const double* val, const double* x, double* y);
+  // 1: per-cell weights from the diagonal blocks instead of the caller's
+  // phase weights (non-transposed systems)
+  void set_cell_weights(bool on) {
+    PMB_REQUIRE(!on || !tr_, "per-cell weights are for the non-transposed system");
+    cell_w_ = on;
+    if (on) wcell_.resize((size_t)nc_ * nph_);
+    since_build_ = 1 << 30;  // rebuild the hierarchy on the next setup
+  }
   int num_levels() const { return f32_ ? amg32_.num_levels() : amg_.num_levels(); }
   int level_size(int l) const { return f32_ ? amg32_.level_size(l) : amg_.level_size(l); }
 
@@ -370,7 +416,8 @@ class CsrCPR {
   DArray<long long> tail_dst_, tg_off_;
   int tail_cnt_ = 0, ngroups_ = 0, max_group_ = 0;
   long long tail_dense_ = 0;
-  DArray<double> inv_, tM_, tInv_, trs_, ytmp_;
+  DArray<double> inv_, tM_, tInv_, trs_, ytmp_, wcell_;
+  bool cell_w_ = false;
   DArray<int> status_;
   PinnedArray<int> st_pin_;
   PinnedArray<double> w_pin_;
@@ -573,8 +620,14 @@ void CsrCPR::setup(const double* d_val, const double* h_w) {
                                                      trs_.get(), status_.get());
     PMB_CHECK_LAUNCH();
   }
+  if (o_.use_pressure_stage && cell_w_) {
+    csr_cell_weights_kernel<<<grid_for(nc_, 256), 256, 0, s_>>>(nc_, nph_, inv_.get(), wcell_.get());
+    PMB_CHECK_LAUNCH();
+  }
   if (o_.use_pressure_stage) {
-    PMB_REQUIRE(h_w != nullptr, "the pressure stage needs the phase weights");
+    PMB_REQUIRE(h_w != nullptr || cell_w_, "the pressure stage needs the phase weights");
+    static const double kUnit[kMaxPhases] = {1.0, 0.0, 0.0};
+    if (cell_w_) h_w = kUnit;
     for (int i = 0; i < nph_; ++i) {
       PMB_REQUIRE(std::isfinite(h_w[i]), "non-finite phase weight");
       w_pin_[i] = h_w[i];
@@ -589,8 +642,12 @@ void CsrCPR::setup(const double* d_val, const double* h_w) {
     const int g = grid_for(pn, 256);
     const bool built = f32_ ? amg32_.built() : amg_.built();
     if (!built || since_build_ >= std::max(1, o_.amg_rebuild_interval)) {
-      csr_pressure_values_kernel<double><<<g, 256, 0, s_>>>(pn, gptr_.get(), gsrc_.get(), gph_.get(), val_, w_.get(),
-                                                           ap_.get());
+      if (cell_w_)
+        csr_pressure_values_cell_kernel<double><<<grid_for(nc_, 128), 128, 0, s_>>>(
+            nc_, nph_, prp_.get(), gptr_.get(), gsrc_.get(), gph_.get(), val_, wcell_.get(), ap_.get());
+      else
+        csr_pressure_values_kernel<double><<<g, 256, 0, s_>>>(pn, gptr_.get(), gsrc_.get(), gph_.get(), val_,
+                                                             w_.get(), ap_.get());
       PMB_CHECK_LAUNCH();
       h_ap_.resize(pn);
       PMB_CUDA(cudaMemcpyAsync(h_ap_.data(), ap_.get(), sizeof(double) * pn, cudaMemcpyDeviceToHost, s_));
@@ -605,13 +662,21 @@ void CsrCPR::setup(const double* d_val, const double* h_w) {
       graph_.invalidate();
     }
     if (f32_) {
-      csr_pressure_values_kernel<float><<<g, 256, 0, s_>>>(pn, gptr_.get(), gsrc_.get(), gph_.get(), val_, w_.get(),
-                                                          amg32_.level0_val());
+      if (cell_w_)
+        csr_pressure_values_cell_kernel<float><<<grid_for(nc_, 128), 128, 0, s_>>>(
+            nc_, nph_, prp_.get(), gptr_.get(), gsrc_.get(), gph_.get(), val_, wcell_.get(), amg32_.level0_val());
+      else
+        csr_pressure_values_kernel<float><<<g, 256, 0, s_>>>(pn, gptr_.get(), gsrc_.get(), gph_.get(), val_,
+                                                            w_.get(), amg32_.level0_val());
       PMB_CHECK_LAUNCH();
       amg32_.refresh(s_, status_.get());
     } else {
-      csr_pressure_values_kernel<double><<<g, 256, 0, s_>>>(pn, gptr_.get(), gsrc_.get(), gph_.get(), val_, w_.get(),
-                                                           amg_.level0_val());
+      if (cell_w_)
+        csr_pressure_values_cell_kernel<double><<<grid_for(nc_, 128), 128, 0, s_>>>(
+            nc_, nph_, prp_.get(), gptr_.get(), gsrc_.get(), gph_.get(), val_, wcell_.get(), amg_.level0_val());
+      else
+        csr_pressure_values_kernel<double><<<g, 256, 0, s_>>>(pn, gptr_.get(), gsrc_.get(), gph_.get(), val_,
+                                                             w_.get(), amg_.level0_val());
       PMB_CHECK_LAUNCH();
       amg_.refresh(s_, status_.get());
     }
@@ -642,7 +707,10 @@ void CsrCPR::precond_body(const double* r, double* z) {
   };
   if (o_.use_pressure_stage) {
     auto pressure_stage = [&](auto* bp, auto* xp, auto& amg) {
-      csr_restrict_kernel<<<grid_for(nc_, 256), 256, 0, s_>>>(nc_, nph_, r, rw_.get(), bp);
+      if (cell_w_)
+        csr_restrict_cell_kernel<<<grid_for(nc_, 256), 256, 0, s_>>>(nc_, nph_, r, wcell_.get(), bp);
+      else
+        csr_restrict_kernel<<<grid_for(nc_, 256), 256, 0, s_>>>(nc_, nph_, r, rw_.get(), bp);
       PMB_CHECK_LAUNCH();
       {
         PhaseTimer pt("cpr.amg_cycle", s_);
@@ -729,6 +797,13 @@ int pmb_csr_cpr_solve(pmb_csr_cpr* h, const double* d_b, double* d_x, double* in
       throw pmb::Error(PMB_ERR_NOCONV, "CPR-GMRES did not reach its tolerance (relres " +
                                            std::to_string(info4[1]) + " after " +
                                            std::to_string((long long)info4[0]) + " iterations)");
+  });
+}
+
+int pmb_csr_cpr_set_cell_weights(pmb_csr_cpr* h, int32_t on) {
+  return pmb::guarded([&] {
+    PMB_REQUIRE(h != nullptr, "NULL argument");
+    h->impl->set_cell_weights(on != 0);
   });
 }
 
