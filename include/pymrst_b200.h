@@ -565,8 +565,8 @@ int pmb_bo_update(pmb_bo* h, double* d_state, const double* d_dx);
 /* One step by Newton (step, :541-565) with the CSR CPR-GMRES as the linear
  * solver; d_state holds the start state and receives the last iterate.
  * h_stats4 = [iterations, converged, Krylov iterations, linear solves that
- * missed their tolerance].  A solve that missed it with a relative residual
- * of at most 1e-6 still updates the iterate; a worse one ends the step
+ * missed their tolerance].  The update of a solve that missed its tolerance
+ * is still used (the Newton test decides); a non-finite one ends the step
  * unconverged. */
 int pmb_bo_step(pmb_bo* h, double* d_state, double dt, int32_t max_iterations, const pmb_cpr_opts* opts,
                 double* h_stats4);

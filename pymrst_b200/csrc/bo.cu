@@ -1280,9 +1280,10 @@ void BOModel::step(double* x, double dt, int maxit, const pmb_cpr_opts& o, doubl
     if (rc != PMB_OK && rc != PMB_ERR_NOCONV) throw Error(rc, std::string("bo: linear solve failed: ") + pmb_last_error());
     lin_its += info[0];
     if (rc != PMB_OK || info[2] == 0.0) {
-      // a solve this close to exact still makes a Newton update; worse fails the step
+      // the update of a solve that stopped above its tolerance is still used
+      // (the Newton test decides); a non-finite one ends the step
       lin_fail += 1.0;
-      if (!(std::isfinite(info[1]) && info[1] <= 1e-6)) break;
+      if (!std::isfinite(info[1])) break;
     }
     update(x, dx_.get());
   }
