@@ -451,8 +451,12 @@ int pmb_tpfa_levels(const pmb_tpfa* h, int32_t max_levels, int64_t* h_sizes, int
  *   [-satwarn, 1 + satwarn] or produces NaN.  h_out4 = [substeps, time
  *   reached, out-of-range flag, NaN flag].
  * pmb_transport_implicit: backward Euler with Newton, bisection line search
- *   and the substep control of newtonRaphson2ph; linear systems by the CSR
- *   CPR-GMRES with one unknown per cell (opts as pmb_csr_cpr_create).
+ *   and the substep control of newtonRaphson2ph; linear systems by FGMRES
+ *   (rtol, maxiter and restart of opts) preconditioned by a Gauss-Seidel
+ *   sweep in flow order: the cells ordered so that every upwind coupling
+ *   points at an earlier level (exact when the upwind graph has no cycle;
+ *   of two cells coupled both ways the weaker coupling lags), one launch per
+ *   level.
  *   h_out6 = [time reached, substeps, Newton iterations, Krylov iterations,
  *   linear solves that missed their tolerance, last substep length]; the
  *   time reached is below tf when the minimum substep tf 2^-tsref failed.

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "pmb_common.cuh"
+#include "pmb_krylov.cuh"
 
 namespace pmb {
 namespace tr {
@@ -383,6 +384,33 @@ __global__ void tr_neg_kernel(int n, const double* __restrict__ a, double* __res
   if (i < n) b[i] = -a[i];
 }
 
+// y = A x for the scalar CSR Jacobian, a thread per row.
+__global__ void tr_spmv_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                               const double* __restrict__ a, const double* __restrict__ x, double* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) s += a[k] * x[ci[k]];
+  y[i] = s;
+}
+
+// One level of the flow-ordered Gauss-Seidel sweep: for the cells
+// perm[lo .. hi), x_c = (r_c - sum of a_cj x_j over the kept couplings) /
+// a_cc; every kept coupling points at a cell of an earlier level.
+__global__ void tr_flow_gs_level_kernel(int lo, int hi, const int* __restrict__ perm, const int* __restrict__ rp,
+                                        const int* __restrict__ ci, const double* __restrict__ a,
+                                        const unsigned char* __restrict__ keep, const int* __restrict__ dpos,
+                                        const double* __restrict__ r, double* __restrict__ x) {
+  const int t = lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= hi) return;
+  const int c = perm[t];
+  double s = r[c];
+  for (int k = rp[c]; k < rp[c + 1]; ++k)
+    if (keep[k]) s -= a[k] * x[ci[k]];
+  const double d = a[dpos[c]];
+  x[c] = d != 0.0 ? s / d : s;
+}
+
 }  // namespace tr
 }  // namespace pmb
 
@@ -414,7 +442,7 @@ class Transport {
   std::vector<int> h_rp_, h_col_;
   std::vector<double> h_pv_;
   double pvmin_ = 0.0;
-  DArray<int> N_, adj_ptr_, adj_, adj_rank_, diag_rank_, rp_;
+  DArray<int> N_, adj_ptr_, adj_, adj_rank_, diag_rank_, rp_, col_;
   DArray<double> pv_, v_, g_, q_, fmax_, part_, sbuf_, res_, vals_, ds_, rhs_, s0_, base_, out1_;
   DArray<tr::Clock> clock_;
   PinnedArray<tr::Clock> h_clock_;
@@ -424,6 +452,17 @@ class Transport {
   bool flow_set_ = false;
   pmb_csr_cpr* cpr_ = nullptr;
   pmb_cpr_opts cpr_opts_{};
+  // flow-ordered Gauss-Seidel preconditioner of the implicit solves
+  std::vector<int> h_dpos_;
+  DArray<int> dpos_, gs_perm_;
+  DArray<unsigned char> gs_keep_;
+  const double* gs_vals_ = nullptr;
+  std::vector<int> gs_level_ptr_;
+  std::vector<double> h_vals_;
+  Fgmres kry_;
+  void flow_order(const double* d_vals);
+  void flow_gs(const double* r, double* z);
+  bool solve_flow(const double* d_vals, const double* b, double* x, const pmb_cpr_opts& o, double* info);
 };
 
 Transport::Transport(int nc, int nf, const int* h_N, const double* h_pv, cudaStream_t s) : s_(s) {
@@ -464,6 +503,9 @@ Transport::Transport(int nc, int nf, const int* h_N, const double* h_pv, cudaStr
     h_col_.insert(h_col_.end(), cl.begin(), cl.end());
     h_rp_[c + 1] = (int)h_col_.size();
   }
+  h_dpos_.resize(nc);
+  for (int c = 0; c < nc; ++c) h_dpos_[c] = h_rp_[c] + diag_rank[c];
+  dpos_.upload(h_dpos_, s);
   N_.upload(N.empty() ? std::vector<int>{0, 0} : N, s);
   pv_.upload(h_pv_, s);
   adj_ptr_.upload(adj_ptr, s);
@@ -471,6 +513,7 @@ Transport::Transport(int nc, int nf, const int* h_N, const double* h_pv, cudaStr
   adj_rank_.upload(adj_rank.empty() ? std::vector<int>{0} : adj_rank, s);
   diag_rank_.upload(diag_rank, s);
   rp_.upload(h_rp_, s);
+  col_.upload(h_col_, s);
   v_.resize(std::max(nf, 1));
   g_.resize(std::max(nf, 1));
   q_.resize(nc);
@@ -607,10 +650,118 @@ void Transport::explicit_run(double* s, double tf, double dt, double max_dt, dou
   h_out4[3] = hc.nan_seen;
 }
 
+// The flow order of the current Jacobian: cell c depends on each cell j with
+// a_cj != 0 (its upwind neighbours).  Where two cells depend on each other
+// (counter-current gravity flow) only the coupling stronger relative to its
+// row's diagonal is kept; any longer cycle that remains is broken by
+// releasing its lowest-numbered cell.  Levels by Kahn's algorithm.
+void Transport::flow_order(const double* d_vals) {
+  const int nc = w_.nc;
+  const int64_t nnz = this->nnz();
+  h_vals_.resize(nnz);
+  PMB_CUDA(cudaMemcpyAsync(h_vals_.data(), d_vals, sizeof(double) * nnz, cudaMemcpyDeviceToHost, s_));
+  PMB_CUDA(cudaStreamSynchronize(s_));
+  const auto& rp = h_rp_;
+  const auto& ci = h_col_;
+  std::vector<unsigned char> keep(nnz, 0);
+  auto rel = [&](int c, int k) {
+    const double d = std::fabs(h_vals_[h_dpos_[c]]);
+    return std::fabs(h_vals_[k]) / (d > 0.0 ? d : 1.0);
+  };
+  for (int c = 0; c < nc; ++c)
+    for (int k = rp[c]; k < rp[c + 1]; ++k) {
+      const int j = ci[k];
+      if (j == c || h_vals_[k] == 0.0) continue;
+      // the reverse coupling a_jc
+      const int* b = ci.data() + rp[j];
+      const int* e = ci.data() + rp[j + 1];
+      const int* it = std::lower_bound(b, e, c);
+      const int kr = (it != e && *it == c) ? (int)(it - ci.data()) : -1;
+      if (kr >= 0 && h_vals_[kr] != 0.0) {
+        const double mine = rel(c, k), theirs = rel(j, kr);
+        if (mine < theirs || (mine == theirs && c < j)) continue;  // the other direction is kept
+      }
+      keep[k] = 1;
+    }
+  // Kahn: indegree = kept couplings of the row; dependents of j
+  std::vector<int> indeg(nc, 0), dptr(nc + 1, 0), deps;
+  for (int c = 0; c < nc; ++c)
+    for (int k = rp[c]; k < rp[c + 1]; ++k)
+      if (keep[k]) {
+        ++indeg[c];
+        ++dptr[ci[k] + 1];
+      }
+  for (int j = 0; j < nc; ++j) dptr[j + 1] += dptr[j];
+  deps.resize(dptr[nc]);
+  {
+    std::vector<int> fill(dptr.begin(), dptr.end() - 1);
+    for (int c = 0; c < nc; ++c)
+      for (int k = rp[c]; k < rp[c + 1]; ++k)
+        if (keep[k]) deps[fill[ci[k]]++] = c;
+  }
+  std::vector<int> perm, cur, next;
+  std::vector<char> done(nc, 0);
+  perm.reserve(nc);
+  gs_level_ptr_.assign(1, 0);
+  for (int c = 0; c < nc; ++c)
+    if (indeg[c] == 0) cur.push_back(c);
+  int released = 0, lowest = 0;
+  while ((int)perm.size() < nc) {
+    if (cur.empty()) {
+      // a cycle: release the lowest-numbered cell not yet ordered, dropping
+      // its remaining couplings (they lag one sweep)
+      while (done[lowest]) ++lowest;
+      for (int k = rp[lowest]; k < rp[lowest + 1]; ++k) keep[k] = 0;
+      indeg[lowest] = 0;
+      cur.push_back(lowest);
+      ++released;
+    }
+    next.clear();
+    for (int c : cur) {
+      done[c] = 1;
+      perm.push_back(c);
+    }
+    for (int c : cur)
+      for (int q = dptr[c]; q < dptr[c + 1]; ++q) {
+        const int d = deps[q];
+        if (!done[d] && --indeg[d] == 0) next.push_back(d);
+      }
+    gs_level_ptr_.push_back((int)perm.size());
+    std::sort(next.begin(), next.end());
+    cur.swap(next);
+  }
+  gs_perm_.upload(perm, s_);
+  gs_keep_.upload(keep, s_);
+}
+
+void Transport::flow_gs(const double* r, double* z) {
+  const int nlev = (int)gs_level_ptr_.size() - 1;
+  for (int l = 0; l < nlev; ++l) {
+    const int lo = gs_level_ptr_[l], hi = gs_level_ptr_[l + 1];
+    tr::tr_flow_gs_level_kernel<<<(hi - lo + 127) / 128, 128, 0, s_>>>(lo, hi, gs_perm_.get(), rp_.get(),
+                                                                        col_.get(), gs_vals_, gs_keep_.get(),
+                                                                        dpos_.get(), r, z);
+    PMB_CHECK_LAUNCH();
+  }
+}
+
+bool Transport::solve_flow(const double* d_vals, const double* b, double* x, const pmb_cpr_opts& o, double* info) {
+  flow_order(d_vals);
+  gs_vals_ = d_vals;
+  const int nc = w_.nc;
+  if (kry_.n() != nc) kry_.init(nc, std::max(1, std::min(o.restart, kMaxRestart)), s_);
+  auto op = [&](const double* in, double* out) {
+    tr::tr_spmv_kernel<<<(nc + 127) / 128, 128, 0, s_>>>(nc, rp_.get(), col_.get(), d_vals, in, out);
+    PMB_CHECK_LAUNCH();
+  };
+  auto pc = [&](const double* in, double* out) { flow_gs(in, out); };
+  return kry_.solve(op, pc, b, x, o.rtol, o.maxiter, info, nullptr, [] {});
+}
+
 // implicit_transport's loop (:335-402): backward Euler per substep, Newton
-// with a bisection line search, the linear systems solved by the CSR
-// CPR-GMRES (one unknown per cell; the AMG acts on the whole matrix), and
-// the substep control of newtonRaphson2ph.
+// with a bisection line search, the linear systems solved by FGMRES with the
+// flow-ordered Gauss-Seidel sweep, and the substep control of
+// newtonRaphson2ph.
 void Transport::implicit_run(double* s, double tf, double nltol, int lstrials, int maxnewt, int tsref,
                              double resred, const pmb_cpr_opts& o, double* h_out6) {
   PMB_REQUIRE(flow_set_, "transport: set the flow first");
@@ -624,20 +775,13 @@ void Transport::implicit_run(double* s, double tf, double nltol, int lstrials, i
     base_.resize(nc);
     vals_.resize(nnz());
   }
-  if (!cpr_ || std::memcmp(&o, &cpr_opts_, sizeof(o)) != 0) {
-    if (cpr_) pmb_csr_cpr_destroy(cpr_);
-    cpr_ = nullptr;
-    const int rc = pmb_csr_cpr_create(nc, nc, 1, h_rp_.data(), h_col_.data(), 0, &o, s_, &cpr_);
-    if (rc != PMB_OK) throw Error(rc, std::string("transport: linear solver setup failed: ") + pmb_last_error());
-    cpr_opts_ = o;
-  }
+  PMB_REQUIRE(o.rtol > 0.0 && o.maxiter >= 1 && o.restart >= 1, "transport: bad linear-solver options");
   const int nb = (nc + 127) / 128;
   double* sn = sbuf_.get();  // the Newton iterate
   const double mints = tf * std::ldexp(1.0, -tsref);
   double t = 0.0, dt = tf, dtprev = -tf;
   int count = 0;
   long long newton = 0, lin_its = 0, lin_fail = 0, substeps = 0;
-  const double one = 1.0;
   while (t < tf && dt >= mints) {
     dt = std::min(dt, tf - t);
     int it = 0;
@@ -652,15 +796,12 @@ void Transport::implicit_run(double* s, double tf, double nltol, int lstrials, i
       bool linfail = false;
       while (err > nltol && !linfail && it < maxnewt) {
         jacobian(sn, dt, vals_.get());
-        int rc = pmb_csr_cpr_setup(cpr_, vals_.get(), &one);
-        if (rc != PMB_OK) throw Error(rc, std::string("transport: ") + pmb_last_error());
         tr::tr_neg_kernel<<<nb, 128, 0, s_>>>(nc, res_.get(), rhs_.get());
         PMB_CHECK_LAUNCH();
-        double info[4];
-        rc = pmb_csr_cpr_solve(cpr_, rhs_.get(), ds_.get(), info);
-        if (rc != PMB_OK && rc != PMB_ERR_NOCONV) throw Error(rc, std::string("transport: ") + pmb_last_error());
+        double info[4] = {0.0, 0.0, 0.0, 0.0};
+        const bool lin_ok = solve_flow(vals_.get(), rhs_.get(), ds_.get(), o, info);
         lin_its += (long long)info[0];
-        if (rc != PMB_OK) ++lin_fail;
+        if (!lin_ok) ++lin_fail;
         // bisection line search (_linesearch, :405-421)
         const double target = resred * err;
         PMB_CUDA(cudaMemcpyAsync(base_.get(), sn, sizeof(double) * nc, cudaMemcpyDeviceToDevice, s_));

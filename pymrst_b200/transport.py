@@ -7,7 +7,8 @@ gravity, nltol, lstrials, maxnewt, tsref, resred)`, each returning the state
 with `state.s` advanced by tf seconds.
 
 The substeps (explicit: the residual, the stable-step estimate and the
-clock; implicit: residual, Jacobian, CPR-GMRES solve and line-search trials)
+clock; implicit: residual, Jacobian, the FGMRES solve preconditioned by a
+Gauss-Seidel sweep in flow order, and line-search trials)
 run on the device through the `pmb_transport_*` entry points
 (`csrc/transport.cu`).  The host forms what the reference freezes for a
 call: the water source of every cell (`transport_source`), the gravity flux
@@ -270,8 +271,7 @@ def implicit_transport(state, g, tf: float, rock, fluid, wells: Optional[Sequenc
     """Backward-Euler transport over tf seconds: Newton with a bisection
     line search and substep halving / growth."""
     hd, s, params, gvec, internal, keep = _prepare(state, g, rock, fluid, wells, src, bc, gravity)
-    opts = _opts_struct(default_cpr_options(**({"rtol": 1e-12, "maxiter": 500, "local_sweeps": 2,
-                                                "amg_rebuild_interval": 1} | dict(cpr_options or {}))))
+    opts = _opts_struct(default_cpr_options(**({"rtol": 1e-12, "maxiter": 500} | dict(cpr_options or {}))))
     out = (N.C.c_double * 6)()
     N.check(N.lib().pmb_transport_implicit(hd, N.ptr(s), float(tf), float(nltol), int(lstrials), int(maxnewt),
                                            int(tsref), float(resred), N.C.byref(opts), out))
