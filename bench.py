@@ -62,6 +62,8 @@ def parse():
                          "(--dims sets the grid)")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (--workload ensemble)")
     ap.add_argument("--ens-graph", type=int, default=1, help="ensemble: replay each member's preconditioner as a graph")
+    ap.add_argument("--ens-workers", type=int, default=0,
+                    help="ensemble: host threads (0: the autotuned count, cached per SM count and ensemble shape)")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
                     help="mixed: FP32 AMG and smoother blocks inside the FP64 FGMRES (the benchmark's method); fp64: all FP64")
     ap.add_argument("--dims", default=None, help="override grid dims, e.g. 30,110,40")
@@ -602,7 +604,8 @@ def run_ensemble_workload(args):
     """Config 3 (`--workload ensemble`): the seeded realisations (nx, ny in
     16..64, nz in 2..8, an independent lognormal permeability and a five-spot
     each) over `--steps` report steps of 30 days.  GPU: every member on its
-    own model, 16 host threads with a stream each (each member's results are
+    own model, host threads with a stream each (their count autotuned on the
+    first report step of 64 members and cached; each member's results are
     those of its single run), wall time bracketed by device synchronisations
     (the work is spread over many streams); CPU: the oracle (numpy + SuperLU;
     the reference's run_ensemble runs members one after another) on the first
@@ -612,7 +615,7 @@ def run_ensemble_workload(args):
     from oracle import ow as oow
     from pymrst_b200 import cases
     from pymrst_b200.build import build
-    from pymrst_b200.ensemble import simulate_members_concurrently
+    from pymrst_b200.ensemble import simulate_members_concurrently, tune_workers
     from pymrst_b200.ow_model import GpuOilWaterModel
     if int(os.environ.get("RANK", "0")) != 0:
         return
@@ -624,12 +627,13 @@ def run_ensemble_workload(args):
            for c in reals]
     dts = np.full(args.steps, reals[0].dt)
     cells = np.array([c.grid.cells.num for c in reals])
-    simulate_members_concurrently(members[:1], reals[0].fluid, st0[:1], dts[:1], gravity=reals[0].gravity, workers=1,
-                                  replay_graph=bool(args.ens_graph))
+    tuned = tune_workers(members, reals[0].fluid, st0, dts, gravity=reals[0].gravity,
+                         replay_graph=bool(args.ens_graph))
+    workers = args.ens_workers or tuned["workers"]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    _, its = simulate_members_concurrently(members, reals[0].fluid, st0, dts, gravity=reals[0].gravity, workers=16,
-                                           replay_graph=bool(args.ens_graph))
+    _, its = simulate_members_concurrently(members, reals[0].fluid, st0, dts, gravity=reals[0].gravity,
+                                           workers=workers, replay_graph=bool(args.ens_graph))
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     work = float(np.sum(cells[:, None] * its))
@@ -652,8 +656,10 @@ def run_ensemble_workload(args):
             "config": {"workload": f"{args.members} oil-water realisations, nx, ny in 16..64, nz in 2..8, "
                                    f"{args.steps} x 30 days", "cells": int(cells.sum()),
                        "newton_iterations": int(its.sum()),
-                       "runner": "one model per member, 16 threads with a stream each, preconditioner "
+                       "runner": f"one model per member, {workers} threads with a stream each, preconditioner "
                                  + ("replayed as a CUDA graph" if args.ens_graph else "launched kernel by kernel"),
+                       "autotune": {"key": tuned["key"], "workers": tuned["workers"],
+                                    "trial_seconds": {str(k): v for k, v in tuned["trials"].items()}},
                        "timing": "wall clock between device synchronisations"},
             "cpu_baseline": {"value": cpu, "unit": UNIT, "cores": 1, "kind": "port",
                              "sample": f"oracle (numpy, SuperLU) on member 0 ({prob.nc} cells): {cits} Newton "

@@ -331,3 +331,69 @@ def simulate_members_concurrently(members: Sequence, fluid, states0: Sequence[OW
     with ThreadPoolExecutor(max_workers=workers) as pool:
         results = list(pool.map(run, range(len(members))))
     return [r[0] for r in results], np.array([r[1] for r in results])
+
+
+# -- autotuning of the concurrent runner ---------------------------------------------------
+
+def _tune_cache_path():
+    import os
+    from pathlib import Path
+    p = os.environ.get("PMB_TUNE_CACHE")
+    if p:
+        return Path(p)
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return Path(base) / "pymrst_b200" / "autotune.json"
+
+
+def tune_key(members, sm_count: int, replay_graph: bool) -> str:
+    """Cache key: SM count, graph replay, and the ensemble's shape as powers
+    of two (member count, mean cells per member)."""
+    n = len(members)
+    cells = float(np.mean([m[0].cells.num for m in members])) if n else 0.0
+    b = lambda v: int(np.ceil(np.log2(max(v, 1.0))))
+    return f"ensemble_workers/sm{sm_count}/graph{int(bool(replay_graph))}/m2^{b(n)}/c2^{b(cells)}"
+
+
+def tune_workers(members: Sequence, fluid, states0: Sequence[OWState], timesteps: Sequence[float],
+                 gravity: float = 0.0, candidates=(4, 8, 16, 32), sample: int = 64, replay_graph: bool = True,
+                 model_options: Optional[dict] = None, refresh: bool = False) -> dict:
+    """The number of host threads (each with its own stream) for
+    simulate_members_concurrently: every candidate runs the first report
+    step of a sample of the members (wall clock between device
+    synchronisations), and the fastest is cached in a JSON file keyed by
+    `tune_key` (PMB_TUNE_CACHE, else the user's cache folder).  Returns
+    {"workers", "key", "trials" (seconds per candidate, empty when cached)}."""
+    import json
+    import time
+    torch = _torch()
+    sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    key = tune_key(members, sm, replay_graph)
+    path = _tune_cache_path()
+    cache = {}
+    if path.exists():
+        try:
+            cache = json.loads(path.read_text())
+        except (OSError, ValueError):
+            cache = {}
+    if key in cache and not refresh:
+        return {"workers": int(cache[key]["workers"]), "key": key, "trials": {}}
+    k = max(1, min(int(sample), len(members)))
+    trials = {}
+    for w in candidates:
+        w = int(w)
+        if w > k:
+            continue
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        simulate_members_concurrently(members[:k], fluid, states0[:k], list(timesteps)[:1], gravity=gravity,
+                                      workers=w, model_options=model_options, replay_graph=replay_graph)
+        torch.cuda.synchronize()
+        trials[w] = time.perf_counter() - t0
+    best = min(trials, key=trials.get) if trials else 1
+    cache[key] = {"workers": best, "trials": {str(a): b for a, b in trials.items()}}
+    try:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        path.write_text(json.dumps(cache, indent=1, sort_keys=True))
+    except OSError:
+        pass
+    return {"workers": best, "key": key, "trials": trials}

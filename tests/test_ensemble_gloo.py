@@ -73,3 +73,29 @@ def test_two_ranks_gather_the_same_result_as_one_process():
     expect = np.column_stack([_qoi(params[:, k]) for k in range(9)])
     for _, qoi in out:
         np.testing.assert_array_equal(qoi, expect)
+
+
+def test_autotune_cache_key_and_reuse(tmp_path, monkeypatch):
+    """The tuner's cache key buckets the ensemble's shape; a cached entry is
+    returned without trials (no GPU needed for either)."""
+    import json
+    from types import SimpleNamespace
+    from pymrst_b200 import ensemble as ens
+    monkeypatch.setenv("PMB_TUNE_CACHE", str(tmp_path / "t.json"))
+    mem = [(SimpleNamespace(cells=SimpleNamespace(num=3000)), None, None)] * 100
+    key = ens.tune_key(mem, 148, True)
+    assert key == "ensemble_workers/sm148/graph1/m2^7/c2^12"
+    (tmp_path / "t.json").write_text(json.dumps({key: {"workers": 8}}))
+
+    class FakeTorch:
+        class cuda:
+            @staticmethod
+            def current_device():
+                return 0
+
+            @staticmethod
+            def get_device_properties(i):
+                return SimpleNamespace(multi_processor_count=148)
+    monkeypatch.setattr(ens, "_torch", lambda: FakeTorch)
+    out = ens.tune_workers(mem, None, [None] * 100, [1.0])
+    assert out == {"workers": 8, "key": key, "trials": {}}
