@@ -440,7 +440,8 @@ def measure_adjoint(torch, GpuOilWaterModel, cpu_steps=3):
             "cpu": f"oracle forward + adjoint (numpy, SuperLU) over the first {cpu_steps} steps, one core"}
 
 
-def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budget=30.0, cpu=True):
+def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budget=30.0, cpu=True,
+                     cpr_options=None):
     """The three-phase black-oil model with dissolved gas (the seeded
     lattice case of cases.blackoil_box: gas injectors, bhp producers, one
     oil-rate producer) over its seven steps (0.5 to 20 days), the whole
@@ -451,7 +452,7 @@ def measure_blackoil(torch, dims=(100, 100, 10), cpu_dims=(20, 20, 5), cpu_budge
     from pymrst_b200 import cases
     from pymrst_b200.blackoil import GpuBlackOilModel
     case = cases.blackoil_box(dims=dims)
-    model = GpuBlackOilModel(case.grid, case.rock, case.deck, case.wells)
+    model = GpuBlackOilModel(case.grid, case.rock, case.deck, case.wells, cpr_options=cpr_options)
     x0 = model.to_device(case.state)
     warm = x0.clone()
     for dt in case.dts[:2]:
@@ -587,13 +588,23 @@ def measure_transport(torch, n=256, cpu=True, implicit=True):
             "cpu": "oracle (numpy; SuperLU for the implicit systems) on the same flux, one core"}
 
 
+def cpr_overrides(text: str) -> dict:
+    """`--cpr k=v,...` as CPR options."""
+    out = {}
+    for kv in filter(None, text.split(",")):
+        k, v = kv.split("=")
+        out[k] = float(v) if k in ("rtol", "amg_theta", "inner_rtol") else int(v)
+    return out
+
+
 def run_side_workload(args):
     """One of the other configurations' measurements as its own JSON line
     (rank 0, one GPU)."""
     import torch
     dims = tuple(int(v) for v in args.dims.split(",")) if args.dims else None
     if args.workload == "blackoil":
-        out = measure_blackoil(torch, dims=dims or (100, 100, 10), cpu=not args.no_cpu_baseline)
+        out = measure_blackoil(torch, dims=dims or (100, 100, 10), cpu=not args.no_cpu_baseline,
+                               cpr_options=cpr_overrides(args.cpr) or None)
     else:
         out = measure_transport(torch, n=dims[0] if dims else 256, cpu=not args.no_cpu_baseline,
                                 implicit=not args.skip_implicit)
@@ -709,9 +720,7 @@ def run_ours(args):
     copts = dict(rtol=1e-8, maxiter=400, restart=50, amg_rebuild_interval=1_000_000,
                  precision=1 if args.precision == "mixed" else 0, amg_cycle=3, local_sweeps=7,
                  amg_smoother_degree=3, amg_coarse_degree=2, amg_theta=0.1)
-    for kv in filter(None, args.cpr.split(",")):
-        k, v = kv.split("=")
-        copts[k] = float(v) if k in ("rtol", "amg_theta", "inner_rtol") else int(v)
+    copts.update(cpr_overrides(args.cpr))
     model = GpuOilWaterModel(case.grid, case.rock, case.fluid, case.wells, gravity=case.gravity,
                              cpr_options=copts, max_iterations=args.max_newton)
     stream = torch.cuda.current_stream()
