@@ -266,6 +266,26 @@ def kernel_roofline(model, x, x0, dt, torch, N, reps=20):
     N.check(N.lib().pmb_cpr_bytes(s, cb))
     out["amg_cycle"] = dict(seconds=ms.value * 1e-3, bytes=float(cb[0]))
     out["cpr_bytes"] = [float(v) for v in cb]
+    # set-up cost on this Jacobian: a fresh CPR handle (the host aggregation
+    # of the pressure matrix, then the device Galerkin products, block
+    # inverses and smoother bounds), then a refresh with the aggregates kept
+    # (what every Newton iteration of the run pays); wall clock around device
+    # synchronisations, since the first includes host work
+    from pymrst_b200.ow_model import _opts_struct
+    opts = _opts_struct(model.cpr_options)
+    h2 = N.c_vp()
+    N.check(N.lib().pmb_cpr_create(model._handle, N.C.byref(opts), N.C.byref(h2)))
+    try:
+        walls = []
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            N.check(N.lib().pmb_cpr_setup(h2, N.ptr(jac), N.ptr(well), N.ptr(x)))
+            torch.cuda.synchronize()
+            walls.append(time.perf_counter() - t0)
+    finally:
+        N.lib().pmb_cpr_destroy(h2)
+    out["cpr_setup"] = dict(first_s=walls[0], refresh_s=walls[1])
     return out
 
 
@@ -931,7 +951,9 @@ def run_ours(args):
                                   "orthogonalisation_bytes_per_step": orth / args.steps},
                          "kernels": {k: {"ms": v["seconds"] * 1e3, "bytes": v["bytes"],
                                          "GBps": (v["bytes"] / v["seconds"] / 1e9) if v["bytes"] else None}
-                                     for k, v in kr.items() if k != "cpr_bytes"}},
+                                     for k, v in kr.items() if k not in ("cpr_bytes", "cpr_setup")},
+                         "cpr_setup_ms": {"first_with_host_aggregation": kr["cpr_setup"]["first_s"] * 1e3,
+                                          "refresh": kr["cpr_setup"]["refresh_s"] * 1e3}},
             "clocks": clocks.summary(),
         }
         if configs:
