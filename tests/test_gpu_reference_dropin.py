@@ -20,6 +20,7 @@ from pathlib import Path
 
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 from fixtures import load
 
@@ -173,3 +174,79 @@ def test_reference_adoo_simulation_with_the_gpu_cpr_solver_ad():
         pa, pb = np.asarray(a["pressure"]), np.asarray(b["pressure"])
         assert np.abs(pa - pb).max() <= 1e-8 * np.abs(pb).max()
         assert np.abs(np.asarray(a["s"])[:, 0] - np.asarray(b["s"])[:, 0]).max() <= 1e-7
+
+
+def _adoo_case(gravity_on):
+    from pymrst.modules.ad_blackoil.models.two_phase_oil_water_model import TwoPhaseOilWaterModel
+    from pymrst.modules.ad_core.utils.schedule import simple_schedule
+    from pymrst.params.wells_and_bc.vertical_well import vertical_well
+    from pymrst.solvers.init_res_sol import init_res_sol
+    from pymrst.utils.units import DARCY, MILLI
+    G = compute_geometry(cart_grid([10, 8, 3], [100.0, 80.0, 6.0]))
+    rng = np.random.default_rng(0)
+    rock = make_rock(G, np.exp(rng.normal(np.log(100), 0.5, G.cells.num))[:, None] * MILLI * DARCY, 0.2)
+    fluid = init_simple_adi_fluid(mu=np.array([1, 5]) * CENTI * POISE, rho=np.array([1000.0, 800.0]), n=[2, 2],
+                                  c=[1e-5 / BARSA, 1e-5 / BARSA], p_ref=200 * BARSA, phases="wo")
+    rate = 0.2 * float(np.sum(0.2 * G.cells.volumes)) / (100 * DAY)
+    W = vertical_well([], G, rock, 0, 0, None, val=rate, well_type="rate", compi=np.array([1.0, 0.0]), name="I")
+    W = vertical_well(W, G, rock, 9, 7, None, val=150 * BARSA, well_type="bhp", compi=np.array([0.0, 1.0]),
+                      name="P")
+    schedule = simple_schedule(np.full(3, 10 * DAY), W=W)
+
+    def model():
+        m = TwoPhaseOilWaterModel(G, rock, fluid)
+        if gravity_on:
+            m.gravity = np.array([0.0, 0.0, 9.80665])
+        return m
+    return G, model, schedule, init_res_sol(G, 200 * BARSA, np.array([0.1, 0.9]))
+
+
+@pytest.mark.parametrize("gravity_on", [False, True])
+def test_adoo_model_with_device_cell_equations(gravity_on):
+    """The reference's AD-OO oil-water model with its cell equations from
+    the device (use_device_cell_equations): one get_equations call gives the
+    reference's equations (values and every Jacobian block to 1e-12 of the
+    block's largest entry), and the reference's AD-OO simulate_schedule_ad
+    with its direct solver takes the same Newton iterations to the same
+    states as with the reference's own equations."""
+    from pymrst.modules.ad_core.ad_oo.simulate_schedule_ad import simulate_schedule_ad as sim_adoo
+    from pymrst.modules.ad_core.solvers.concrete_solvers import BackslashSolverAD
+    from pymrst_b200.adoo import use_device_cell_equations
+    G, model, schedule, init = _adoo_case(gravity_on)
+    runs = {}
+    for name in ("reference", "device"):
+        m = model() if name == "reference" else use_device_cell_equations(model())
+        _, states, rep = sim_adoo(init, m, schedule, LinearSolver=BackslashSolverAD())
+        runs[name] = (m, states, [r["Iterations"] for r in rep["ControlstepReports"]])
+    (mr, sr, ir), (md, sd, idev) = runs["reference"], runs["device"]
+    assert ir == idev
+    for a, b in zip(sd, sr):
+        pa, pb = np.asarray(a["pressure"]), np.asarray(b["pressure"])
+        assert np.abs(pa - pb).max() <= 1e-9 * np.abs(pb).max()
+        assert np.abs(np.asarray(a["s"])[:, 0] - np.asarray(b["s"])[:, 0]).max() <= 1e-9
+    # one call at a perturbed mid-run state, the facility model prepared for
+    # the control step as the reference's nonlinear solver prepares it
+    from pymrst.modules.ad_core.ad_oo.physical_model import copy_state
+    base = model()
+    forces = dict(base.get_valid_driving_forces())
+    forces.update(base.get_driving_forces(schedule.controls[0]))
+
+    def prepared(mm):
+        mm = mm.validate_model(forces)
+        st = copy_state(sr[1])
+        st["pressure"] = np.asarray(st["pressure"]) + np.linspace(-2.0, 2.0, G.cells.num) * BARSA
+        mm, st = mm.prepare_report_step(st, sr[0], 10 * DAY, forces)
+        mm, st = mm.prepare_timestep(st, sr[0], 10 * DAY, forces)
+        return mm, st
+    mr, st_r = prepared(model())
+    md, st_d = prepared(use_device_cell_equations(model()))
+    pr, _ = mr.get_equations(sr[0], st_r, 10 * DAY, forces, iteration=1)
+    pd, _ = md.get_equations(sr[0], st_d, 10 * DAY, forces, iteration=1)
+    assert pr.equationNames == pd.equationNames and pr.primaryVariables == pd.primaryVariables
+    for er, ed in zip(pr.equations, pd.equations):
+        vr, vd = np.asarray(er.val), np.asarray(ed.val)
+        assert np.abs(vr - vd).max() <= 1e-12 * max(np.abs(vr).max(), 1e-300)
+        for jr, jd in zip(er.jac, ed.jac):
+            jr, jd = sp.csr_array(jr), sp.csr_array(jd)
+            scale = abs(jr).max() if jr.nnz else 1.0
+            assert (abs(jr - jd).max() if (jr - jd).nnz else 0.0) <= 1e-12 * max(scale, 1e-300)
