@@ -261,11 +261,26 @@ def kernel_roofline(model, x, x0, dt, torch, N, reps=20):
     blk = 16 if int(model.cpr_options.get("precision", 0)) == 1 else 32
     sweep_bytes = nnzb * blk + max(nnzb - 3 * nc, 0) * 4 + nc * (16 + 32 + 4)
     out["line_gs_sweep"] = dict(seconds=ms.value * 1e-3 / sweeps, bytes=sweep_bytes)
-    N.check(N.lib().pmb_cpr_time_stage(s, 1, N.ptr(res), N.ptr(z), reps, N.C.byref(ms)))
     cb = (N.C.c_double * 8)()
     N.check(N.lib().pmb_cpr_bytes(s, cb))
-    out["amg_cycle"] = dict(seconds=ms.value * 1e-3, bytes=float(cb[0]))
     out["cpr_bytes"] = [float(v) for v in cb]
+    # one visit of each level (the cycle from that level down), replayed from
+    # a CUDA graph as the solver replays the preconditioner; level 0's visit
+    # is one whole AMG cycle
+    sizes = (N.C.c_int64 * 32)()
+    nl = N.C.c_int32()
+    N.check(N.lib().pmb_cpr_levels(s, 32, sizes, N.C.byref(nl)))
+    levels = []
+    nnz = N.C.c_int64()
+    for lev in range(0, min(nl.value, 32)):
+        N.check(N.lib().pmb_cpr_time_level(s, lev, 50, N.C.byref(ms), N.C.byref(nnz)))
+        levels.append(dict(level=lev, rows=int(sizes[lev]), nnz=int(nnz.value), visit_ms=ms.value))
+    out["amg_levels"] = levels
+    out["amg_cycle"] = dict(seconds=levels[0]["visit_ms"] * 1e-3, bytes=float(cb[0]))
+    # the whole preconditioner (restriction, AMG cycle, prolongation, the line
+    # sweeps), replayed from its graph
+    N.check(N.lib().pmb_cpr_time_stage(s, 3, N.ptr(res), N.ptr(z), reps, N.C.byref(ms)))
+    out["preconditioner"] = dict(seconds=ms.value * 1e-3, bytes=float(cb[0] + sweeps * cb[1] + cb[3]))
     # set-up cost on this Jacobian: a fresh CPR handle (the host aggregation
     # of the pressure matrix, then the device Galerkin products, block
     # inverses and smoother bounds), then a refresh with the aggregates kept
@@ -951,7 +966,8 @@ def run_ours(args):
                                   "orthogonalisation_bytes_per_step": orth / args.steps},
                          "kernels": {k: {"ms": v["seconds"] * 1e3, "bytes": v["bytes"],
                                          "GBps": (v["bytes"] / v["seconds"] / 1e9) if v["bytes"] else None}
-                                     for k, v in kr.items() if k not in ("cpr_bytes", "cpr_setup")},
+                                     for k, v in kr.items() if k not in ("cpr_bytes", "cpr_setup", "amg_levels")},
+                         "amg_level_visits": kr["amg_levels"],
                          "cpr_setup_ms": {"first_with_host_aggregation": kr["cpr_setup"]["first_s"] * 1e3,
                                           "refresh": kr["cpr_setup"]["refresh_s"] * 1e3}},
             "clocks": clocks.summary(),

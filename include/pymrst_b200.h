@@ -247,7 +247,9 @@ int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* h_sizes, int32
  * application of a preconditioner stage on the solver's stream (CUDA events,
  * after one untimed application).  stage 0: the second stage (all local
  * sweeps, updating d_z in place); 1: one AMG cycle on the restricted d_r;
- * 2: the whole preconditioner z = M^{-1} r.  Needs pmb_cpr_setup first. */
+ * 2: the whole preconditioner z = M^{-1} r, launched kernel by kernel; 3:
+ * the same, replayed from its CUDA graph as the solver applies it.  Needs
+ * pmb_cpr_setup first. */
 /* Measurement aid, no counterpart in the reference: algorithmic bytes of the
  * solver's launches on its current hierarchy (every array read or written
  * once per launch, in its storage type), h_out8 = [one AMG cycle, one
@@ -258,6 +260,12 @@ int pmb_cpr_levels(const pmb_cpr* s, int32_t max_levels, int64_t* h_sizes, int32
 int pmb_cpr_bytes(const pmb_cpr* s, double* h_out8);
 int pmb_cpr_time_stage(pmb_cpr* s, int32_t stage, const double* d_r, double* d_z, int32_t reps,
                        double* h_ms);
+/* Diagnostics: the mean time of one visit of AMG level `level` (0 .. the
+ * coarsest; the cycle from that level down, on its own right-hand side,
+ * zero for level 0, replayed `reps` times from a CUDA graph) and the entries
+ * stored for that level (the dense inverse's n * n on the coarsest).
+ * Overwrites the AMG's work vectors; needs pmb_cpr_setup first. */
+int pmb_cpr_time_level(pmb_cpr* s, int32_t level, int32_t reps, double* h_ms, int64_t* h_nnz);
 
 /* A batch of independent models (an ensemble of realisations, run_ensemble,
  * pymrst/modules/ensemble/ensemble_impl.py:49-67, which runs them one after

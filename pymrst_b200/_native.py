@@ -125,6 +125,7 @@ SIGNATURES = {
     "pmb_cpr_levels": (c_int, [c_vp, c_int, P_i64, P_i32]),
     "pmb_cpr_bytes": (c_int, [c_vp, P_dbl]),
     "pmb_cpr_time_stage": (c_int, [c_vp, c_int, c_vp, c_vp, c_int, P_dbl]),
+    "pmb_cpr_time_level": (c_int, [c_vp, c_int, c_int, P_dbl, P_i64]),
     "pmb_ow_step": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_int, P_dbl]),
     "pmb_ow_step_members": (c_int, [c_vp, c_vp, c_vp, c_dbl, c_int, c_int, P_i32, P_i32, P_i32, P_i32, P_dbl]),
     "pmb_csr_cpr_create": (c_int, [c_int, c_int, c_int, P_i32, P_i32, c_int, C.POINTER(CPROpts), c_vp,

@@ -7,9 +7,13 @@
 #include <numeric>
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 #include "pmb_amg.cuh"
 
 namespace pmb {
+
+namespace cg = cooperative_groups;
 
 // ---------------------------------------------------------------------------
 // host: pairwise aggregation and Galerkin structure
@@ -220,8 +224,21 @@ __global__ void diag_kernel(int n, const int* __restrict__ rp, const int* __rest
   atomicMax(lmax_bits, (unsigned long long)__double_as_longlong(g));
 }
 
-__global__ void lmax_from_bits(const unsigned long long* bits, double* lmax) {
-  lmax[0] = __longlong_as_double((long long)bits[0]);
+// The Chebyshev table of a level, after its Gershgorin bound: tab[0] = the
+// bound, tab[1 + 2k], tab[2 + 2k] = the coefficients (c1, c2) of step k.
+// Computed once per refresh, so that a step kernel loads its two
+// coefficients instead of deriving them (a chain of FP64 divisions before
+// its first row could finish).
+constexpr int kMaxChebSteps = 16;
+constexpr int kChebTable = 1 + 2 * kMaxChebSteps;
+
+__device__ __forceinline__ void cheb_coeffs(double lm, int step, double& c1, double& c2);
+
+__global__ void cheb_table_kernel(const unsigned long long* bits, double* tab) {
+  const double lm = __longlong_as_double((long long)bits[0]);
+  const int k = threadIdx.x;
+  if (k == 0) tab[0] = lm;
+  if (k < kMaxChebSteps) cheb_coeffs(lm, k, tab[1 + 2 * k], tab[2 + 2 * k]);
 }
 
 template <class T>
@@ -241,6 +258,44 @@ __device__ __forceinline__ double group_sum(double v) {
 #pragma unroll
   for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// A lane's first two entries of a CSR row (entries rp[i] + sub,
+// + LANES, ...), loaded before the kernel waits on its predecessor grid: a
+// level's matrix is written only when the hierarchy is refreshed, never
+// inside a cycle, so its loads may overlap the predecessor's tail; only the
+// iterate has to wait.  row_sum then folds the row in the same entry order
+// as a plain loop over k.
+template <class T>
+struct RowPre {
+  int k = 0, end = 0, c0 = 0, c1 = 0;
+  T v0 = T(0), v1 = T(0);
+};
+
+template <class T, int LANES>
+__device__ __forceinline__ RowPre<T> row_prefetch(long long i, int sub, const int* __restrict__ rp,
+                                                  const int* __restrict__ ci, const T* __restrict__ a) {
+  RowPre<T> p;
+  p.k = rp[i] + sub;
+  p.end = rp[i + 1];
+  if (p.k < p.end) {
+    p.c0 = ci[p.k];
+    p.v0 = a[p.k];
+  }
+  if (p.k + LANES < p.end) {
+    p.c1 = ci[p.k + LANES];
+    p.v1 = a[p.k + LANES];
+  }
+  return p;
+}
+
+template <class T, int LANES, class F>
+__device__ __forceinline__ double row_sum(const RowPre<T> p, const int* __restrict__ ci, const T* __restrict__ a,
+                                          double acc, F f) {
+  if (p.k < p.end) acc = f(acc, (double)p.v0, p.c0);
+  if (p.k + LANES < p.end) acc = f(acc, (double)p.v1, p.c1);
+  for (int k = p.k + 2 * LANES; k < p.end; k += LANES) acc = f(acc, (double)a[k], ci[k]);
+  return acc;
 }
 
 // Calls f(std::integral_constant<int, L>) with L the row-group width.
@@ -317,26 +372,37 @@ __global__ void __launch_bounds__(256) cheb_step_kernel(int n, const int* __rest
                                                         T* __restrict__ xout, T* __restrict__ d, const double* lmax,
                                                         int step, const int* __restrict__ agg = nullptr,
                                                         const T* __restrict__ xc = nullptr) {
-  pdl_enter();
-  __shared__ double s_c[2];
-  if (threadIdx.x == 0) cheb_coeffs(lmax[0], step, s_c[0], s_c[1]);  // once per block
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long i = t / LANES;
   const int sub = (int)(t % LANES);
+  RowPre<T> p;
+  double di = 0.0;
+  if (i < n) {
+    if (!ZERO) p = row_prefetch<T, LANES>(i, sub, rp, ci, a);
+    if (sub == 0) di = (double)dinv[i];
+  }
+  const double c1 = lmax[1 + 2 * step], c2 = lmax[2 + 2 * step];  // written at the refresh
+  pdl_enter();
+  // the row's own values first, so that they travel with the gathers below
+  double bi = 0.0, dold = 0.0, xi = 0.0;
+  if (i < n && sub == 0) {
+    bi = (double)b[i];
+    if (step != 0) dold = (double)d[i];
+    if (!ZERO) xi = cheb_x<T, PRO>(xin, agg, xc, (int)i);
+  }
   double ax = 0.0;
   if (!ZERO) {
     if (i < n)
-      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES)
-        ax = __fma_rn((double)a[k], cheb_x<T, PRO>(xin, agg, xc, ci[k]), ax);
+      ax = row_sum<T, LANES>(p, ci, a, 0.0, [=](double acc, double v, int j) {
+        return __fma_rn(v, cheb_x<T, PRO>(xin, agg, xc, j), acc);
+      });
     ax = group_sum<LANES>(ax);
   }
-  __syncthreads();
   if (i >= n || sub != 0) return;
-  const double c1 = s_c[0], c2 = s_c[1];
-  const double r = cheb_res((double)b[i], ax, (double)dinv[i]);
-  const double dn = cheb_dir(step, c1, c2, step == 0 ? 0.0 : (double)d[i], r);
+  const double r = cheb_res(bi, ax, di);
+  const double dn = cheb_dir(step, c1, c2, dold, r);
   d[i] = (T)dn;
-  xout[i] = (T)__dadd_rn(ZERO ? 0.0 : cheb_x<T, PRO>(xin, agg, xc, (int)i), dn);
+  xout[i] = (T)__dadd_rn(xi, dn);
 }
 
 // b_c[I] = sum over members i of (b_i - (A x)_i); LANES threads per aggregate
@@ -376,22 +442,34 @@ __global__ void __launch_bounds__(256) restrict_rows_kernel(const int* __restric
                                                             const int* __restrict__ rp, const int* __restrict__ ci,
                                                             const T* __restrict__ a, const T* __restrict__ b,
                                                             const T* __restrict__ x, T* __restrict__ bc) {
-  pdl_enter();
   extern __shared__ double rr_smem[];
+  // the plan, the member lists and the first member rows: loaded before the
+  // wait (none is written inside a cycle)
   const int I0 = blk[blockIdx.x], I1 = blk[blockIdx.x + 1];
   const int m0 = cptr[I0], m1 = cptr[I1];
   const int groups = blockDim.x / LANES;
   const int g = threadIdx.x / LANES, sub = threadIdx.x % LANES;
+  RowPre<T> p;
+  int i = 0;
+  if (m0 + g < m1) {
+    i = cmem[m0 + g];
+    p = row_prefetch<T, LANES>(i, sub, rp, ci, a);
+  }
+  pdl_enter();
   for (int mb = m0; mb < m1; mb += groups) {  // the same trip count for every thread
     const int m = mb + g;
-    int i = 0;
-    double s = 0.0;
+    double s = 0.0, bi = 0.0;
     if (m < m1) {
-      i = cmem[m];
-      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s = __fma_rn(-(double)a[k], (double)x[ci[k]], s);
+      if (mb != m0) {
+        i = cmem[m];
+        p = row_prefetch<T, LANES>(i, sub, rp, ci, a);
+      }
+      if (sub == 0) bi = (double)b[i];
+      s = row_sum<T, LANES>(p, ci, a, 0.0,
+                            [=](double acc, double v, int j) { return __fma_rn(-v, (double)x[j], acc); });
     }
     s = group_sum<LANES>(s);
-    if (m < m1 && sub == 0) rr_smem[m - m0] = __dadd_rn((double)b[i], s);
+    if (m < m1 && sub == 0) rr_smem[m - m0] = __dadd_rn(bi, s);
   }
   __syncthreads();
   for (int I = I0 + threadIdx.x; I < I1; I += blockDim.x) {
@@ -415,6 +493,131 @@ __global__ void copy_kernel(int n, const T* __restrict__ a, T* __restrict__ b) {
   pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = a[i];
+}
+
+// ELL levels (AMGLevel::ell_k > 0) ------------------------------------------
+//
+// One thread per row: the row's slots are loaded together, then the iterate
+// at every column, so a thread has all its loads in flight at once instead
+// of the CSR kernels' chain of row start -> column -> iterate.  The row is
+// summed in slot order, then its overflow entries.
+constexpr int kEllMaxK = 8;
+
+// A row's slots, loaded before the kernel waits on its predecessor (the
+// ELL copy is written only at a refresh); ovf >= 0 names its overflow row.
+template <class T>
+struct EllPre {
+  int c[kEllMaxK];
+  T v[kEllMaxK];
+  int ovf;
+};
+
+template <class T>
+__device__ __forceinline__ void ell_load(EllPre<T>& e, long long n, int i, int K, const int* __restrict__ ecol,
+                                         const T* __restrict__ eval) {
+#pragma unroll
+  for (int k = 0; k < kEllMaxK; ++k)
+    if (k < K) {
+      e.c[k] = ecol[k * n + i];
+      e.v[k] = eval[k * n + i];
+    }
+  e.ovf = -1;
+#pragma unroll
+  for (int k = 0; k < kEllMaxK; ++k)
+    if (k == K - 1 && e.c[k] < 0) {
+      e.ovf = -1 - e.c[k];
+      e.c[k] = i;  // its value is zero
+    }
+}
+
+template <class T, bool PRO, bool NEG>
+__device__ __forceinline__ double ell_sum(const EllPre<T>& e, int K, const int* __restrict__ optr,
+                                          const int* __restrict__ ocol, const T* __restrict__ oval,
+                                          const T* __restrict__ xin, const int* __restrict__ agg,
+                                          const T* __restrict__ xc) {
+  double xv[kEllMaxK];
+#pragma unroll
+  for (int k = 0; k < kEllMaxK; ++k)
+    if (k < K) xv[k] = cheb_x<T, PRO>(xin, agg, xc, e.c[k]);
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kEllMaxK; ++k)
+    if (k < K) s = __fma_rn(NEG ? -(double)e.v[k] : (double)e.v[k], xv[k], s);
+  if (e.ovf >= 0)
+    for (int q = optr[e.ovf]; q < optr[e.ovf + 1]; ++q)
+      s = __fma_rn(NEG ? -(double)oval[q] : (double)oval[q], cheb_x<T, PRO>(xin, agg, xc, ocol[q]), s);
+  return s;
+}
+
+// cheb_step_kernel (non-zero start) on an ELL level: the same row update.
+template <class T, bool PRO>
+__global__ void __launch_bounds__(256) cheb_ell_kernel(int n, int K, const int* __restrict__ ecol,
+                                                       const T* __restrict__ eval, const int* __restrict__ optr,
+                                                       const int* __restrict__ ocol, const T* __restrict__ oval,
+                                                       const T* __restrict__ dinv, const T* __restrict__ b,
+                                                       const T* __restrict__ xin, T* __restrict__ xout,
+                                                       T* __restrict__ d, const double* lmax, int step,
+                                                       const int* __restrict__ agg, const T* __restrict__ xc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  EllPre<T> e;
+  double di = 0.0;
+  if (i < n) {
+    ell_load(e, n, i, K, ecol, eval);
+    di = (double)dinv[i];
+  }
+  const double c1 = lmax[1 + 2 * step], c2 = lmax[2 + 2 * step];
+  pdl_enter();
+  if (i >= n) return;
+  const double bi = (double)b[i];
+  const double dold = step == 0 ? 0.0 : (double)d[i];
+  const double xi = cheb_x<T, PRO>(xin, agg, xc, i);
+  const double ax = ell_sum<T, PRO, false>(e, K, optr, ocol, oval, xin, agg, xc);
+  const double r = cheb_res(bi, ax, di);
+  const double dn = cheb_dir(step, c1, c2, dold, r);
+  d[i] = (T)dn;
+  xout[i] = (T)__dadd_rn(xi, dn);
+}
+
+// rr[i] = b_i - (A x)_i on an ELL level, accumulated as the restriction
+// kernels do (the negated products, then b).
+template <class T>
+__global__ void __launch_bounds__(256) ell_residual_kernel(int n, int K, const int* __restrict__ ecol,
+                                                           const T* __restrict__ eval, const int* __restrict__ optr,
+                                                           const int* __restrict__ ocol,
+                                                           const T* __restrict__ oval, const T* __restrict__ b,
+                                                           const T* __restrict__ x, double* __restrict__ rr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  EllPre<T> e;
+  if (i < n) ell_load(e, n, i, K, ecol, eval);
+  pdl_enter();
+  if (i >= n) return;
+  const double bi = (double)b[i];
+  const double s = ell_sum<T, false, true>(e, K, optr, ocol, oval, x, nullptr, nullptr);
+  rr[i] = __dadd_rn(bi, s);
+}
+
+// bc[I] = the sum of rr over the members of aggregate I, in member order.
+template <class T>
+__global__ void __launch_bounds__(256) aggregate_sum_kernel(int nc, const int* __restrict__ cptr,
+                                                            const int* __restrict__ cmem,
+                                                            const double* __restrict__ rr, T* __restrict__ bc) {
+  pdl_enter();
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nc) return;
+  double v = 0.0;
+  for (int m = cptr[I]; m < cptr[I + 1]; ++m) v = __dadd_rn(v, rr[cmem[m]]);
+  bc[I] = (T)v;
+}
+
+// dst[k] = val[src[k]] (zero where src is -1): the ELL copy's values after a
+// refresh of the CSR values.
+template <class T>
+__global__ void ell_values_kernel(long long total, const int* __restrict__ src, const T* __restrict__ val,
+                                  T* __restrict__ dst) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= total) return;
+  const int j = src[k];
+  dst[k] = j >= 0 ? val[j] : T(0);
 }
 
 // Dense coarsest level (FP64): assemble, invert by Gauss-Jordan with
@@ -598,166 +801,225 @@ __device__ __forceinline__ double group_sum_rt(double v, int lanes) {
 
 // Cluster tail cycle --------------------------------------------------------
 //
-// The V-cycle from level `first` (the first level below the K-cycle levels)
-// down to the dense coarsest solve runs as ONE launch of one thread-block
-// cluster: the steps of the per-step path (Chebyshev steps, member residuals,
-// aggregate sums, the dense coarsest product, the post-smoothing with the
-// prolongation folded into its first step) separated by the hardware cluster
-// barrier instead of kernel boundaries.  Each step uses the same row grouping,
-// summation order and explicit roundings as its per-step kernel, and the
-// same buffers, so the result is bitwise that of the per-step path.  The
-// tail levels are small (the largest a few tens of thousands of rows) and
-// L2-resident; launched per step they are latency-bound, at 5 to 10 us per
-// kernel, and under the K-cycle every cycle visits them 8 times.
-//
-// Vectors written inside the kernel are read with ld.global.cg (L2, never a
-// stale L1 line of another SM); the barrier orders the writes before it.
+// The V-cycle from level `first` (a level below the K-cycle levels) down to
+// the dense coarsest solve, as ONE launch of one thread-block cluster whose
+// shared memory holds those levels.  Every level's rows are split into
+// contiguous chunks, one per CTA; a CTA keeps its rows' matrix entries,
+// vectors and restriction lists in its own shared memory, and reads the
+// other chunks' vector entries through distributed shared memory.  A column
+// (or a member row, or an aggregate) is stored packed as (owning CTA << 16)
+// | row within that CTA's chunk.  The steps of the per-step path (Chebyshev
+// steps, member residuals, aggregate sums, the dense coarsest product, the
+// prolongation and post-smoothing) are separated by the hardware cluster
+// barrier instead of kernel boundaries, with the same row grouping, sum
+// order and explicit roundings as the per-step kernels, so the result is
+// bitwise that of the per-step path.  On these levels a launch per step
+// costs more than its work, and under the K-cycle every cycle visits them 8
+// times; here every dependent load of a step is a shared-memory access.
 constexpr int kTailThreads = 1024;
 constexpr int kTailMaxRows = 65536;
+constexpr int kFusedMaxRows = 65536;  // the largest level of the fused coarse cycle
 
 template <class T>
-struct TailLevel {
-  int n, lanes, steps;
-  const int* rp;
-  const int* ci;
-  const T* val;
-  const T* dinv;
-  const double* lmax;
-  T* b;  // right-hand side (level below the first: written by the restriction)
-  T* x;
-  T* d;  // Chebyshev direction
-  T* t;
-  T* u;
-  const int* cptr;  // members of each aggregate of the next level
-  const int* cmem;
-  const int* agg;
-};
-
-__device__ __forceinline__ void cluster_barrier() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+__device__ __forceinline__ T* ct_sec(unsigned char* base, int off) {
+  return reinterpret_cast<T*>(base + off);
 }
 
-template <class T>
-__device__ __forceinline__ double ldv(const T* p) {
-  return (double)__ldcg(p);
+// The entry `p` (packed) of the section at offset `off`, in its owner's
+// shared memory.
+template <class V>
+__device__ __forceinline__ V ct_remote(cg::cluster_group& cl, unsigned char* base, int off, unsigned p) {
+  V* loc = reinterpret_cast<V*>(base + off) + (p & 0xffffu);
+  return *cl.map_shared_rank(loc, (int)(p >> 16));
 }
 
-template <class T, bool ZERO, bool PRO>
-__device__ void tail_cheb(const TailLevel<T>& L, const T* b, const T* xin, T* xout, int step, const T* xc,
-                          long long tid, long long nthr) {
-  double c1, c2;
-  cheb_coeffs(L.lmax[0], step, c1, c2);
+// One Chebyshev step of level L on the CTA's rows: xout = xin + d,
+// d = c1 d + c2 D^-1 (b - A xin); ZERO: from xin = 0 (no product).
+template <class T, bool ZERO>
+__device__ void ct_step(cg::cluster_group& cl, unsigned char* sm, const CtLevel<T>& L, const CtPart& P, int sin,
+                        int sout, int step) {
+  const double c1 = L.tab[1 + 2 * step], c2 = L.tab[2 + 2 * step];
   const int LN = L.lanes;
-  const long long total = ((long long)L.n * LN + 31) / 32 * 32;
-  for (long long t = tid; t < total; t += nthr) {
-    const long long i = t / LN;
-    const int sub = (int)(t % LN);
+  const int* rp = ct_sec<int>(sm, L.s_rp);
+  const unsigned* col = ct_sec<unsigned>(sm, L.s_col);
+  const T* val = ct_sec<T>(sm, L.s_val);
+  const T* dinv = ct_sec<T>(sm, L.s_dinv);
+  const T* b = ct_sec<T>(sm, L.s_b);
+  const T* xin = ct_sec<T>(sm, sin);
+  T* xout = ct_sec<T>(sm, sout);
+  T* d = ct_sec<T>(sm, L.s_d);
+  const int total = (P.nr * LN + 31) / 32 * 32;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int i = t / LN, sub = t % LN;
     double ax = 0.0;
     if (!ZERO) {
-      if (i < L.n)
-        for (int k = L.rp[i] + sub; k < L.rp[i + 1]; k += LN) {
-          const int j = L.ci[k];
-          const double xv = PRO ? (double)(T)__dadd_rn(ldv(xin + j), ldv(xc + L.agg[j])) : ldv(xin + j);
-          ax = __fma_rn((double)L.val[k], xv, ax);
-        }
+      if (i < P.nr)
+        for (int k = rp[i] + sub; k < rp[i + 1]; k += LN)
+          ax = __fma_rn((double)val[k], (double)ct_remote<T>(cl, sm, sin, col[k]), ax);
       ax = group_sum_rt(ax, LN);
     }
-    if (i < L.n && sub == 0) {
-      const double r = cheb_res(ldv(b + i), ax, (double)L.dinv[i]);
-      const double dn = cheb_dir(step, c1, c2, step == 0 ? 0.0 : ldv(L.d + i), r);
-      double xo = 0.0;
-      if (!ZERO) xo = PRO ? (double)(T)__dadd_rn(ldv(xin + i), ldv(xc + L.agg[i])) : ldv(xin + i);
-      L.d[i] = (T)dn;
-      xout[i] = (T)__dadd_rn(xo, dn);
+    if (i < P.nr && sub == 0) {
+      const double r = cheb_res((double)b[i], ax, (double)dinv[i]);
+      const double dn = cheb_dir(step, c1, c2, step == 0 ? 0.0 : (double)d[i], r);
+      d[i] = (T)dn;
+      xout[i] = (T)__dadd_rn(ZERO ? 0.0 : (double)xin[i], dn);
     }
   }
-  cluster_barrier();
+  cl.sync();
 }
 
-// AMG<T>::smooth, step for step (the same output buffer of every step)
+// AMG<T>::smooth on the CTA's rows, buffer for buffer.
 template <class T>
-__device__ void tail_smooth(const TailLevel<T>& L, const T* b, T* x, bool zero_start, const T* xc, long long tid,
-                            long long nthr) {
+__device__ void ct_smooth(cg::cluster_group& cl, unsigned char* sm, const CtLevel<T>& L, const CtPart& P,
+                          bool zero_start) {
   const int steps = L.steps;
-  T* cur = x;
+  int cur = L.s_x;
   int step = 0;
   if (zero_start) {
-    T* out = (steps % 2 == 1) ? x : L.t;
-    tail_cheb<T, true, false>(L, b, nullptr, out, 0, nullptr, tid, nthr);
+    const int out = (steps % 2 == 1) ? L.s_x : L.s_t;
+    ct_step<T, true>(cl, sm, L, P, L.s_x, out, 0);
     cur = out;
     step = 1;
   }
   for (; step < steps; ++step) {
-    T* out = ((steps - 1 - step) % 2 == 0) ? x : L.t;
-    if (out == cur) out = L.u;
-    if (xc && step == 0)
-      tail_cheb<T, false, true>(L, b, cur, out, step, xc, tid, nthr);
-    else
-      tail_cheb<T, false, false>(L, b, cur, out, step, nullptr, tid, nthr);
+    int out = ((steps - 1 - step) % 2 == 0) ? L.s_x : L.s_t;
+    if (out == cur) out = L.s_u;
+    ct_step<T, false>(cl, sm, L, P, cur, out, step);
     cur = out;
   }
-  if (cur != x) {
-    for (long long i = tid; i < L.n; i += nthr) x[i] = __ldcg(cur + i);
-    cluster_barrier();
+  if (cur != L.s_x) {
+    T* x = ct_sec<T>(sm, L.s_x);
+    const T* c = ct_sec<T>(sm, cur);
+    for (int i = threadIdx.x; i < P.nr; i += blockDim.x) x[i] = c[i];
+    cl.sync();
   }
 }
 
 template <class T>
-__global__ void __launch_bounds__(kTailThreads, 1) amg_tail_kernel(const TailLevel<T>* __restrict__ lv, int nlev,
-                                                                   int nco, const double* __restrict__ co_inv,
-                                                                   T* co_b, T* co_x, const T* b_top, T* x_top,
-                                                                   double* rr) {
-  pdl_enter();
-  const long long nthr = (long long)gridDim.x * blockDim.x;
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kTailThreads, 1)
+    amg_ctail_kernel(const CtLevel<T>* __restrict__ lv, const CtPart* __restrict__ parts, int nlev, CtCoarse co,
+                     const T* b_top, T* x_top) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int me = (int)cl.block_rank();
+  const CtPart* my = parts + (size_t)me * (nlev + 1);  // nlev levels, then the coarsest rows
+  // the hierarchy's entries (written at a refresh, never inside a cycle):
+  // loaded before the wait on the predecessor grid
   for (int j = 0; j < nlev; ++j) {
-    const TailLevel<T> L = lv[j];
-    const T* b = j == 0 ? b_top : L.b;
-    T* x = j == 0 ? x_top : L.x;
-    tail_smooth(L, b, x, true, (const T*)nullptr, tid, nthr);
-    // restrict_rows_kernel: member residuals b_i - (A x)_i ...
-    const int LN = L.lanes;
-    const long long total = ((long long)L.n * LN + 31) / 32 * 32;
-    for (long long t = tid; t < total; t += nthr) {
-      const long long m = t / LN;
-      const int sub = (int)(t % LN);
-      int i = 0;
-      double sres = 0.0;
-      if (m < L.n) {
-        i = L.cmem[m];
-        for (int k = L.rp[i] + sub; k < L.rp[i + 1]; k += LN) sres = __fma_rn(-(double)L.val[k], ldv(x + L.ci[k]), sres);
-      }
-      sres = group_sum_rt(sres, LN);
-      if (m < L.n && sub == 0) rr[m] = __dadd_rn(ldv(b + i), sres);
+    const CtLevel<T>& L = lv[j];
+    const CtPart P = my[j];
+    int* rp = ct_sec<int>(sm, L.s_rp);
+    for (int k = threadIdx.x; k <= P.nr; k += blockDim.x) rp[k] = L.rp[P.r0 + k] - P.z0;
+    unsigned* col = ct_sec<unsigned>(sm, L.s_col);
+    T* val = ct_sec<T>(sm, L.s_val);
+    for (int k = threadIdx.x; k < P.nz; k += blockDim.x) {
+      col[k] = L.pcol[P.z0 + k];
+      val[k] = L.val[P.z0 + k];
     }
-    cluster_barrier();
-    // ... summed per aggregate in member order
-    T* bc = j + 1 < nlev ? lv[j + 1].b : co_b;
-    const int nn = j + 1 < nlev ? lv[j + 1].n : nco;
-    for (long long I = tid; I < nn; I += nthr) {
-      double v = 0.0;
-      for (int m = L.cptr[I]; m < L.cptr[I + 1]; ++m) v = __dadd_rn(v, __ldcg(rr + m));
-      bc[I] = (T)v;
+    T* dinv = ct_sec<T>(sm, L.s_dinv);
+    unsigned* agg = ct_sec<unsigned>(sm, L.s_agg);
+    for (int k = threadIdx.x; k < P.nr; k += blockDim.x) {
+      dinv[k] = L.dinv[P.r0 + k];
+      agg[k] = L.pagg[P.r0 + k];
     }
-    cluster_barrier();
+    int* cptr = ct_sec<int>(sm, L.s_cptr);
+    for (int k = threadIdx.x; k <= P.ncr; k += blockDim.x) cptr[k] = L.cptr[P.R0 + k] - P.m0;
+    unsigned* mem = ct_sec<unsigned>(sm, L.s_mem);
+    for (int k = threadIdx.x; k < P.nm; k += blockDim.x) mem[k] = L.pmem[P.m0 + k];
   }
-  // dense_apply_kernel: one warp per row of the coarsest inverse
+  const CtPart PC = my[nlev];  // coarsest rows [r0, r0 + nr)
   {
-    const long long lane = tid & 31, nwarp = nthr >> 5;
-    for (long long row = tid >> 5; row < nco; row += nwarp) {
-      double sv = 0.0;
-      for (long long jj = lane; jj < nco; jj += 32) sv = __fma_rn(co_inv[row * nco + jj], ldv(co_b + jj), sv);
-      sv = warp_sum(sv);
-      if (lane == 0) co_x[row] = (T)sv;
-    }
-    cluster_barrier();
+    double* inv = ct_sec<double>(sm, co.s_inv);
+    const long long cnt = (long long)PC.nr * co.nco;
+    const double* src = co.inv + (long long)PC.r0 * co.nco;
+    for (long long k = threadIdx.x; k < cnt; k += blockDim.x) inv[k] = src[k];
+    unsigned* pco = ct_sec<unsigned>(sm, co.s_pco);
+    for (int k = threadIdx.x; k < co.nco; k += blockDim.x) pco[k] = co.pco[k];
   }
+  pdl_enter();
+  {
+    const CtLevel<T>& L = lv[0];
+    const CtPart P = my[0];
+    T* b = ct_sec<T>(sm, L.s_b);
+    for (int k = threadIdx.x; k < P.nr; k += blockDim.x) b[k] = b_top[P.r0 + k];
+  }
+  cl.sync();
+  for (int j = 0; j < nlev; ++j) {
+    const CtLevel<T>& L = lv[j];
+    const CtPart P = my[j];
+    ct_smooth(cl, sm, L, P, true);
+    // restrict_rows_kernel: member residuals b_i - (A x)_i of the CTA's rows ...
+    {
+      const int LN = L.lanes;
+      const int* rp = ct_sec<int>(sm, L.s_rp);
+      const unsigned* col = ct_sec<unsigned>(sm, L.s_col);
+      const T* val = ct_sec<T>(sm, L.s_val);
+      const T* b = ct_sec<T>(sm, L.s_b);
+      double* rr = ct_sec<double>(sm, L.s_rr);
+      const int total = (P.nr * LN + 31) / 32 * 32;
+      for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        const int i = t / LN, sub = t % LN;
+        double s = 0.0;
+        if (i < P.nr)
+          for (int k = rp[i] + sub; k < rp[i + 1]; k += LN)
+            s = __fma_rn(-(double)val[k], (double)ct_remote<T>(cl, sm, L.s_x, col[k]), s);
+        s = group_sum_rt(s, LN);
+        if (i < P.nr && sub == 0) rr[i] = __dadd_rn((double)b[i], s);
+      }
+      cl.sync();
+    }
+    // ... summed per aggregate in member order into the next level's b
+    {
+      const int* cptr = ct_sec<int>(sm, L.s_cptr);
+      const unsigned* mem = ct_sec<unsigned>(sm, L.s_mem);
+      T* bc = j + 1 < nlev ? ct_sec<T>(sm, lv[j + 1].s_b) : ct_sec<T>(sm, co.s_b);
+      for (int I = threadIdx.x; I < P.ncr; I += blockDim.x) {
+        double v = 0.0;
+        for (int m = cptr[I]; m < cptr[I + 1]; ++m) v = __dadd_rn(v, ct_remote<double>(cl, sm, L.s_rr, mem[m]));
+        bc[I] = (T)v;
+      }
+      cl.sync();
+    }
+  }
+  // dense_apply_kernel: one warp per row of the coarsest inverse, on the
+  // whole coarse right-hand side gathered into every CTA
+  {
+    const unsigned* pco = ct_sec<unsigned>(sm, co.s_pco);
+    T* bfull = ct_sec<T>(sm, co.s_bfull);
+    for (int k = threadIdx.x; k < co.nco; k += blockDim.x) bfull[k] = ct_remote<T>(cl, sm, co.s_b, pco[k]);
+    __syncthreads();
+    const double* inv = ct_sec<double>(sm, co.s_inv);
+    T* cx = ct_sec<T>(sm, co.s_x);
+    const int lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    for (int r = threadIdx.x >> 5; r < PC.nr; r += nwarp) {
+      double s = 0.0;
+      for (int k = lane; k < co.nco; k += 32) s = __fma_rn(inv[(long long)r * co.nco + k], (double)bfull[k], s);
+      s = warp_sum(s);
+      if (lane == 0) cx[r] = (T)s;
+    }
+    cl.sync();
+  }
+  // post-smoothing from the prolonged correction, back up to the first level
   for (int j = nlev - 1; j >= 0; --j) {
-    const TailLevel<T> L = lv[j];
-    const T* b = j == 0 ? b_top : L.b;
-    T* x = j == 0 ? x_top : L.x;
-    const T* xc = j + 1 < nlev ? lv[j + 1].x : co_x;
-    tail_smooth(L, b, x, false, xc, tid, nthr);  // prolongation folded into the first step
+    const CtLevel<T>& L = lv[j];
+    const CtPart P = my[j];
+    {
+      // prolong_add_kernel: x += P xc (the folded first step of the
+      // per-step path reads these same values)
+      const int sxc = j + 1 < nlev ? lv[j + 1].s_x : co.s_x;
+      T* x = ct_sec<T>(sm, L.s_x);
+      const unsigned* agg = ct_sec<unsigned>(sm, L.s_agg);
+      for (int i = threadIdx.x; i < P.nr; i += blockDim.x)
+        x[i] = (T)__dadd_rn((double)x[i], (double)ct_remote<T>(cl, sm, sxc, agg[i]));
+      cl.sync();
+    }
+    ct_smooth(cl, sm, L, P, false);
+  }
+  {
+    const CtLevel<T>& L = lv[0];
+    const CtPart P = my[0];
+    const T* x = ct_sec<T>(sm, L.s_x);
+    for (int k = threadIdx.x; k < P.nr; k += blockDim.x) x_top[P.r0 + k] = x[k];
   }
 }
 
@@ -806,8 +1068,7 @@ __device__ __forceinline__ void grid_barrier(unsigned int* bar, int* status) {
 template <class T, bool ZERO>
 __device__ void fused_cheb_rows(const CoopLevel<T>& L, const T* b, const T* xin, T* xout, int step, long long tid,
                                 long long nthr) {
-  double c1, c2;
-  cheb_coeffs(L.lmax[0], step, c1, c2);
+  const double c1 = L.lmax[1 + 2 * step], c2 = L.lmax[2 + 2 * step];
   const long long total = ((long long)L.n * L.lanes + 31) / 32 * 32;
   for (long long t = tid; t < total; t += nthr) {
     const long long i = t / L.lanes;
@@ -911,13 +1172,16 @@ template <class T, int LANES>
 __global__ void __launch_bounds__(256) csr_spmv_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                                                        const T* __restrict__ a, const T* __restrict__ x,
                                                        T* __restrict__ y) {
-  pdl_enter();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long i = t / LANES;
   const int sub = (int)(t % LANES);
+  RowPre<T> p;
+  if (i < n) p = row_prefetch<T, LANES>(i, sub, rp, ci, a);  // the matrix, before the wait
+  pdl_enter();
   double s = 0.0;
-  if (i < n)
-    for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) s += (double)a[k] * (double)x[ci[k]];
+  if (i < n) s = row_sum<T, LANES>(p, ci, a, 0.0, [=](double acc, double v, int j) {
+      return __fma_rn(v, (double)x[j], acc);
+    });
   s = group_sum<LANES>(s);
   if (i < n && sub == 0) y[i] = (T)s;
 }
@@ -1018,6 +1282,8 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
     const char* e = std::getenv("PMB_AMG_AGGRESSIVE_BELOW");
     return e ? std::atoi(e) : 0;
   }();
+  PMB_REQUIRE(degree >= 0 && degree <= kMaxChebSteps && coarse_degree >= 0 && coarse_degree <= kMaxChebSteps,
+              "the AMG smoother degree must be at most 16");
   auto H = amg_build_hierarchy(n, h_row_ptr.data(), h_col.data(), h_val.data(), theta, 2, coarse_size, 40,
                                aggressive);
   levels_.clear();
@@ -1070,7 +1336,8 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
     L.cmem.upload(h.cmem, s);
     L.gptr.upload(h.gptr, s);
     L.gidx.upload(h.gidx, s);
-    L.lmax.resize(1);
+    L.lmax.resize(kChebTable);
+    build_ell(L, h, s);
     if (l >= 1) {  // K-cycle work vectors of a coarse level
       L.kc1.resize(L.n);
       L.kc2.resize(L.n);
@@ -1100,101 +1367,249 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
   gj_layout(nco_, gj_rows_, gj_smem_);
   bits_.resize(std::max<size_t>(levels_.size(), 1));
   build_fused(s);
-  build_tail(s);
+  build_tail(H, s);
   PMB_CUDA(cudaStreamSynchronize(s));
 }
 
+// The ELL copy of a level, where it pays: rows of nearly equal length (at
+// most 0.1% longer than the slot count, which is at most kEllMaxK, and the
+// padding at most 30% of the entries), on levels above the sizes the cluster
+// tail and the fused cycle take (those read the CSR arrays and must give the
+// per-step path's bits).  PMB_AMG_ELL=0 keeps every level in CSR.
 template <class T>
-void AMG<T>::build_tail(cudaStream_t s) {
+void AMG<T>::build_ell(AMGLevel<T>& L, const AMGHostLevel& h, cudaStream_t s) {
+  L.ell_k = 0;
+  L.ell_ovf = 0;
+  const char* e = std::getenv("PMB_AMG_ELL");
+  if ((e && e[0] == '0') || L.n <= std::max(kTailMaxRows, kFusedMaxRows)) return;
+  const int n = L.n;
+  std::vector<long long> count(kEllMaxK + 2, 0);  // rows of each length, the last bin longer
+  for (int i = 0; i < n; ++i) ++count[std::min(h.row_ptr[i + 1] - h.row_ptr[i], kEllMaxK + 1)];
+  int K = 0;
+  long long over = 0;  // rows longer than k
+  for (int q = 1; q <= kEllMaxK + 1; ++q) over += count[q];
+  for (int k = 1; k <= kEllMaxK; ++k) {
+    over -= count[k];
+    if (over * 1000 <= n) {
+      K = k;
+      break;
+    }
+  }
+  if (K < 2 || (double)K * n > 1.3 * (double)L.nnz) return;
+  std::vector<int> col((size_t)K * n), src((size_t)K * n), optr(1, 0), ocol, osrc;
+  for (int i = 0; i < n; ++i) {
+    const int a = h.row_ptr[i], len = h.row_ptr[i + 1] - a;
+    const int in_slots = len > K ? K - 1 : len;
+    for (int k = 0; k < K; ++k) {
+      const size_t at = (size_t)k * n + i;
+      if (k < in_slots) {
+        col[at] = h.col[a + k];
+        src[at] = a + k;
+      } else {
+        col[at] = i;
+        src[at] = -1;
+      }
+    }
+    if (len > K) {
+      col[(size_t)(K - 1) * n + i] = -1 - ((int)optr.size() - 1);
+      for (int q = in_slots; q < len; ++q) {
+        ocol.push_back(h.col[a + q]);
+        osrc.push_back(a + q);
+      }
+      optr.push_back((int)ocol.size());
+    }
+  }
+  L.ell_col.upload(col, s);
+  L.ell_src.upload(src, s);
+  L.ell_val.resize((size_t)K * n);
+  L.ell_optr.upload(optr, s);
+  L.ell_ovf = (long long)ocol.size();
+  if (!ocol.empty()) {
+    L.ell_ocol.upload(ocol, s);
+    L.ell_osrc.upload(osrc, s);
+    L.ell_oval.resize(ocol.size());
+  }
+  L.ell_rr.resize(n);
+  L.ell_k = K;
+}
+
+// The cluster tail's layout: from the first level below the K-cycle levels
+// with at most PMB_AMG_TAIL_ROWS rows (at most 65,536; unset or 0: the
+// per-step kernels) whose levels, down to the coarsest, fit the shared
+// memory of a cluster of 16 (else 8) CTAs; a level that does not fit moves
+// the start one level down.
+template <class T>
+void AMG<T>::build_tail(const std::vector<AMGHostLevel>& H, cudaStream_t s) {
   tail_start_ = -1;
   tail_cluster_ = 0;
-  // Off by default: measured on the channelised model (1.12M cells, mixed
-  // precision) with every level below the K-cycle levels in the tail
-  // (29,438 rows and down), one AMG cycle took 2.90 ms against 1.43 ms for
-  // the per-step kernels: 16 SMs move the level of 29k rows far slower than
-  // the whole GPU does.  PMB_AMG_TAIL_ROWS=<n> turns it on for the levels of
-  // at most n rows (n <= 65,536), PMB_AMG_TAIL_CLUSTER=<c> picks the cluster
-  // size (16, 8 or 4).
   const char* e = std::getenv("PMB_AMG_TAIL_ROWS");
   const int max_rows = e ? std::min(std::atoi(e), kTailMaxRows) : 0;
-  if (max_rows <= 0) return;
-  const char* ec = std::getenv("PMB_AMG_TAIL_CLUSTER");
-  const int want_cluster = ec ? std::atoi(ec) : 16;
   const int L = (int)levels_.size();
-  int first = -1;
-  for (int l = std::max(0, k_levels); l < L; ++l)
-    if (levels_[l].n <= max_rows) {
-      first = l;
-      break;
+  if (max_rows <= 0 || L == 0 || nco_ < 1) return;
+  int dev = 0, smem_max = 0;
+  PMB_CUDA(cudaGetDevice(&dev));
+  PMB_CUDA(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  for (int first = std::max(0, k_levels); first < L; ++first) {
+    if (levels_[first].n > max_rows) continue;
+    for (int C : {16, 8}) {
+      // row chunks: level rows balanced by entries, coarsest rows evenly
+      const int nq = L - first;
+      std::vector<std::vector<int>> cut(nq + 1, std::vector<int>(C + 1, 0));
+      for (int q = 0; q < nq; ++q) {
+        const AMGHostLevel& h = H[first + q];
+        const long long nnz = h.row_ptr[h.n];
+        int r = 0;
+        for (int c = 1; c < C; ++c) {
+          const long long want = nnz * c / C;
+          while (r < h.n && h.row_ptr[r] < want) ++r;
+          cut[q][c] = r;
+        }
+        cut[q][C] = h.n;
+      }
+      for (int c = 0; c <= C; ++c) cut[nq][c] = (int)((long long)nco_ * c / C);
+      bool ok = true;
+      for (int q = 0; q <= nq && ok; ++q)
+        for (int c = 0; c < C; ++c)
+          if (cut[q][c + 1] - cut[q][c] > 65535) ok = false;
+      if (!ok) continue;
+      auto pack = [&](int q, int g) -> unsigned {
+        const std::vector<int>& k = cut[q];
+        const int c = (int)(std::upper_bound(k.begin(), k.end(), g) - k.begin()) - 1;
+        return ((unsigned)c << 16) | (unsigned)(g - k[c]);
+      };
+      // shared-memory layout (the largest chunk of every section)
+      size_t off = 0;
+      auto take = [&](size_t bytes) {
+        const size_t at = off;
+        off += (bytes + 15) / 16 * 16;
+        return (int)at;
+      };
+      std::vector<CtLevel<T>> lv(nq);
+      std::vector<CtPart> parts((size_t)C * (nq + 1));
+      for (int q = 0; q < nq; ++q) {
+        const AMGHostLevel& h = H[first + q];
+        int NR = 0, NZ = 0, NC = 0, NM = 0;
+        for (int c = 0; c < C; ++c) {
+          CtPart& P = parts[(size_t)c * (nq + 1) + q];
+          P.r0 = cut[q][c];
+          P.nr = cut[q][c + 1] - P.r0;
+          P.z0 = h.row_ptr[P.r0];
+          P.nz = h.row_ptr[P.r0 + P.nr] - P.z0;
+          P.R0 = cut[q + 1][c];
+          P.ncr = cut[q + 1][c + 1] - P.R0;
+          P.m0 = h.cptr[P.R0];
+          P.nm = h.cptr[P.R0 + P.ncr] - P.m0;
+          NR = std::max(NR, P.nr);
+          NZ = std::max(NZ, P.nz);
+          NC = std::max(NC, P.ncr);
+          NM = std::max(NM, P.nm);
+        }
+        CtLevel<T>& t = lv[q];
+        const AMGLevel<T>& V = levels_[first + q];
+        t.lanes = V.lanes;
+        t.steps = std::max(1, V.degree > 0 ? V.degree : degree);
+        t.s_rp = take(4 * (size_t)(NR + 1));
+        t.s_col = take(4 * (size_t)NZ);
+        t.s_val = take(sizeof(T) * (size_t)NZ);
+        t.s_dinv = take(sizeof(T) * (size_t)NR);
+        t.s_b = take(sizeof(T) * (size_t)NR);
+        t.s_x = take(sizeof(T) * (size_t)NR);
+        t.s_t = take(sizeof(T) * (size_t)NR);
+        t.s_u = take(sizeof(T) * (size_t)NR);
+        t.s_d = take(sizeof(T) * (size_t)NR);
+        t.s_rr = take(8 * (size_t)NR);
+        t.s_agg = take(4 * (size_t)NR);
+        t.s_cptr = take(4 * (size_t)(NC + 1));
+        t.s_mem = take(4 * (size_t)NM);
+      }
+      int NRC = 0;
+      for (int c = 0; c < C; ++c) {
+        CtPart& P = parts[(size_t)c * (nq + 1) + nq];
+        P = CtPart{cut[nq][c], cut[nq][c + 1] - cut[nq][c], 0, 0, 0, 0, 0, 0};
+        NRC = std::max(NRC, P.nr);
+      }
+      CtCoarse co{};
+      co.nco = nco_;
+      co.s_inv = take(8 * (size_t)NRC * nco_);
+      co.s_b = take(sizeof(T) * (size_t)NRC);
+      co.s_x = take(sizeof(T) * (size_t)NRC);
+      co.s_pco = take(4 * (size_t)nco_);
+      co.s_bfull = take(sizeof(T) * (size_t)nco_);
+      if (off > (size_t)smem_max) continue;
+      // the cluster must be schedulable with this shared memory
+      if (C > 8 && cudaFuncSetAttribute(amg_ctail_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                       cudaSuccess) {
+        (void)cudaGetLastError();
+        continue;
+      }
+      if (cudaFuncSetAttribute(amg_ctail_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)off) !=
+          cudaSuccess) {
+        (void)cudaGetLastError();
+        continue;
+      }
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(C);
+      cfg.blockDim = dim3(kTailThreads);
+      cfg.dynamicSmemBytes = off;
+      cudaLaunchAttribute a[1];
+      a[0].id = cudaLaunchAttributeClusterDimension;
+      a[0].val.clusterDim.x = C;
+      a[0].val.clusterDim.y = 1;
+      a[0].val.clusterDim.z = 1;
+      cfg.attrs = a;
+      cfg.numAttrs = 1;
+      int active = 0;
+      if (cudaOccupancyMaxActiveClusters(&active, amg_ctail_kernel<T>, &cfg) != cudaSuccess || active < 1) {
+        (void)cudaGetLastError();
+        continue;
+      }
+      // packed indices on the device
+      for (int q = 0; q < nq; ++q) {
+        const AMGHostLevel& h = H[first + q];
+        AMGLevel<T>& V = levels_[first + q];
+        std::vector<unsigned> pcol(h.col.size()), pagg(h.n), pmem(h.cmem.size());
+        for (size_t k = 0; k < h.col.size(); ++k) pcol[k] = pack(q, h.col[k]);
+        for (int i = 0; i < h.n; ++i) pagg[i] = pack(q + 1, h.agg[i]);
+        for (size_t m = 0; m < h.cmem.size(); ++m) pmem[m] = pack(q, h.cmem[m]);
+        V.ct_pcol.upload(pcol, s);
+        V.ct_pagg.upload(pagg, s);
+        V.ct_pmem.upload(pmem, s);
+        CtLevel<T>& t = lv[q];
+        t.val = V.val.get();
+        t.dinv = V.dinv.get();
+        t.pcol = V.ct_pcol.get();
+        t.rp = V.row_ptr;
+        t.pagg = V.ct_pagg.get();
+        t.cptr = V.cptr.get();
+        t.pmem = V.ct_pmem.get();
+        t.tab = V.lmax.get();
+      }
+      std::vector<unsigned> pco(nco_);
+      for (int g = 0; g < nco_; ++g) pco[g] = pack(nq, g);
+      ct_pco_.upload(pco, s);
+      co.inv = co_inv_.get();
+      co.pco = ct_pco_.get();
+      tail_levels_.resize(sizeof(CtLevel<T>) * lv.size());
+      PMB_CUDA(cudaMemcpyAsync(tail_levels_.get(), lv.data(), sizeof(CtLevel<T>) * lv.size(),
+                               cudaMemcpyHostToDevice, s));
+      tail_parts_.upload(parts, s);
+      tail_co_ = co;
+      tail_smem_ = off;
+      tail_start_ = first;
+      tail_cluster_ = C;
+      return;
     }
-  if (first < 0) return;
-  // 16 CTAs of 1024 threads where the device schedules such a cluster
-  // (a non-portable size), else 8, else 4
-  int cs = 0;
-  for (int c : {16, 8, 4}) {
-    if (c > want_cluster) continue;
-    if (c > 8 && cudaFuncSetAttribute(amg_tail_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-                     cudaSuccess) {
-      (void)cudaGetLastError();
-      continue;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(c);
-    cfg.blockDim = dim3(kTailThreads);
-    cudaLaunchAttribute a[1];
-    a[0].id = cudaLaunchAttributeClusterDimension;
-    a[0].val.clusterDim.x = c;
-    a[0].val.clusterDim.y = 1;
-    a[0].val.clusterDim.z = 1;
-    cfg.attrs = a;
-    cfg.numAttrs = 1;
-    int active = 0;
-    if (cudaOccupancyMaxActiveClusters(&active, amg_tail_kernel<T>, &cfg) == cudaSuccess && active > 0) {
-      cs = c;
-      break;
-    }
-    (void)cudaGetLastError();
   }
-  if (!cs) return;
-  std::vector<TailLevel<T>> h;
-  int maxn = 1;
-  for (int l = first; l < L; ++l) {
-    AMGLevel<T>& V = levels_[l];
-    TailLevel<T> t;
-    t.n = V.n;
-    t.lanes = V.lanes;
-    t.steps = std::max(1, V.degree > 0 ? V.degree : degree);
-    t.rp = V.row_ptr;
-    t.ci = V.col;
-    t.val = V.val.get();
-    t.dinv = V.dinv.get();
-    t.lmax = V.lmax.get();
-    t.b = V.b.get();
-    t.x = V.x.get();
-    t.d = V.r.get();
-    t.t = V.t.get();
-    t.u = V.u.get();
-    t.cptr = V.cptr.get();
-    t.cmem = V.cmem.get();
-    t.agg = V.agg.get();
-    h.push_back(t);
-    maxn = std::max(maxn, V.n);
-  }
-  tail_levels_.resize(sizeof(TailLevel<T>) * h.size());
-  PMB_CUDA(cudaMemcpyAsync(tail_levels_.get(), h.data(), sizeof(TailLevel<T>) * h.size(), cudaMemcpyHostToDevice, s));
-  tail_rr_.resize(maxn);
-  tail_start_ = first;
-  tail_cluster_ = cs;
 }
 
 template <class T>
 void AMG<T>::launch_tail(const T* b, T* x, cudaStream_t s) {
-  const TailLevel<T>* lv = reinterpret_cast<const TailLevel<T>*>(tail_levels_.get());
+  const CtLevel<T>* lv = reinterpret_cast<const CtLevel<T>*>(tail_levels_.get());
   const int nlev = (int)levels_.size() - tail_start_;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(tail_cluster_);
   cfg.blockDim = dim3(kTailThreads);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = tail_smem_;
   cfg.stream = s;
   cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1205,12 +1620,8 @@ void AMG<T>::launch_tail(const T* b, T* x, cudaStream_t s) {
   attr[1].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
   cfg.attrs = attr;
   cfg.numAttrs = 2;
-  int nco = nco_;
-  const double* inv = co_inv_.get();
-  T* cob = co_b_.get();
-  T* cox = co_x_.get();
-  double* rr = tail_rr_.get();
-  PMB_CUDA(cudaLaunchKernelEx(&cfg, amg_tail_kernel<T>, lv, nlev, nco, inv, cob, cox, b, x, rr));
+  const CtPart* parts = tail_parts_.get();
+  PMB_CUDA(cudaLaunchKernelEx(&cfg, amg_ctail_kernel<T>, lv, parts, nlev, tail_co_, b, x));
   PMB_CHECK_LAUNCH();
 }
 
@@ -1219,11 +1630,21 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
   coop_status_ = d_status;
   for (size_t l = 0; l < levels_.size(); ++l) {
     AMGLevel<T>& L = levels_[l];
+    if (L.ell_k > 0) {
+      const long long tot = (long long)L.ell_k * L.n;
+      ell_values_kernel<T><<<grid_for(tot, 256), 256, 0, s>>>(tot, L.ell_src.get(), L.val.get(), L.ell_val.get());
+      PMB_CHECK_LAUNCH();
+      if (L.ell_ovf > 0) {
+        ell_values_kernel<T><<<grid_for(L.ell_ovf, 256), 256, 0, s>>>(L.ell_ovf, L.ell_osrc.get(), L.val.get(),
+                                                                       L.ell_oval.get());
+        PMB_CHECK_LAUNCH();
+      }
+    }
     PMB_CUDA(cudaMemsetAsync(bits_.get() + l, 0, sizeof(unsigned long long), s));
     diag_kernel<T><<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.row_ptr, L.col, L.val.get(), L.dinv.get(),
                                                        bits_.get() + l, d_status);
     PMB_CHECK_LAUNCH();
-    lmax_from_bits<<<1, 1, 0, s>>>(bits_.get() + l, L.lmax.get());
+    cheb_table_kernel<<<1, 32, 0, s>>>(bits_.get() + l, L.lmax.get());
     PMB_CHECK_LAUNCH();
     const bool last = (l + 1 == levels_.size());
     T* cval = last ? co_val_.get() : levels_[l + 1].val.get();
@@ -1265,7 +1686,20 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
     for (; step < steps; ++step) {
       T* out = out_for(step);
       if (out == cur) out = u;
-      if (xc && step == 0)  // x + P xc, folded into the first step
+      if (L.ell_k > 0) {
+        const int ge = grid_for(L.n, 256);
+        const T* oval = L.ell_ovf > 0 ? (const T*)L.ell_oval.get() : (const T*)nullptr;
+        const int* ocol = L.ell_ovf > 0 ? (const int*)L.ell_ocol.get() : (const int*)nullptr;
+        if (xc && step == 0)
+          launch_pdl(cheb_ell_kernel<T, true>, ge, 256, 0, s, L.n, L.ell_k, (const int*)L.ell_col.get(),
+                     (const T*)L.ell_val.get(), (const int*)L.ell_optr.get(), ocol, oval, (const T*)L.dinv.get(), b,
+                     (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step, (const int*)L.agg.get(), xc);
+        else
+          launch_pdl(cheb_ell_kernel<T, false>, ge, 256, 0, s, L.n, L.ell_k, (const int*)L.ell_col.get(),
+                     (const T*)L.ell_val.get(), (const int*)L.ell_optr.get(), ocol, oval, (const T*)L.dinv.get(), b,
+                     (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step, (const int*)nullptr,
+                     (const T*)nullptr);
+      } else if (xc && step == 0)  // x + P xc, folded into the first step
         launch_pdl(cheb_step_kernel<T, false, LN, true>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
                    (const T*)L.dinv.get(), b, (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step,
                    (const int*)L.agg.get(), xc);
@@ -1281,7 +1715,6 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
   }
 }
 
-constexpr int kFusedMaxRows = 65536;
 // Levels below this size fold the prolongation into the first post-smoothing
 // step (one launch less per visit); on larger levels the extra gathers of agg
 // and the correction cost more than the launch.
@@ -1417,17 +1850,26 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
       const char* e = std::getenv("PMB_RESTRICT_ROWS");
       return !(e && e[0] == '0');
     }();
-    with_lanes(L.lanes, [&](auto ln) {
-      constexpr int LN = decltype(ln)::value;
-      if (by_rows)
-        launch_pdl(restrict_rows_kernel<T, LN>, L.rblocks, 256, L.rsmem, s, (const int*)L.rblk.get(),
-                   (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
-                   (const T*)x, bc);
-      else
-        launch_pdl(restrict_residual_kernel<T, LN>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
-                   (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
-                   (const T*)x, bc);
-    });
+    if (L.ell_k > 0) {
+      launch_pdl(ell_residual_kernel<T>, grid_for(L.n, 256), 256, 0, s, L.n, L.ell_k, (const int*)L.ell_col.get(),
+                 (const T*)L.ell_val.get(), (const int*)L.ell_optr.get(),
+                 L.ell_ovf > 0 ? (const int*)L.ell_ocol.get() : (const int*)nullptr,
+                 L.ell_ovf > 0 ? (const T*)L.ell_oval.get() : (const T*)nullptr, b, (const T*)x, L.ell_rr.get());
+      launch_pdl(aggregate_sum_kernel<T>, grid_for(nc, 256), 256, 0, s, nc, (const int*)L.cptr.get(),
+                 (const int*)L.cmem.get(), (const double*)L.ell_rr.get(), bc);
+    } else {
+      with_lanes(L.lanes, [&](auto ln) {
+        constexpr int LN = decltype(ln)::value;
+        if (by_rows)
+          launch_pdl(restrict_rows_kernel<T, LN>, L.rblocks, 256, L.rsmem, s, (const int*)L.rblk.get(),
+                     (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
+                     (const T*)x, bc);
+        else
+          launch_pdl(restrict_residual_kernel<T, LN>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
+                     (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
+                     (const T*)x, bc);
+      });
+    }
   }
   coarse_correction(l, bc, xc, s);
   PhaseTimer pt(level_phase(l, 2), s);
@@ -1484,13 +1926,68 @@ void AMG<T>::apply(const T* b, T* x, cudaStream_t s) {
   cycle(0, b, x, s);
 }
 
+template <class T>
+double AMG<T>::time_visit(int l, int reps, cudaStream_t s) {
+  PMB_REQUIRE(l >= 0 && l <= (int)levels_.size(), "level out of range");
+  PMB_REQUIRE(reps >= 1, "reps must be positive");
+  const bool co = l == (int)levels_.size();
+  T* bw = co ? co_b_.get() : levels_[l].b.get();
+  // level 0's own vectors are not written by a cycle: a zero right-hand side
+  if (l == 0) PMB_CUDA(cudaMemsetAsync(bw, 0, sizeof(T) * levels_[0].n, s));
+  const T* b = bw;
+  T* x = co ? co_x_.get() : levels_[l].x.get();
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  // captured on a private stream (the legacy default stream cannot be
+  // captured), replayed on s
+  cudaStream_t cap = nullptr;
+  PMB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  cudaError_t ce = cudaStreamSynchronize(s);
+  if (ce == cudaSuccess) ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (ce == cudaSuccess) {
+    try {
+      cycle(l, b, x, cap);
+    } catch (...) {
+      cudaStreamEndCapture(cap, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaStreamDestroy(cap);
+      throw;
+    }
+    ce = cudaStreamEndCapture(cap, &g);
+  }
+  cudaStreamDestroy(cap);
+  PMB_CUDA(ce);
+  const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  PMB_CUDA(ie);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float ms = 0.f;
+  cudaError_t err = cudaGraphLaunch(ge, s);
+  if (err == cudaSuccess) err = cudaEventCreate(&e0);
+  if (err == cudaSuccess) err = cudaEventCreate(&e1);
+  if (err == cudaSuccess) err = cudaEventRecord(e0, s);
+  for (int i = 0; i < reps && err == cudaSuccess; ++i) err = cudaGraphLaunch(ge, s);
+  if (err == cudaSuccess) err = cudaEventRecord(e1, s);
+  if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+  if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaGraphExecDestroy(ge);
+  PMB_CUDA(err);
+  return ms / reps;
+}
+
 // Byte model of the launches of cycle() and coarse_correction() above.
 template <class T>
 double AMG<T>::cycle_bytes_from(int l) const {
   const double vb = sizeof(T);
   if (l == (int)levels_.size()) return (double)nco_ * nco_ * 8.0 + 2.0 * nco_ * vb;  // dense_apply_kernel
   const AMGLevel<T>& L = levels_[l];
-  const double n = L.n, mat = (double)L.nnz * (vb + 4.0) + (n + 1.0) * 4.0;
+  const double n = L.n;
+  // the matrix as stored: CSR (values, columns, row starts) or the ELL slots
+  // (padding included) and the overflow entries
+  const double mat = L.ell_k > 0 ? ((double)L.ell_k * n + (double)L.ell_ovf) * (vb + 4.0)
+                                 : (double)L.nnz * (vb + 4.0) + (n + 1.0) * 4.0;
   const int steps = std::max(1, L.degree > 0 ? L.degree : degree);
   const double nc = (l + 1 == (int)levels_.size()) ? nco_ : levels_[l + 1].n;
   // pre-smoothing from zero: the first step reads b and D^-1 and writes d, x
@@ -1500,7 +1997,9 @@ double AMG<T>::cycle_bytes_from(int l) const {
   double bytes = 4.0 * n * vb + (steps - 1) * step;
   // restriction: matrix, b and x of every member row, the member lists, the
   // coarse right-hand side written
-  bytes += mat + 2.0 * n * vb + n * 4.0 + (nc + 1.0) * 4.0 + nc * vb;
+  // (ELL: the member residuals written in FP64 and read back by the
+  // aggregate sums)
+  bytes += mat + 2.0 * n * vb + n * 4.0 + (nc + 1.0) * 4.0 + nc * vb + (L.ell_k > 0 ? 16.0 * n : 0.0);
   bytes += coarse_bytes(l);
   // post-smoothing from the prolonged correction: agg and the coarse
   // correction once (folded into the first step, or a separate launch that
@@ -1533,6 +2032,10 @@ double AMG<T>::refresh_bytes() const {
     // Galerkin gather: every fine value once through its index, the coarse
     // values and their index ranges
     bytes += (double)L.nnz * (vb + 4.0) + nnz_next * (vb + 4.0);
+    // the ELL copy's values: the source index and value of every slot read
+    // (padding: the index only), the slot written
+    if (L.ell_k > 0)
+      bytes += ((double)L.ell_k * L.n + (double)L.ell_ovf) * (4.0 + vb) + (double)L.nnz * vb;
   }
   // dense coarsest matrix assembled and inverted in place
   bytes += (double)co_nnz_ * (vb + 4.0) + 3.0 * (double)nco_ * nco_ * 8.0;

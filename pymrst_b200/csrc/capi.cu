@@ -421,11 +421,20 @@ int pmb_cpr_bytes(const pmb_cpr* s, double* h_out8) {
   });
 }
 
+int pmb_cpr_time_level(pmb_cpr* s, int32_t level, int32_t reps, double* h_ms, int64_t* h_nnz) {
+  return guarded([&] {
+    PMB_REQUIRE(s && h_ms && h_nnz, "NULL argument");
+    long long nnz = 0;
+    *h_ms = s->s->time_level(level, reps, &nnz);
+    *h_nnz = nnz;
+  });
+}
+
 int pmb_cpr_time_stage(pmb_cpr* s, int32_t stage, const double* d_r, double* d_z, int32_t reps,
                        double* h_ms) {
   return guarded([&] {
     PMB_REQUIRE(s && d_r && d_z && h_ms, "NULL argument");
-    PMB_REQUIRE(stage >= 0 && stage <= 2, "stage must be 0, 1 or 2");
+    PMB_REQUIRE(stage >= 0 && stage <= 3, "stage must be 0, 1, 2 or 3");
     PMB_REQUIRE(reps >= 1, "reps must be positive");
     require_aligned(d_r, 16, "r");
     require_aligned(d_z, 16, "z");

@@ -55,6 +55,55 @@ struct AMGLevel {
   int rblocks = 0;
   size_t rsmem = 0;
   int degree = 0;  // Chebyshev degree of this level; 0: the hierarchy's
+  // Slot-major ELL copy of the matrix, on levels whose rows are short and of
+  // nearly equal length (ell_k > 0): entry k of row i at [k * n + i], so that
+  // one thread per row issues all its loads at once and a warp's loads of
+  // one slot are contiguous.  Short rows are padded with their own column
+  // and a zero value.  A row longer than ell_k keeps ell_k - 1 entries in the
+  // slots; its last slot holds -1 - o (o: its overflow row) and value zero,
+  // and the rest of its entries follow in the overflow CSR.
+  int ell_k = 0;
+  DArray<int> ell_col, ell_src;  // ell_src: CSR index of each slot's value (-1: zero)
+  DArray<T> ell_val;
+  DArray<int> ell_optr, ell_ocol, ell_osrc;
+  DArray<T> ell_oval;
+  long long ell_ovf = 0;  // overflow entries
+  DArray<double> ell_rr;  // member residuals of the restriction
+  // cluster tail: packed (CTA << 16 | row in its chunk) columns, aggregates
+  // and member rows
+  DArray<unsigned> ct_pcol, ct_pagg, ct_pmem;
+};
+
+// The cluster tail cycle (amg.cu): the levels from its first one down to
+// the coarsest, resident in the shared memory of one thread-block cluster.
+// One tail level: global sources (loaded at every launch: the values change
+// at every refresh) and the byte offsets of its sections in shared memory
+// (the same in every CTA; each section is sized for the largest chunk).
+template <class T>
+struct CtLevel {
+  int lanes, steps;
+  const T* val;                  // CSR values of the level
+  const T* dinv;
+  const unsigned* pcol;          // packed column of every entry
+  const int* rp;                 // CSR row starts
+  const unsigned* pagg;          // packed aggregate of every row (next level / coarsest)
+  const int* cptr;               // member ranges of the next level's rows
+  const unsigned* pmem;          // packed member rows
+  const double* tab;             // Chebyshev table
+  int s_rp, s_col, s_val, s_dinv, s_b, s_x, s_t, s_u, s_d, s_rr, s_agg, s_cptr, s_mem;
+};
+
+// The chunk of CTA c on a level: rows [r0, r0 + nr), entries [z0, z0 + nz),
+// the next level's rows [R0, R0 + ncr) with members [m0, m0 + nm).
+struct CtPart {
+  int r0, nr, z0, nz, R0, ncr, m0, nm;
+};
+
+struct CtCoarse {
+  int nco;
+  const double* inv;     // dense inverse, row-major
+  const unsigned* pco;   // packed owner of every coarsest row
+  int s_inv, s_b, s_x, s_pco, s_bfull;
 };
 
 // One level as seen by the fused coarse-cycle kernel.
@@ -107,6 +156,10 @@ class AMG {
   double cycle_bytes() const { return num_levels() ? cycle_bytes_from(0) : 0.0; }
   double refresh_bytes() const;
   long long level_nnz(int l) const { return l < (int)levels_.size() ? levels_[l].nnz : co_nnz_; }
+  // Mean time of one visit of level l (the cycle from l down, on the level's
+  // own right-hand side; level 0: the whole cycle on a zero right-hand side),
+  // replayed from a CUDA graph.
+  double time_visit(int l, int reps, cudaStream_t s);
   // The levels from tail_first_level() down (the first level below the
   // K-cycle levels with at most PMB_AMG_TAIL_ROWS rows, and all coarser
   // ones) run as one thread-block-cluster launch per visit
@@ -118,8 +171,11 @@ class AMG {
  private:
   int tail_start_ = -1, tail_cluster_ = 0;
   DArray<unsigned char> tail_levels_;
-  DArray<double> tail_rr_;
-  void build_tail(cudaStream_t s);
+  DArray<CtPart> tail_parts_;
+  DArray<unsigned> ct_pco_;
+  CtCoarse tail_co_{};
+  size_t tail_smem_ = 0;
+  void build_tail(const std::vector<AMGHostLevel>& H, cudaStream_t s);
   void launch_tail(const T* b, T* x, cudaStream_t s);
   double cycle_bytes_from(int l) const;
   double coarse_bytes(int l) const;
@@ -133,6 +189,7 @@ class AMG {
   void coarse_correction(int l, const T* rc, T* ec, cudaStream_t s);
   // xc (non-zero start only): fold x += P xc into the first step
   void smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start, const T* xc = nullptr);
+  void build_ell(AMGLevel<T>& L, const AMGHostLevel& h, cudaStream_t s);
   std::vector<AMGLevel<T>> levels_;
   // coarsest level: dense inverse in FP64
   int nco_ = 0, co_nnz_ = 0;

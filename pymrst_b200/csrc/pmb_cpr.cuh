@@ -23,6 +23,16 @@ class CPRSolver {
   // whole preconditioner, not replayed from a graph), by CUDA events on the
   // solver's stream, after one untimed application.
   double time_stage(int stage, const double* r, double* z, int reps);
+  // One visit of AMG level l >= 1 (graph replay) and the level's stored entries.
+  double time_level(int l, int reps, long long* nnz) {
+    PMB_REQUIRE(o_.use_pressure_stage, "the pressure stage is switched off");
+    if (f32_) {
+      *nnz = amg32_.level_nnz(l);
+      return amg32_.time_visit(l, reps, s_);
+    }
+    *nnz = amg_.level_nnz(l);
+    return amg_.time_visit(l, reps, s_);
+  }
   // Algorithmic bytes (every array read or written once per launch, storage
   // types): [AMG cycle, one second-stage sweep, operator product, pressure
   // restriction + prolongation of one application, one setup without
