@@ -684,21 +684,15 @@ __global__ void line_enter_kernel(int nc, int nw, bool from_z, bool pw, const in
 // sweep) the cell's new z is also written to z in cell order.  The well
 // unknowns are read from z (they stay in cell order).
 template <class BT, class CT, bool OUT>
-__global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3) line_pcr_ell_kernel(OWView v, int lstart, const int* __restrict__ clines,
-                                                                  const int* __restrict__ lptr,
-                                                                  const int* __restrict__ lcells, int nslots,
-                                                                  const BT* __restrict__ blk,
-                                                                  const int* __restrict__ ecol,
-                                                                  const int* __restrict__ epc,
-                                                                  const double* __restrict__ wj,
-                                                                  const double* __restrict__ rl,
-                                                                  double* __restrict__ zl, double* __restrict__ z,
-                                                                  int* status) {
+__global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3)
+    line_pcr_ell_kernel(OWView v, int lstart, const int2* __restrict__ crange, const int* __restrict__ lcells,
+                        int nslots, const BT* __restrict__ blk, const int* __restrict__ ecol,
+                        const int* __restrict__ epc, const double* __restrict__ wj, const double* __restrict__ rl,
+                        double* __restrict__ zl, double* __restrict__ z, int* status) {
   extern __shared__ __align__(16) unsigned char pcr_raw[];
   __shared__ int sBad;
-  const int line = clines[lstart + blockIdx.x];
-  const int t0 = lptr[line];
-  const int len = lptr[line + 1] - t0;
+  const int2 lr = crange[lstart + blockIdx.x];  // (first position, length) of the CTA's line
+  const int t0 = lr.x, len = lr.y;
   const int u = threadIdx.x;
   const bool act = u < len;
   if (u == 0) sBad = 0;
@@ -710,13 +704,27 @@ __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3) line_pcr_
   Blk2<CT> D = {CT(1), CT(0), CT(0), CT(1)}, Lb = zero, Ub = zero;
   Vec2<CT> y = {CT(0), CT(0)};
   double2 zs = z0;
-  if (act) {
-    const int nlat = nslots - 3;
-    int cj[kEllPrefetch];
+  // the lateral columns and the perforation index (written at the set-up,
+  // never inside a solve) are loaded before the wait on the predecessor
+  // grid, so that after it the blocks, r, z and the lateral z gathers all go
+  // out together
+  const int nlat = nslots - 3;
+  const BT bz = blk_store<BT>(make_double4(0.0, 0.0, 0.0, 0.0));
+  int cj[kEllPrefetch];
+  int pc = -1;
 #pragma unroll
-    for (int q = 0; q < kEllPrefetch; ++q) cj[q] = q < nlat ? ecol[q * n + t] : t;
-    // blocks stay in their storage type until used (fewer registers in FP32)
-    const BT bz = blk_store<BT>(make_double4(0.0, 0.0, 0.0, 0.0));
+  for (int q = 0; q < kEllPrefetch; ++q) cj[q] = t;
+  if (act) {
+#pragma unroll
+    for (int q = 0; q < kEllPrefetch; ++q)
+      if (q < nlat) cj[q] = ecol[q * n + t];
+    pc = epc[t];
+  }
+  pdl_enter();
+  if (act) {
+    BT aq[kEllPrefetch];
+#pragma unroll
+    for (int q = 0; q < kEllPrefetch; ++q) aq[q] = q < nlat ? blk[(3 + q) * n + t] : bz;
     const BT Dr = blk[t];
     const BT Lr = u > 0 ? blk[n + t] : bz;
     const BT Ur = u + 1 < len ? blk[2 * n + t] : bz;
@@ -724,16 +732,8 @@ __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3) line_pcr_
     const double2 zlo = u > 0 ? zl2[t - 1] : z0;
     const double2 zup = u + 1 < len ? zl2[t + 1] : z0;
     double2 zq[kEllPrefetch];
-    BT aq[kEllPrefetch];
 #pragma unroll
-    for (int q = 0; q < kEllPrefetch; ++q) {
-      zq[q] = z0;
-      aq[q] = bz;
-      if (q < nlat) {
-        zq[q] = zl2[cj[q]];
-        aq[q] = blk[(3 + q) * n + t];
-      }
-    }
+    for (int q = 0; q < kEllPrefetch; ++q) zq[q] = q < nlat ? zl2[cj[q]] : z0;
     double2 rc = reinterpret_cast<const double2*>(rl)[t];
     double2 m = mv2(ld4(Dr), zs);
     rc.x -= m.x;
@@ -755,7 +755,7 @@ __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3) line_pcr_
       rc.x -= m.x;
       rc.y -= m.y;
     }
-    sub_wells(v, wj, z, epc[t], rc);
+    sub_wells(v, wj, z, pc, rc);
     D = blk_of<CT>(ld4(Dr));
     Lb = blk_of<CT>(ld4(Lr));
     Ub = blk_of<CT>(ld4(Ur));
@@ -776,6 +776,7 @@ __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3) line_pcr_
 __global__ void __launch_bounds__(256) gs_well_kernel(OWView v, const double* __restrict__ wj,
                                                       const double* __restrict__ r, double* __restrict__ z,
                                                       const double* __restrict__ zc, const int* __restrict__ ppos) {
+  pdl_enter();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int k = warp; k < v.nw; k += nwarp) {
     double s0 = 0.0, s1 = 0.0;
@@ -1099,11 +1100,9 @@ void CPRSolver::local_stage(const double* r, double* z, bool entered) {
         const int cnt = Ls.h_color_ptr[q + 1] - Ls.h_color_ptr[q];
         if (cnt <= 0) continue;
         auto go = [&](auto kernel, auto* blk, size_t smem) {
-          kernel<<<cnt, nb, (size_t)nb * smem, s_>>>(v, Ls.h_color_ptr[q], Ls.color_lines.get(), Ls.line_ptr.get(),
-                                                     Ls.line_cells.get(), ell_.slots, blk, ell_.col.get(),
-                                                     ell_.pc.get(), well_, ell_.rl.get(), ell_.zl.get(), z,
-                                                     status_.get());
-          PMB_CHECK_LAUNCH();
+          launch_pdl(kernel, cnt, nb, (size_t)nb * smem, s_, v, Ls.h_color_ptr[q], Ls.color_range.get(),
+                     Ls.line_cells.get(), ell_.slots, blk, ell_.col.get(), ell_.pc.get(), well_, ell_.rl.get(),
+                     ell_.zl.get(), z, status_.get());
         };
         const size_t smem32 = 3 * sizeof(Blk2<float>) + sizeof(Vec2<float>);
         const size_t smem64 = 3 * sizeof(Blk2<double>) + sizeof(Vec2<double>);
@@ -1116,10 +1115,7 @@ void CPRSolver::local_stage(const double* r, double* z, bool entered) {
           out ? go(line_pcr_ell_kernel<double4, double, true>, b64, smem64)
               : go(line_pcr_ell_kernel<double4, double, false>, b64, smem64);
       }
-      if (v.nw) {
-        gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z, ell_.zl.get(), ell_.perf_pos.get());
-        PMB_CHECK_LAUNCH();
-      }
+      if (v.nw) launch_pdl(gs_well_kernel, 1, 256, 0, s_, v, well_, r, z, ell_.zl.get(), ell_.perf_pos.get());
     }
     return;
   }

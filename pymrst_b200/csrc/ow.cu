@@ -1144,6 +1144,9 @@ void OWModel::build_lines(const pmb_ow_desc& d, const std::vector<int>& code) {
   lines_.line_lo.upload(lo, stream_);
   lines_.line_up.upload(up, stream_);
   lines_.color_lines.upload(clines, stream_);
+  std::vector<int2> crange(nl);
+  for (int k = 0; k < nl; ++k) crange[k] = make_int2(line_ptr[clines[k]], line_ptr[clines[k] + 1] - line_ptr[clines[k]]);
+  lines_.color_range.upload(crange, stream_);
 }
 
 void OWModel::update(double* x, const double* dx, double sgn) {

@@ -90,6 +90,7 @@ class OWModel {
     int nlines = 0, max_len = 0;
     std::vector<int> h_color_ptr;  // per colour: range in color_lines
     DArray<int> line_ptr, line_cells, line_lo, line_up, color_lines;
+    DArray<int2> color_range;  // per entry of color_lines: (line_ptr, length) of that line
   };
   const Lines& lines() const { return lines_; }
   bool has_lines() const { return lines_.nlines > 0 && lines_.max_len > 1; }
