@@ -755,6 +755,225 @@ __global__ void __launch_bounds__(kGJThreads) gauss_jordan_kernel(int n, int m, 
     for (int j = lane; j < n; j += 32) Inv[(size_t)i * n + j] = srows[(size_t)i * n + j];
 }
 
+// The same Gauss-Jordan inverse on a thread-block cluster of C CTAs when the
+// working matrix does not fit one CTA's shared memory: CTA c holds rows
+// [c R, c R + R) in its own shared memory and reads the others' through
+// distributed shared memory.  Every step does what gauss_jordan_kernel does,
+// with the same operations on every element (the pivot is the largest |a|
+// of the column, the lowest row on ties, so the cluster agrees on it), so
+// the inverse is bitwise that kernel's.  The cluster barriers are taken by
+// every thread of every CTA in the same order (the branches around them
+// depend only on the pivot, which all CTAs compute alike).
+__global__ void __launch_bounds__(kGJThreads) gauss_jordan_cluster_kernel(int n, int R, const double* __restrict__ M,
+                                                                          double* __restrict__ Inv,
+                                                                          int* __restrict__ status) {
+  extern __shared__ __align__(16) double gjc_smem[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int me = (int)cl.block_rank(), C = (int)cl.num_blocks();
+  double* rows = gjc_smem;                    // R x n, the CTA's rows
+  double* prow = rows + (size_t)R * n;        // n: the scaled pivot row
+  double* tmp = prow + n;                     // n: a row arriving in a swap
+  double* fcol = tmp + n;                     // R: column k of the CTA's rows
+  double* cand = fcol + R;                    // 2: this CTA's pivot candidate (value, row)
+  int* piv = reinterpret_cast<int*>(cand + 2);  // n
+  __shared__ double w_best[kGJThreads / 32];
+  __shared__ int w_idx[kGJThreads / 32];
+  __shared__ int s_p;
+  const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
+  const int r0 = me * R, r1 = min(n, r0 + R);
+  auto row_of = [&](int r) -> double* {  // row r of the matrix, wherever it lives
+    return cl.map_shared_rank(rows + (size_t)(r % R) * n, r / R);
+  };
+  for (int i = r0 + warp; i < r1; i += nwarps)
+    for (int j = lane; j < n; j += 32) rows[(size_t)(i - r0) * n + j] = M[(size_t)i * n + j];
+  cl.sync();
+  for (int k = 0; k < n; ++k) {
+    // the CTA's candidate: the largest |A[i][k]| over its rows i >= k
+    double best = -1.0;
+    int bi = n;
+    for (int i = max(k, r0) + t; i < r1; i += nt) {
+      const double v = fabs(rows[(size_t)(i - r0) * n + k]);
+      if (v > best) {
+        best = v;
+        bi = i;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_down_sync(0xffffffffu, best, o);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      w_best[warp] = best;
+      w_idx[warp] = bi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      best = lane < nwarps ? w_best[lane] : -1.0;
+      bi = lane < nwarps ? w_idx[lane] : n;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (lane == 0) {
+        cand[0] = best;
+        cand[1] = (double)bi;
+      }
+    }
+    cl.sync();
+    // every CTA reduces the candidates alike
+    if (t == 0) {
+      double b = -1.0;
+      int p = n;
+      for (int c = 0; c < C; ++c) {
+        const double* oc = cl.map_shared_rank(cand, c);
+        const double ob = oc[0];
+        const int oi = (int)oc[1];
+        if (ob > b || (ob == b && oi < p)) {
+          b = ob;
+          p = oi;
+        }
+      }
+      if (!(b > 0.0) || !isfinite(b) || p >= n) {
+        if (me == 0) atomicExch(status, PMB_ERR_PIVOT);
+        p = k;
+      }
+      s_p = p;
+      piv[k] = p;
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p != k) {
+      // the owners of rows k and p each copy in the other row, then store it
+      const bool own_k = k >= r0 && k < r1, own_p = p >= r0 && p < r1;
+      if (own_k) {
+        const double* src = row_of(p);
+        for (int j = t; j < n; j += nt) tmp[j] = src[j];
+      }
+      if (own_p && !own_k) {
+        const double* src = row_of(k);
+        for (int j = t; j < n; j += nt) tmp[j] = src[j];
+      }
+      cl.sync();
+      if (own_k && own_p) {
+        double* rk = rows + (size_t)(k - r0) * n;
+        double* rp = rows + (size_t)(p - r0) * n;
+        for (int j = t; j < n; j += nt) {
+          rp[j] = rk[j];
+          rk[j] = tmp[j];
+        }
+      } else if (own_k) {
+        double* rk = rows + (size_t)(k - r0) * n;
+        for (int j = t; j < n; j += nt) rk[j] = tmp[j];
+      } else if (own_p) {
+        double* rp = rows + (size_t)(p - r0) * n;
+        for (int j = t; j < n; j += nt) rp[j] = tmp[j];
+      }
+      cl.sync();
+    }
+    {
+      const double* rk = row_of(k);
+      const double d = rk[k];
+      const double inv_d = (d != 0.0 && isfinite(d)) ? 1.0 / d : 1.0;
+      for (int j = t; j < n; j += nt) prow[j] = j == k ? inv_d : rk[j] * inv_d;
+      for (int i = r0 + t; i < r1; i += nt) fcol[i - r0] = i == k ? 0.0 : rows[(size_t)(i - r0) * n + k];
+    }
+    cl.sync();  // row k is read by every CTA before its owner overwrites it
+    for (int i = r0 + warp; i < r1; i += nwarps) {
+      double* ri = rows + (size_t)(i - r0) * n;
+      if (i == k) {
+        for (int j = lane; j < n; j += 32) ri[j] = prow[j];
+      } else {
+        const double f = fcol[i - r0];
+        for (int j = lane; j < n; j += 32) ri[j] = (j == k ? 0.0 : ri[j]) - f * prow[j];
+      }
+    }
+    __syncthreads();
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    const int p = piv[k];
+    if (p != k)
+      for (int r = r0 + t; r < r1; r += nt) {
+        double* rr = rows + (size_t)(r - r0) * n;
+        const double a = rr[k];
+        rr[k] = rr[p];
+        rr[p] = a;
+      }
+    __syncthreads();
+  }
+  for (int i = r0 + warp; i < r1; i += nwarps)
+    for (int j = lane; j < n; j += 32) Inv[(size_t)i * n + j] = rows[(size_t)(i - r0) * n + j];
+  cl.sync();  // no CTA leaves while another may still read its rows
+}
+
+// Cluster size and shared memory of gauss_jordan_cluster_kernel for n, or 0
+// when one CTA holds the whole matrix or no cluster of at most 8 does.
+static int gj_cluster_layout(int n, size_t& smem) {
+  const char* e = std::getenv("PMB_GJ_CLUSTER");
+  if (e && e[0] == '0') return 0;
+  int dev = 0, optin = 0;
+  PMB_CUDA(cudaGetDevice(&dev));
+  PMB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const long long budget = (long long)optin - 1024;
+  if (3LL * n * sizeof(double) + (long long)n * n * sizeof(double) + (long long)n * sizeof(int) <= budget)
+    return 0;  // one CTA holds it
+  for (int C : {2, 4, 8}) {
+    const int R = (n + C - 1) / C;
+    const long long need = ((long long)R * n + 2LL * n + R + 2) * sizeof(double) + (long long)n * sizeof(int);
+    if (need > budget) continue;
+    if (cudaFuncSetAttribute(gauss_jordan_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)budget) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return 0;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(kGJThreads);
+    cfg.dynamicSmemBytes = (size_t)need;
+    cudaLaunchAttribute a[1];
+    a[0].id = cudaLaunchAttributeClusterDimension;
+    a[0].val.clusterDim.x = C;
+    a[0].val.clusterDim.y = 1;
+    a[0].val.clusterDim.z = 1;
+    cfg.attrs = a;
+    cfg.numAttrs = 1;
+    int active = 0;
+    if (cudaOccupancyMaxActiveClusters(&active, gauss_jordan_cluster_kernel, &cfg) != cudaSuccess || active < 1) {
+      (void)cudaGetLastError();
+      continue;
+    }
+    smem = (size_t)need;
+    return C;
+  }
+  return 0;
+}
+
+static void gj_cluster_launch(int C, size_t smem, int n, const double* a, double* inv, int* d_status,
+                              cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(kGJThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const int R = (n + C - 1) / C;
+  PMB_CUDA(cudaLaunchKernelEx(&cfg, gauss_jordan_cluster_kernel, n, R, a, inv, d_status));
+  PMB_CHECK_LAUNCH();
+}
+
 // Rows of an n x n Gauss-Jordan working matrix that fit in shared memory, and
 // the kernel's dynamic shared memory for them.  The kernel's limit is raised
 // once to the whole opt-in budget (the same value for every caller), so that
@@ -772,6 +991,12 @@ static void gj_layout(int n, int& rows, size_t& smem) {
 }
 
 void dense_inverse(int n, const double* a, double* inv, int* d_status, cudaStream_t s) {
+  size_t csmem = 0;
+  const int C = gj_cluster_layout(n, csmem);
+  if (C > 0) {
+    gj_cluster_launch(C, csmem, n, a, inv, d_status, s);
+    return;
+  }
   int rows = 0;
   size_t smem = 0;
   gj_layout(n, rows, smem);
@@ -1365,6 +1590,7 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
   co_x_.resize(nco_);
   co_b_.resize(nco_);
   gj_layout(nco_, gj_rows_, gj_smem_);
+  gj_cluster_ = gj_cluster_layout(nco_, gj_csmem_);
   bits_.resize(std::max<size_t>(levels_.size(), 1));
   build_fused(s);
   build_tail(H, s);
@@ -1656,8 +1882,12 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
   dense_assemble_kernel<T><<<grid_for(nco_, 128), 128, 0, s>>>(nco_, co_row_ptr_.get(), co_col_.get(),
                                                                 co_val_.get(), co_dense_.get());
   PMB_CHECK_LAUNCH();
-  gauss_jordan_kernel<<<1, kGJThreads, gj_smem_, s>>>(nco_, gj_rows_, co_dense_.get(), co_inv_.get(), d_status);
-  PMB_CHECK_LAUNCH();
+  if (gj_cluster_ > 0) {
+    gj_cluster_launch(gj_cluster_, gj_csmem_, nco_, co_dense_.get(), co_inv_.get(), d_status, s);
+  } else {
+    gauss_jordan_kernel<<<1, kGJThreads, gj_smem_, s>>>(nco_, gj_rows_, co_dense_.get(), co_inv_.get(), d_status);
+    PMB_CHECK_LAUNCH();
+  }
 }
 
 template <class T>

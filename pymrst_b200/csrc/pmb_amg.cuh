@@ -195,6 +195,8 @@ class AMG {
   int nco_ = 0, co_nnz_ = 0;
   int gj_rows_ = 0;     // rows of the coarse inverse's working matrix held in shared memory
   size_t gj_smem_ = 0;  // its dynamic shared memory
+  int gj_cluster_ = 0;  // > 0: the inverse runs on a cluster of this many CTAs
+  size_t gj_csmem_ = 0;
   DArray<int> co_row_ptr_, co_col_;
   DArray<T> co_val_;
   DArray<double> co_dense_, co_inv_;

@@ -1,7 +1,9 @@
 """The AMG coarsest-level solver, `pmb_dense_inverse` (in-place Gauss-Jordan
-with row pivoting in one CTA), against numpy: sizes whose working matrix fits
-in shared memory and sizes that spill rows to global memory, matrices that
-need pivoting, and a singular matrix, which is an error, not a fault."""
+with row pivoting in one CTA, or on a cluster of CTAs when the working
+matrix outgrows one CTA's shared memory), against numpy: sizes whose working
+matrix fits in shared memory, sizes that take a cluster, sizes that spill
+rows to global memory, matrices that need pivoting, and a singular matrix,
+which is an error, not a fault."""
 
 import numpy as np
 import pytest
@@ -51,3 +53,19 @@ def test_singular_matrix_is_an_error_not_a_fault():
     # the library stays usable
     rc, inv = _inverse(np.eye(3) * 2.0)
     assert rc == N.PMB_OK and np.allclose(inv, np.eye(3) * 0.5)
+
+
+@pytest.mark.parametrize("n", [190, 300])
+def test_cluster_inverse_is_bitwise_the_one_cta_inverse(n, monkeypatch):
+    """Matrices too large for one CTA's shared memory are inverted on a
+    cluster (rows split over the CTAs' distributed shared memory); the
+    result equals the one-CTA kernel's (rows spilled to global memory) bit
+    for bit."""
+    rng = np.random.default_rng(100 + n)
+    a = rng.standard_normal((n, n))
+    rc, inv_cluster = _inverse(a)
+    assert rc == N.PMB_OK
+    monkeypatch.setenv("PMB_GJ_CLUSTER", "0")
+    rc, inv_one = _inverse(a)
+    assert rc == N.PMB_OK
+    assert np.array_equal(inv_cluster, inv_one)
