@@ -121,6 +121,51 @@ __global__ void ext_wells_kernel(OWView v, const double* __restrict__ wj, const 
   }
 }
 
+// ext_wells_kernel with a thread per perforation (and one per well for the
+// well's diagonal), for wells that perforate each cell once, so that every
+// perforation owns its two entries: the same values as the serial loop.
+__global__ void ext_wells_par_kernel(OWView v, const double* __restrict__ wj, const double* __restrict__ w,
+                                     const int* __restrict__ perf_cw, const int* __restrict__ perf_wc,
+                                     const int* __restrict__ well_diag, double* __restrict__ ext,
+                                     double* __restrict__ g_perf, double* __restrict__ a_well) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double ww = w[0], wo = w[1];
+  auto well_inverse = [&](int k, double& i00, double& i01, double& i10, double& i11, double& a0, double& a1) {
+    const double* D = wj + v.wl.D + 9LL * k;
+    const double det = D[0] * D[4] - D[1] * D[3];
+    const bool ok = det != 0.0 && isfinite(det);
+    const double id = ok ? 1.0 / det : 0.0;
+    i00 = id * D[4];
+    i01 = -id * D[1];
+    i10 = -id * D[3];
+    i11 = id * D[0];
+    a0 = D[6] * i00 + D[7] * i10;
+    a1 = D[6] * i01 + D[7] * i11;
+  };
+  if (i < v.nperf) {
+    const int k = v.perf_well[i];
+    double i00, i01, i10, i11, a0, a1;
+    well_inverse(k, i00, i01, i10, i11, a0, a1);
+    const double* D = wj + v.wl.D + 9LL * k;
+    const double* C = wj + v.wl.C + 4LL * i;
+    ext[perf_wc[i]] = 0.0 + -(a0 * C[0] + a1 * C[2]);
+    const double* B = wj + v.wl.B + 6LL * i;
+    const double wb0 = ww * B[0] + wo * B[3], wb1 = ww * B[1] + wo * B[4], wb2 = ww * B[2] + wo * B[5];
+    const double g0 = wb0 * i00 + wb1 * i10, g1 = wb0 * i01 + wb1 * i11;
+    g_perf[2 * i] = g0;
+    g_perf[2 * i + 1] = g1;
+    ext[perf_cw[i]] = 0.0 + (wb2 - (g0 * D[2] + g1 * D[5]));
+  }
+  if (i < v.nw) {
+    double i00, i01, i10, i11, a0, a1;
+    well_inverse(i, i00, i01, i10, i11, a0, a1);
+    const double* D = wj + v.wl.D + 9LL * i;
+    a_well[2 * i] = a0;
+    a_well[2 * i + 1] = a1;
+    ext[well_diag[i]] = D[8] - (a0 * D[2] + a1 * D[5]);
+  }
+}
+
 // Right-hand side of the well-augmented pressure system: perforated cells
 // lose g_i r_w[0:2]; well rows get r_ctrl - a r_w[0:2].  Cell rows were
 // written by restrict_p_kernel.
@@ -901,6 +946,11 @@ void CPRSolver::build_pressure_pattern() {
   erp_.upload(h_erp_, s_);
   ecol_.upload(h_ecol_, s_);
   bsr2ext_.upload(bsr2ext, s_);
+  {
+    std::vector<int> e(perf_cw);
+    std::sort(e.begin(), e.end());
+    ext_par_ = std::adjacent_find(e.begin(), e.end()) == e.end();  // no cell perforated twice by one well
+  }
   perf_cw_.upload(perf_cw, s_);
   perf_wc_.upload(perf_wc, s_);
   well_diag_.upload(well_diag, s_);
@@ -1002,7 +1052,11 @@ void CPRSolver::pressure_values(double* ext) {
   ext_cells_kernel<<<grid_for(nnzb, 256), 256, 0, s_>>>(nnzb, reinterpret_cast<const double4*>(jac_), w_.get(),
                                                          bsr2ext_.get(), ext);
   PMB_CHECK_LAUNCH();
-  ext_wells_kernel<<<1, 128, 0, s_>>>(v, well_, w_.get(), perf_cw_.get(), perf_wc_.get(), well_diag_.get(), ext,
+  if (ext_par_)
+    ext_wells_par_kernel<<<grid_for(std::max(v.nperf, v.nw), 128), 128, 0, s_>>>(
+        v, well_, w_.get(), perf_cw_.get(), perf_wc_.get(), well_diag_.get(), ext, g_perf_.get(), a_well_.get());
+  else
+    ext_wells_kernel<<<1, 128, 0, s_>>>(v, well_, w_.get(), perf_cw_.get(), perf_wc_.get(), well_diag_.get(), ext,
                                       g_perf_.get(), a_well_.get());
   PMB_CHECK_LAUNCH();
 }

@@ -91,6 +91,7 @@ class CPRSolver {
   int np_ = 0;
   std::vector<int> h_erp_, h_ecol_;
   DArray<int> erp_, ecol_, bsr2ext_, perf_cw_, perf_wc_, well_diag_;
+  bool ext_par_ = false;  // the pressure system's well entries by a thread per perforation
   DArray<double> g_perf_, a_well_;
   void build_pressure_pattern();
   void pressure_values(double* ext);
