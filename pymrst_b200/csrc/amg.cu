@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <numeric>
 #include <type_traits>
+#include <unordered_map>
 
 #include <cooperative_groups.h>
 
@@ -499,9 +500,11 @@ __global__ void copy_kernel(int n, const T* __restrict__ a, T* __restrict__ b) {
 //
 // One thread per row: the row's slots are loaded together, then the iterate
 // at every column, so a thread has all its loads in flight at once instead
-// of the CSR kernels' chain of row start -> column -> iterate.  The row is
-// summed in slot order, then its overflow entries.
-constexpr int kEllMaxK = 8;
+// of the CSR kernels' chain of row start -> column -> iterate.  In the
+// diagonal form (a level whose entries lie on a few column offsets, as a
+// structured grid's do) slot k of row i is column i + off[k], so the iterate
+// gathers need no column load at all.  The row is summed in slot order,
+// then its overflow entries.
 
 // A row's slots, loaded before the kernel waits on its predecessor (the
 // ELL copy is written only at a refresh); ovf >= 0 names its overflow row.
@@ -513,14 +516,20 @@ struct EllPre {
 };
 
 template <class T>
-__device__ __forceinline__ void ell_load(EllPre<T>& e, long long n, int i, int K, const int* __restrict__ ecol,
-                                         const T* __restrict__ eval) {
+__device__ __forceinline__ void ell_load(EllPre<T>& e, int i, const EllView<T>& E) {
+  const long long n = E.n;
+  const int K = E.K;
 #pragma unroll
-  for (int k = 0; k < kEllMaxK; ++k)
-    if (k < K) {
-      e.c[k] = ecol[k * n + i];
-      e.v[k] = eval[k * n + i];
-    }
+  for (int k = 0; k < kEllMaxK; ++k) e.v[k] = k < K ? E.val[k * n + i] : T(0);
+  if (E.col == nullptr) {
+    // padded slots hold zero: any column in range will do for them
+#pragma unroll
+    for (int k = 0; k < kEllMaxK; ++k) e.c[k] = k < K ? min(max(i + E.off[k], 0), E.n - 1) : i;
+    e.ovf = E.orow[i];
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < kEllMaxK; ++k) e.c[k] = k < K ? E.col[k * n + i] : i;
   e.ovf = -1;
 #pragma unroll
   for (int k = 0; k < kEllMaxK; ++k)
@@ -531,10 +540,9 @@ __device__ __forceinline__ void ell_load(EllPre<T>& e, long long n, int i, int K
 }
 
 template <class T, bool PRO, bool NEG>
-__device__ __forceinline__ double ell_sum(const EllPre<T>& e, int K, const int* __restrict__ optr,
-                                          const int* __restrict__ ocol, const T* __restrict__ oval,
-                                          const T* __restrict__ xin, const int* __restrict__ agg,
-                                          const T* __restrict__ xc) {
+__device__ __forceinline__ double ell_sum(const EllPre<T>& e, const EllView<T>& E, const T* __restrict__ xin,
+                                          const int* __restrict__ agg, const T* __restrict__ xc) {
+  const int K = E.K;
   double xv[kEllMaxK];
 #pragma unroll
   for (int k = 0; k < kEllMaxK; ++k)
@@ -544,25 +552,24 @@ __device__ __forceinline__ double ell_sum(const EllPre<T>& e, int K, const int* 
   for (int k = 0; k < kEllMaxK; ++k)
     if (k < K) s = __fma_rn(NEG ? -(double)e.v[k] : (double)e.v[k], xv[k], s);
   if (e.ovf >= 0)
-    for (int q = optr[e.ovf]; q < optr[e.ovf + 1]; ++q)
-      s = __fma_rn(NEG ? -(double)oval[q] : (double)oval[q], cheb_x<T, PRO>(xin, agg, xc, ocol[q]), s);
+    for (int q = E.optr[e.ovf]; q < E.optr[e.ovf + 1]; ++q)
+      s = __fma_rn(NEG ? -(double)E.oval[q] : (double)E.oval[q], cheb_x<T, PRO>(xin, agg, xc, E.ocol[q]), s);
   return s;
 }
 
 // cheb_step_kernel (non-zero start) on an ELL level: the same row update.
 template <class T, bool PRO>
-__global__ void __launch_bounds__(256) cheb_ell_kernel(int n, int K, const int* __restrict__ ecol,
-                                                       const T* __restrict__ eval, const int* __restrict__ optr,
-                                                       const int* __restrict__ ocol, const T* __restrict__ oval,
-                                                       const T* __restrict__ dinv, const T* __restrict__ b,
-                                                       const T* __restrict__ xin, T* __restrict__ xout,
-                                                       T* __restrict__ d, const double* lmax, int step,
-                                                       const int* __restrict__ agg, const T* __restrict__ xc) {
+__global__ void __launch_bounds__(256) cheb_ell_kernel(EllView<T> E, const T* __restrict__ dinv,
+                                                       const T* __restrict__ b, const T* __restrict__ xin,
+                                                       T* __restrict__ xout, T* __restrict__ d, const double* lmax,
+                                                       int step, const int* __restrict__ agg,
+                                                       const T* __restrict__ xc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = E.n;
   EllPre<T> e;
   double di = 0.0;
   if (i < n) {
-    ell_load(e, n, i, K, ecol, eval);
+    ell_load(e, i, E);
     di = (double)dinv[i];
   }
   const double c1 = lmax[1 + 2 * step], c2 = lmax[2 + 2 * step];
@@ -571,7 +578,7 @@ __global__ void __launch_bounds__(256) cheb_ell_kernel(int n, int K, const int* 
   const double bi = (double)b[i];
   const double dold = step == 0 ? 0.0 : (double)d[i];
   const double xi = cheb_x<T, PRO>(xin, agg, xc, i);
-  const double ax = ell_sum<T, PRO, false>(e, K, optr, ocol, oval, xin, agg, xc);
+  const double ax = ell_sum<T, PRO, false>(e, E, xin, agg, xc);
   const double r = cheb_res(bi, ax, di);
   const double dn = cheb_dir(step, c1, c2, dold, r);
   d[i] = (T)dn;
@@ -581,18 +588,15 @@ __global__ void __launch_bounds__(256) cheb_ell_kernel(int n, int K, const int* 
 // rr[i] = b_i - (A x)_i on an ELL level, accumulated as the restriction
 // kernels do (the negated products, then b).
 template <class T>
-__global__ void __launch_bounds__(256) ell_residual_kernel(int n, int K, const int* __restrict__ ecol,
-                                                           const T* __restrict__ eval, const int* __restrict__ optr,
-                                                           const int* __restrict__ ocol,
-                                                           const T* __restrict__ oval, const T* __restrict__ b,
+__global__ void __launch_bounds__(256) ell_residual_kernel(EllView<T> E, const T* __restrict__ b,
                                                            const T* __restrict__ x, double* __restrict__ rr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   EllPre<T> e;
-  if (i < n) ell_load(e, n, i, K, ecol, eval);
+  if (i < E.n) ell_load(e, i, E);
   pdl_enter();
-  if (i >= n) return;
+  if (i >= E.n) return;
   const double bi = (double)b[i];
-  const double s = ell_sum<T, false, true>(e, K, optr, ocol, oval, x, nullptr, nullptr);
+  const double s = ell_sum<T, false, true>(e, E, x, nullptr, nullptr);
   rr[i] = __dadd_rn(bi, s);
 }
 
@@ -1597,18 +1601,93 @@ void AMG<T>::build(int n, const std::vector<int>& h_row_ptr, const std::vector<i
   PMB_CUDA(cudaStreamSynchronize(s));
 }
 
+template <class T>
+static EllView<T> ell_view(const AMGLevel<T>& L) {
+  EllView<T> E;
+  E.n = L.n;
+  E.K = L.ell_k;
+  E.col = L.ell_dia ? nullptr : L.ell_col.get();
+  E.val = L.ell_val.get();
+  E.orow = L.ell_dia ? L.ell_orow.get() : nullptr;
+  E.optr = L.ell_optr.get();
+  E.ocol = L.ell_ovf > 0 ? L.ell_ocol.get() : nullptr;
+  E.oval = L.ell_ovf > 0 ? L.ell_oval.get() : nullptr;
+  for (int k = 0; k < kEllMaxK; ++k) E.off[k] = L.ell_off[k];
+  return E;
+}
+
 // The ELL copy of a level, where it pays: rows of nearly equal length (at
 // most 0.1% longer than the slot count, which is at most kEllMaxK, and the
 // padding at most 30% of the entries), on levels above the sizes the cluster
 // tail and the fused cycle take (those read the CSR arrays and must give the
-// per-step path's bits).  PMB_AMG_ELL=0 keeps every level in CSR.
+// per-step path's bits).  The diagonal form is taken where it fits, the
+// column form otherwise.  PMB_AMG_ELL=0 keeps every level in CSR,
+// PMB_AMG_ELL=1 allows only the column form.
 template <class T>
 void AMG<T>::build_ell(AMGLevel<T>& L, const AMGHostLevel& h, cudaStream_t s) {
   L.ell_k = 0;
   L.ell_ovf = 0;
+  L.ell_dia = false;
   const char* e = std::getenv("PMB_AMG_ELL");
   if ((e && e[0] == '0') || L.n <= std::max(kTailMaxRows, kFusedMaxRows)) return;
   const int n = L.n;
+  const long long nnz = h.row_ptr[n];
+  if (!(e && e[0] == '1')) {
+    // diagonal form: the fewest column offsets, most frequent first, that
+    // hold all but 0.1% of the entries, with at most 0.1% of the rows
+    // reaching off them and at most 30% padding
+    std::unordered_map<int, long long> freq;
+    for (int i = 0; i < n; ++i)
+      for (int k = h.row_ptr[i]; k < h.row_ptr[i + 1]; ++k) ++freq[h.col[k] - i];
+    std::vector<std::pair<long long, int>> byf;
+    for (const auto& kv : freq) byf.push_back({kv.second, kv.first});
+    std::sort(byf.begin(), byf.end(), [](const std::pair<long long, int>& a, const std::pair<long long, int>& b) {
+      return a.first != b.first ? a.first > b.first : a.second < b.second;
+    });
+    long long covered = 0;
+    for (int K = 1; K <= std::min<int>(kEllMaxK, (int)byf.size()); ++K) {
+      covered += byf[K - 1].first;
+      if ((nnz - covered) * 1000 > nnz || (double)K * n > 1.3 * (double)nnz) continue;
+      std::vector<int> off(K);
+      for (int k = 0; k < K; ++k) off[k] = byf[k].second;
+      std::sort(off.begin(), off.end());
+      std::vector<int> src((size_t)K * n, -1), orow(n, -1), optr(1, 0), ocol, osrc;
+      for (int i = 0; i < n; ++i) {
+        bool extra = false;
+        for (int q = h.row_ptr[i]; q < h.row_ptr[i + 1]; ++q) {
+          const int d = h.col[q] - i;
+          const int slot = (int)(std::find(off.begin(), off.end(), d) - off.begin());
+          if (slot < K) {
+            src[(size_t)slot * n + i] = q;
+          } else {
+            ocol.push_back(h.col[q]);
+            osrc.push_back(q);
+            extra = true;
+          }
+        }
+        if (extra) {
+          orow[i] = (int)optr.size() - 1;
+          optr.push_back((int)ocol.size());
+        }
+      }
+      if ((long long)(optr.size() - 1) * 1000 > n) break;  // too many rows off the diagonals
+      L.ell_src.upload(src, s);
+      L.ell_val.resize((size_t)K * n);
+      L.ell_orow.upload(orow, s);
+      L.ell_optr.upload(optr, s);
+      L.ell_ovf = (long long)ocol.size();
+      if (!ocol.empty()) {
+        L.ell_ocol.upload(ocol, s);
+        L.ell_osrc.upload(osrc, s);
+        L.ell_oval.resize(ocol.size());
+      }
+      for (int k = 0; k < kEllMaxK; ++k) L.ell_off[k] = k < K ? off[k] : 0;
+      L.ell_rr.resize(n);
+      L.ell_k = K;
+      L.ell_dia = true;
+      return;
+    }
+  }
   std::vector<long long> count(kEllMaxK + 2, 0);  // rows of each length, the last bin longer
   for (int i = 0; i < n; ++i) ++count[std::min(h.row_ptr[i + 1] - h.row_ptr[i], kEllMaxK + 1)];
   int K = 0;
@@ -1918,17 +1997,13 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
       if (out == cur) out = u;
       if (L.ell_k > 0) {
         const int ge = grid_for(L.n, 256);
-        const T* oval = L.ell_ovf > 0 ? (const T*)L.ell_oval.get() : (const T*)nullptr;
-        const int* ocol = L.ell_ovf > 0 ? (const int*)L.ell_ocol.get() : (const int*)nullptr;
+        const EllView<T> E = ell_view(L);
         if (xc && step == 0)
-          launch_pdl(cheb_ell_kernel<T, true>, ge, 256, 0, s, L.n, L.ell_k, (const int*)L.ell_col.get(),
-                     (const T*)L.ell_val.get(), (const int*)L.ell_optr.get(), ocol, oval, (const T*)L.dinv.get(), b,
-                     (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step, (const int*)L.agg.get(), xc);
+          launch_pdl(cheb_ell_kernel<T, true>, ge, 256, 0, s, E, (const T*)L.dinv.get(), b, (const T*)cur, out,
+                     L.r.get(), (const double*)L.lmax.get(), step, (const int*)L.agg.get(), xc);
         else
-          launch_pdl(cheb_ell_kernel<T, false>, ge, 256, 0, s, L.n, L.ell_k, (const int*)L.ell_col.get(),
-                     (const T*)L.ell_val.get(), (const int*)L.ell_optr.get(), ocol, oval, (const T*)L.dinv.get(), b,
-                     (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step, (const int*)nullptr,
-                     (const T*)nullptr);
+          launch_pdl(cheb_ell_kernel<T, false>, ge, 256, 0, s, E, (const T*)L.dinv.get(), b, (const T*)cur, out,
+                     L.r.get(), (const double*)L.lmax.get(), step, (const int*)nullptr, (const T*)nullptr);
       } else if (xc && step == 0)  // x + P xc, folded into the first step
         launch_pdl(cheb_step_kernel<T, false, LN, true>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
                    (const T*)L.dinv.get(), b, (const T*)cur, out, L.r.get(), (const double*)L.lmax.get(), step,
@@ -2081,10 +2156,8 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
       return !(e && e[0] == '0');
     }();
     if (L.ell_k > 0) {
-      launch_pdl(ell_residual_kernel<T>, grid_for(L.n, 256), 256, 0, s, L.n, L.ell_k, (const int*)L.ell_col.get(),
-                 (const T*)L.ell_val.get(), (const int*)L.ell_optr.get(),
-                 L.ell_ovf > 0 ? (const int*)L.ell_ocol.get() : (const int*)nullptr,
-                 L.ell_ovf > 0 ? (const T*)L.ell_oval.get() : (const T*)nullptr, b, (const T*)x, L.ell_rr.get());
+      launch_pdl(ell_residual_kernel<T>, grid_for(L.n, 256), 256, 0, s, ell_view(L), b, (const T*)x,
+                 L.ell_rr.get());
       launch_pdl(aggregate_sum_kernel<T>, grid_for(nc, 256), 256, 0, s, nc, (const int*)L.cptr.get(),
                  (const int*)L.cmem.get(), (const double*)L.ell_rr.get(), bc);
     } else {
@@ -2215,8 +2288,10 @@ double AMG<T>::cycle_bytes_from(int l) const {
   const AMGLevel<T>& L = levels_[l];
   const double n = L.n;
   // the matrix as stored: CSR (values, columns, row starts) or the ELL slots
-  // (padding included) and the overflow entries
-  const double mat = L.ell_k > 0 ? ((double)L.ell_k * n + (double)L.ell_ovf) * (vb + 4.0)
+  // (padding included; the diagonal form has no columns but a per-row
+  // overflow index) and the overflow entries
+  const double mat = L.ell_k > 0 ? (L.ell_dia ? (double)L.ell_k * n * vb + n * 4.0 + (double)L.ell_ovf * (vb + 4.0)
+                                              : ((double)L.ell_k * n + (double)L.ell_ovf) * (vb + 4.0))
                                  : (double)L.nnz * (vb + 4.0) + (n + 1.0) * 4.0;
   const int steps = std::max(1, L.degree > 0 ? L.degree : degree);
   const double nc = (l + 1 == (int)levels_.size()) ? nco_ : levels_[l + 1].n;

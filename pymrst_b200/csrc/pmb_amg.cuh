@@ -35,6 +35,24 @@ std::vector<AMGHostLevel> amg_build_hierarchy(int n, const int* row_ptr, const i
                                               const double* val, double theta, int passes,
                                               int coarse_size, int max_levels, int aggressive_below = 0);
 
+constexpr int kEllMaxK = 8;  // slots of an ELL level
+
+// An ELL level as its kernels see it (by value).  Column form: col holds
+// every slot's column, a row longer than K marks its last slot -1 - o (o its
+// overflow row).  Diagonal form (col null): slot k of row i is column
+// i + off[k], and orow[i] is the row's overflow row or -1.
+template <class T>
+struct EllView {
+  int n = 0, K = 0;
+  const int* col = nullptr;
+  const T* val = nullptr;
+  const int* orow = nullptr;
+  const int* optr = nullptr;
+  const int* ocol = nullptr;
+  const T* oval = nullptr;
+  int off[kEllMaxK] = {};
+};
+
 template <class T>
 struct AMGLevel {
   int n = 0, nnz = 0;
@@ -63,6 +81,9 @@ struct AMGLevel {
   // slots; its last slot holds -1 - o (o: its overflow row) and value zero,
   // and the rest of its entries follow in the overflow CSR.
   int ell_k = 0;
+  bool ell_dia = false;  // diagonal form: slot k of row i is column i + ell_off[k]
+  int ell_off[kEllMaxK] = {};
+  DArray<int> ell_orow;          // diagonal form: the row's overflow row or -1
   DArray<int> ell_col, ell_src;  // ell_src: CSR index of each slot's value (-1: zero)
   DArray<T> ell_val;
   DArray<int> ell_optr, ell_ocol, ell_osrc;
