@@ -256,10 +256,13 @@ def kernel_roofline(model, x, x0, dt, torch, N, reps=20):
     # and the well update) on the line-ordered operator copy: every block (FP64
     # 32 B or FP32 16 B) once, the column index of every block off the line
     # (4 B; the diagonal and the two line couplings need none), and per cell r
-    # (16 B), z read and written (32 B) and its perforation index (4 B).  The
-    # zero padding of short rows is not counted.
-    blk = 16 if int(model.cpr_options.get("precision", 0)) == 1 else 32
-    sweep_bytes = nnzb * blk + max(nnzb - 3 * nc, 0) * 4 + nc * (16 + 32 + 4)
+    # and z read and z written (FP64 16 B each, FP32 8 B in mixed precision)
+    # and its perforation index (4 B).  The zero padding of short rows is not
+    # counted.
+    mixed = int(model.cpr_options.get("precision", 0)) == 1
+    blk = 16 if mixed else 32
+    lv = 8 if mixed else 16
+    sweep_bytes = nnzb * blk + max(nnzb - 3 * nc, 0) * 4 + nc * (3 * lv + 4)
     out["line_gs_sweep"] = dict(seconds=ms.value * 1e-3 / sweeps, bytes=sweep_bytes)
     cb = (N.C.c_double * 8)()
     N.check(N.lib().pmb_cpr_bytes(s, cb))

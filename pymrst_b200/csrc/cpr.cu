@@ -705,16 +705,49 @@ __global__ void ell_gather_kernel(long long n, const int* __restrict__ src, cons
 // prolonged pressure correction (xp_c, 0) (xp null: zero).  Without from_z
 // the well part of z is prolonged as well: (0, 0, xp[nc + k]) when the
 // pressure system has bhp unknowns (pw), else zero.
-template <class T>
+// The line-ordered r and z of the smoother: FP64, or FP32 in mixed precision
+// (their residual is still formed and summed in FP64).
+__device__ __forceinline__ double2 lv_load(const double* p, long long t) {
+  return reinterpret_cast<const double2*>(p)[t];
+}
+__device__ __forceinline__ double2 lv_load(const float* p, long long t) {
+  const float2 v = reinterpret_cast<const float2*>(p)[t];
+  return make_double2((double)v.x, (double)v.y);
+}
+// The raw pair, converted only where it is used (fewer registers in FP32).
+template <class LV>
+struct LvPair;
+template <>
+struct LvPair<double> {
+  using type = double2;
+};
+template <>
+struct LvPair<float> {
+  using type = float2;
+};
+template <class LV>
+__device__ __forceinline__ typename LvPair<LV>::type lv_raw(const LV* p, long long t) {
+  return reinterpret_cast<const typename LvPair<LV>::type*>(p)[t];
+}
+__device__ __forceinline__ double2 lv_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 lv_d2(float2 v) { return make_double2((double)v.x, (double)v.y); }
+
+__device__ __forceinline__ void lv_store(double* p, long long t, double2 v) {
+  reinterpret_cast<double2*>(p)[t] = v;
+}
+__device__ __forceinline__ void lv_store(float* p, long long t, double2 v) {
+  reinterpret_cast<float2*>(p)[t] = make_float2((float)v.x, (float)v.y);
+}
+
+template <class T, class LV>
 __global__ void line_enter_kernel(int nc, int nw, bool from_z, bool pw, const int* __restrict__ lcells,
                                   const T* __restrict__ xp, const double* __restrict__ r, double* __restrict__ z,
-                                  double* __restrict__ rl, double* __restrict__ zl) {
+                                  LV* __restrict__ rl, LV* __restrict__ zl) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < nc) {
     const int c = lcells[t];
-    reinterpret_cast<double2*>(rl)[t] = reinterpret_cast<const double2*>(r)[c];
-    reinterpret_cast<double2*>(zl)[t] =
-        from_z ? reinterpret_cast<const double2*>(z)[c] : make_double2(xp ? (double)xp[c] : 0.0, 0.0);
+    lv_store(rl, t, reinterpret_cast<const double2*>(r)[c]);
+    lv_store(zl, t, from_z ? reinterpret_cast<const double2*>(z)[c] : make_double2(xp ? (double)xp[c] : 0.0, 0.0));
   }
   if (from_z) return;
   if (t < nw) {
@@ -728,12 +761,12 @@ __global__ void line_enter_kernel(int nc, int nw, bool from_z, bool pw, const in
 // thread u on position t0 + u.  zl is updated in place; with OUT (the last
 // sweep) the cell's new z is also written to z in cell order.  The well
 // unknowns are read from z (they stay in cell order).
-template <class BT, class CT, bool OUT>
+template <class BT, class CT, bool OUT, class LV>
 __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3)
     line_pcr_ell_kernel(OWView v, int lstart, const int2* __restrict__ crange, const int* __restrict__ lcells,
                         int nslots, const BT* __restrict__ blk, const int* __restrict__ ecol,
-                        const int* __restrict__ epc, const double* __restrict__ wj, const double* __restrict__ rl,
-                        double* __restrict__ zl, double* __restrict__ z, int* status) {
+                        const int* __restrict__ epc, const double* __restrict__ wj, const LV* __restrict__ rl,
+                        LV* __restrict__ zl, double* __restrict__ z, int* status) {
   extern __shared__ __align__(16) unsigned char pcr_raw[];
   __shared__ int sBad;
   const int2 lr = crange[lstart + blockIdx.x];  // (first position, length) of the CTA's line
@@ -745,7 +778,6 @@ __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3)
   const int t = t0 + u;
   const Blk2<CT> zero = {CT(0), CT(0), CT(0), CT(0)};
   const double2 z0 = make_double2(0.0, 0.0);
-  const double2* zl2 = reinterpret_cast<const double2*>(zl);
   Blk2<CT> D = {CT(1), CT(0), CT(0), CT(1)}, Lb = zero, Ub = zero;
   Vec2<CT> y = {CT(0), CT(0)};
   double2 zs = z0;
@@ -773,13 +805,13 @@ __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3)
     const BT Dr = blk[t];
     const BT Lr = u > 0 ? blk[n + t] : bz;
     const BT Ur = u + 1 < len ? blk[2 * n + t] : bz;
-    zs = zl2[t];
-    const double2 zlo = u > 0 ? zl2[t - 1] : z0;
-    const double2 zup = u + 1 < len ? zl2[t + 1] : z0;
-    double2 zq[kEllPrefetch];
+    zs = lv_load(zl, t);
+    const double2 zlo = u > 0 ? lv_load(zl, t - 1) : z0;
+    const double2 zup = u + 1 < len ? lv_load(zl, t + 1) : z0;
+    typename LvPair<LV>::type zq[kEllPrefetch];
 #pragma unroll
-    for (int q = 0; q < kEllPrefetch; ++q) zq[q] = q < nlat ? zl2[cj[q]] : z0;
-    double2 rc = reinterpret_cast<const double2*>(rl)[t];
+    for (int q = 0; q < kEllPrefetch; ++q) zq[q] = lv_raw(zl, q < nlat ? cj[q] : t);
+    double2 rc = lv_load(rl, t);
     double2 m = mv2(ld4(Dr), zs);
     rc.x -= m.x;
     rc.y -= m.y;
@@ -791,12 +823,12 @@ __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3)
     rc.y -= m.y;
 #pragma unroll
     for (int q = 0; q < kEllPrefetch; ++q) {
-      m = mv2(ld4(aq[q]), zq[q]);
+      m = mv2(ld4(aq[q]), lv_d2(zq[q]));  // a zero block where q >= nlat
       rc.x -= m.x;
       rc.y -= m.y;
     }
     for (int q = kEllPrefetch; q < nlat; ++q) {
-      m = mv2(ld4(blk[(3 + q) * n + t]), zl2[ecol[q * n + t]]);
+      m = mv2(ld4(blk[(3 + q) * n + t]), lv_load(zl, ecol[q * n + t]));
       rc.x -= m.x;
       rc.y -= m.y;
     }
@@ -810,7 +842,7 @@ __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3)
   if (!pcr_line<CT>(pcr_raw, u, len, act, D, Lb, Ub, y, &sBad, status, x)) return;
   zs.x += (double)x.x;
   zs.y += (double)x.y;
-  reinterpret_cast<double2*>(zl)[t] = zs;
+  lv_store(zl, t, zs);
   if (OUT) reinterpret_cast<double2*>(z)[lcells[t]] = zs;
 }
 
@@ -818,9 +850,10 @@ __global__ void __launch_bounds__(kPcrMaxLen, sizeof(CT) == 4 ? 4 : 3)
 // well, the lanes over its perforations.  The cells' z is read from zc at the
 // perforated cell (ppos null) or at its line position ppos[i]; the wells' z
 // and r are in z and r.
+template <class ZT>
 __global__ void __launch_bounds__(256) gs_well_kernel(OWView v, const double* __restrict__ wj,
                                                       const double* __restrict__ r, double* __restrict__ z,
-                                                      const double* __restrict__ zc, const int* __restrict__ ppos) {
+                                                      const ZT* __restrict__ zc, const int* __restrict__ ppos) {
   pdl_enter();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int k = warp; k < v.nw; k += nwarp) {
@@ -828,7 +861,7 @@ __global__ void __launch_bounds__(256) gs_well_kernel(OWView v, const double* __
     for (int i = v.perf_ptr[k] + lane; i < v.perf_ptr[k + 1]; i += 32) {
       const int c = ppos ? ppos[i] : v.perf_cell[i];
       const double* C = wj + v.wl.C + 4LL * i;
-      const double zp = zc[2LL * c], zs = zc[2LL * c + 1];
+      const double zp = (double)zc[2LL * c], zs = (double)zc[2LL * c + 1];
       s0 += C[0] * zp + C[1] * zs;
       s1 += C[2] * zp + C[3] * zs;
     }
@@ -1022,8 +1055,13 @@ void CPRSolver::build_line_ell() {
     ell_.blk32.resize(4LL * slots * n);
   else
     ell_.blk64.resize(4LL * slots * n);
-  ell_.rl.resize(2 * n);
-  ell_.zl.resize(2 * n);
+  if (f32_) {
+    ell_.rl32.resize(2 * n);
+    ell_.zl32.resize(2 * n);
+  } else {
+    ell_.rl.resize(2 * n);
+    ell_.zl.resize(2 * n);
+  }
   use_ell_ = true;
 }
 
@@ -1135,17 +1173,26 @@ void CPRSolver::setup(const double* jac, const double* well, const double* x) {
   ++since_build_;
 }
 
+template <class T>
+void CPRSolver::enter_lines(const T* xp, const double* r, double* z, bool from_z, bool pw) {
+  const OWView v = m_.view();
+  const int g = grid_for(std::max(v.nc, v.nw), 256);
+  if (f32_)
+    line_enter_kernel<T, float><<<g, 256, 0, s_>>>(v.nc, v.nw, from_z, pw, m_.lines().line_cells.get(), xp, r, z,
+                                                    ell_.rl32.get(), ell_.zl32.get());
+  else
+    line_enter_kernel<T, double><<<g, 256, 0, s_>>>(v.nc, v.nw, from_z, pw, m_.lines().line_cells.get(), xp, r, z,
+                                                     ell_.rl.get(), ell_.zl.get());
+  PMB_CHECK_LAUNCH();
+}
+
 void CPRSolver::local_stage(const double* r, double* z, bool entered) {
   const OWView v = m_.view();
   const auto& cp = m_.h_color_ptr();
   const double4* A = reinterpret_cast<const double4*>(jac_);
   if (use_ell_) {
     const auto& Ls = m_.lines();
-    if (!entered) {
-      line_enter_kernel<double><<<grid_for(v.nc, 256), 256, 0, s_>>>(
-          v.nc, v.nw, true, false, Ls.line_cells.get(), nullptr, r, z, ell_.rl.get(), ell_.zl.get());
-      PMB_CHECK_LAUNCH();
-    }
+    if (!entered) enter_lines((const double*)nullptr, r, z, true, false);
     const int nb = std::max(32, (Ls.max_len + 31) / 32 * 32);
     const int sweeps = std::max(1, o_.local_sweeps);
     for (int sweep = 0; sweep < sweeps; ++sweep) {
@@ -1153,23 +1200,34 @@ void CPRSolver::local_stage(const double* r, double* z, bool entered) {
       for (int q = 0; q + 1 < (int)Ls.h_color_ptr.size(); ++q) {
         const int cnt = Ls.h_color_ptr[q + 1] - Ls.h_color_ptr[q];
         if (cnt <= 0) continue;
-        auto go = [&](auto kernel, auto* blk, size_t smem) {
+        auto go = [&](auto kernel, auto* blk, size_t smem, auto* rl, auto* zl) {
           launch_pdl(kernel, cnt, nb, (size_t)nb * smem, s_, v, Ls.h_color_ptr[q], Ls.color_range.get(),
-                     Ls.line_cells.get(), ell_.slots, blk, ell_.col.get(), ell_.pc.get(), well_, ell_.rl.get(),
-                     ell_.zl.get(), z, status_.get());
+                     Ls.line_cells.get(), ell_.slots, blk, ell_.col.get(), ell_.pc.get(), well_, rl, zl, z,
+                     status_.get());
         };
         const size_t smem32 = 3 * sizeof(Blk2<float>) + sizeof(Vec2<float>);
         const size_t smem64 = 3 * sizeof(Blk2<double>) + sizeof(Vec2<double>);
         const float4* b32 = reinterpret_cast<const float4*>(ell_.blk32.get());
         const double4* b64 = reinterpret_cast<const double4*>(ell_.blk64.get());
+        float* rl32 = ell_.rl32.get();
+        float* zl32 = ell_.zl32.get();
+        double* rl64 = ell_.rl.get();
+        double* zl64 = ell_.zl.get();
         if (f32_)
-          out ? go(line_pcr_ell_kernel<float4, float, true>, b32, smem32)
-              : go(line_pcr_ell_kernel<float4, float, false>, b32, smem32);
+          out ? go(line_pcr_ell_kernel<float4, float, true, float>, b32, smem32, rl32, zl32)
+              : go(line_pcr_ell_kernel<float4, float, false, float>, b32, smem32, rl32, zl32);
         else
-          out ? go(line_pcr_ell_kernel<double4, double, true>, b64, smem64)
-              : go(line_pcr_ell_kernel<double4, double, false>, b64, smem64);
+          out ? go(line_pcr_ell_kernel<double4, double, true, double>, b64, smem64, rl64, zl64)
+              : go(line_pcr_ell_kernel<double4, double, false, double>, b64, smem64, rl64, zl64);
       }
-      if (v.nw) launch_pdl(gs_well_kernel, 1, 256, 0, s_, v, well_, r, z, ell_.zl.get(), ell_.perf_pos.get());
+      if (v.nw) {
+        if (f32_)
+          launch_pdl(gs_well_kernel<float>, 1, 256, 0, s_, v, well_, r, z, (const float*)ell_.zl32.get(),
+                     (const int*)ell_.perf_pos.get());
+        else
+          launch_pdl(gs_well_kernel<double>, 1, 256, 0, s_, v, well_, r, z, (const double*)ell_.zl.get(),
+                     (const int*)ell_.perf_pos.get());
+      }
     }
     return;
   }
@@ -1209,7 +1267,7 @@ void CPRSolver::local_stage(const double* r, double* z, bool entered) {
         PMB_CHECK_LAUNCH();
       }
       if (v.nw) {
-        gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z, z, nullptr);
+        gs_well_kernel<double><<<1, 256, 0, s_>>>(v, well_, r, z, z, nullptr);
         PMB_CHECK_LAUNCH();
       }
     }
@@ -1224,7 +1282,7 @@ void CPRSolver::local_stage(const double* r, double* z, bool entered) {
       PMB_CHECK_LAUNCH();
     }
     if (v.nw) {
-      gs_well_kernel<<<1, 256, 0, s_>>>(v, well_, r, z, z, nullptr);
+      gs_well_kernel<double><<<1, 256, 0, s_>>>(v, well_, r, z, z, nullptr);
       PMB_CHECK_LAUNCH();
     }
   }
@@ -1257,8 +1315,7 @@ void CPRSolver::precond_body(const double* r, double* z) {
     }
     if (use_ell_) {
       // prolongation straight into line order, with r
-      line_enter_kernel<<<gpro, 256, 0, s_>>>(v.nc, v.nw, false, np_ > v.nc, m_.lines().line_cells.get(), xp, r, z,
-                                              ell_.rl.get(), ell_.zl.get());
+      enter_lines(xp, r, z, false, np_ > v.nc);
     } else if (np_ > v.nc) {
       prolong_pw_kernel<<<gpro, 256, 0, s_>>>(v.nc, v.nw, xp, z);
     } else {
@@ -1272,9 +1329,7 @@ void CPRSolver::precond_body(const double* r, double* z) {
     else
       pressure_stage(bp_.get(), xp_.get(), amg_);
   } else if (use_ell_) {
-    line_enter_kernel<double><<<gpro, 256, 0, s_>>>(v.nc, v.nw, false, false, m_.lines().line_cells.get(), nullptr,
-                                                    r, z, ell_.rl.get(), ell_.zl.get());
-    PMB_CHECK_LAUNCH();
+    enter_lines((const double*)nullptr, r, z, false, false);
   } else {
     prolong_p_kernel<double><<<gpro, 256, 0, s_>>>(v.nc, 3 * v.nw, nullptr, z);
     PMB_CHECK_LAUNCH();
@@ -1333,14 +1388,18 @@ void CPRSolver::bytes(double* out) const {
   // block once, the index of every block off the line (the line-ordered copy
   // needs none for the diagonal and the two line couplings; the block-CSR one
   // per block plus row pointers), r, z read and written, perforation index
-  out[1] = use_ell_ ? nnzb * blk + std::max(nnzb - 3.0 * nc, 0.0) * 4.0 + nc * (16.0 + 32.0 + 4.0)
+  // (the line-ordered r and z are FP32 in mixed precision)
+  const double lv = f32_ ? 8.0 : 16.0;
+  out[1] = use_ell_ ? nnzb * blk + std::max(nnzb - 3.0 * nc, 0.0) * 4.0 + nc * (lv + 2.0 * lv + 4.0)
                     : nnzb * (blk + 4.0) + (nc + 1.0) * 4.0 + nc * (16.0 + 32.0 + 4.0);
   // y = J x: blocks, column indices, row pointers, x read, y written
   out[2] = nnzb * 36.0 + (nc + 1.0) * 4.0 + nvec * 16.0;
   // restriction (r read, weights, pressure right-hand side written) and the
   // prolongation into line order (pressure correction, r, the line's cell
   // index read; r and z in line order written)
-  out[3] = o_.use_pressure_stage ? nc * (16.0 + vb) + nc * (vb + 16.0 + 4.0 + 32.0) : 0.0;
+  out[3] = o_.use_pressure_stage
+               ? nc * (16.0 + vb) + nc * (vb + 16.0 + 4.0 + (use_ell_ ? 2.0 * lv : 32.0))
+               : 0.0;
   // setup: the second stage's copy of the Jacobian (gather index, FP64 block
   // read, block written), the weights (pressures read), the pressure values
   // (blocks read, values written), FP32 conversion of level 0

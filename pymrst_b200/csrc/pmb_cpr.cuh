@@ -44,6 +44,9 @@ class CPRSolver {
   void precond_body(const double* r, double* z);
   // entered: rl / zl already hold r and z in line order (ell_ path only)
   void local_stage(const double* r, double* z, bool entered = false);
+  // r (and z, or the prolonged pressure correction xp) into line order
+  template <class T>
+  void enter_lines(const T* xp, const double* r, double* z, bool from_z, bool pw);
   void prepare_local(const double* jac);
   void build_line_ell();
   void check_status();
@@ -80,7 +83,8 @@ class CPRSolver {
   struct LineEll {
     int slots = 0;
     DArray<int> src, col, pc, perf_pos;
-    DArray<double> blk64, rl, zl;
+    DArray<double> blk64, rl, zl;  // rl, zl: r and z in line order (FP64 arithmetic)
+    DArray<float> rl32, zl32;       // the same in mixed precision
     DArray<float> blk32;
   } ell_;
   bool use_ell_ = false;

@@ -1,7 +1,8 @@
 """The line smoother on its line-ordered operator copy (the default) against
 the block-CSR line kernel (PMB_LINE_ELL=0): the same Newton step, run in two
-processes, converges in the same Newton iterations to the same state; only
-the summation order of the smoother's residual differs."""
+processes, converges in the same Newton iterations to the same state; the
+summation order of the smoother's residual differs and, in mixed precision,
+the line-ordered r and z are FP32."""
 
 import json
 import os
