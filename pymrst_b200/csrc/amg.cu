@@ -353,6 +353,15 @@ __device__ __forceinline__ double cheb_dir(int step, double c1, double c2, doubl
   return step == 0 ? t : __fma_rn(c1, d_old, t);
 }
 
+// ZeroStep (pmb_amg.cuh): the arithmetic of cheb_step_kernel<T, true>.
+template <class T>
+__device__ __forceinline__ void zero_step(const ZeroStep<T>& z, long long i, T b) {
+  const double r = cheb_res((double)b, 0.0, (double)z.dinv[i]);
+  const double dn = cheb_dir(0, z.tab[1], z.tab[2], 0.0, r);
+  z.d[i] = (T)dn;
+  z.x[i] = (T)__dadd_rn(0.0, dn);
+}
+
 // Chebyshev on D^{-1} A over [lmax/10, lmax]: step `step` of the
 // three-term recurrence; x_out = x_in + d, d = c1 d + c2 D^{-1}(b - A x_in).
 // LANES threads share a row.
@@ -442,7 +451,8 @@ __global__ void __launch_bounds__(256) restrict_rows_kernel(const int* __restric
                                                             const int* __restrict__ cmem,
                                                             const int* __restrict__ rp, const int* __restrict__ ci,
                                                             const T* __restrict__ a, const T* __restrict__ b,
-                                                            const T* __restrict__ x, T* __restrict__ bc) {
+                                                            const T* __restrict__ x, T* __restrict__ bc,
+                                                            ZeroStep<T> zs) {
   extern __shared__ double rr_smem[];
   // the plan, the member lists and the first member rows: loaded before the
   // wait (none is written inside a cycle)
@@ -477,6 +487,7 @@ __global__ void __launch_bounds__(256) restrict_rows_kernel(const int* __restric
     double v = 0.0;
     for (int m = cptr[I]; m < cptr[I + 1]; ++m) v = __dadd_rn(v, rr_smem[m - m0]);
     bc[I] = (T)v;
+    if (zs.dinv) zero_step(zs, I, (T)v);
   }
 }
 
@@ -604,13 +615,15 @@ __global__ void __launch_bounds__(256) ell_residual_kernel(EllView<T> E, const T
 template <class T>
 __global__ void __launch_bounds__(256) aggregate_sum_kernel(int nc, const int* __restrict__ cptr,
                                                             const int* __restrict__ cmem,
-                                                            const double* __restrict__ rr, T* __restrict__ bc) {
+                                                            const double* __restrict__ rr, T* __restrict__ bc,
+                                                            ZeroStep<T> zs) {
   pdl_enter();
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= nc) return;
   double v = 0.0;
   for (int m = cptr[I]; m < cptr[I + 1]; ++m) v = __dadd_rn(v, rr[cmem[m]]);
   bc[I] = (T)v;
+  if (zs.dinv) zero_step(zs, I, (T)v);
 }
 
 // dst[k] = val[src[k]] (zero where src is -1): the ELL copy's values after a
@@ -1480,12 +1493,16 @@ __device__ __forceinline__ void kcoef_block(int G, int mode, const double* __res
 // out = a - c0 b, c0 = (v1.rc)/(v1.v1) from the kdots partials
 template <class T>
 __global__ void __launch_bounds__(256) kaxpy_kernel(int n, const T* __restrict__ a, const T* __restrict__ b, int G,
-                                                    const double* __restrict__ part, T* __restrict__ out) {
+                                                    const double* __restrict__ part, T* __restrict__ out,
+                                                    ZeroStep<T> zs) {
   pdl_enter();
   __shared__ double c[3];
   kcoef_block(G, 0, part, c);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    out[i] = (T)((double)a[i] - c[0] * (double)b[i]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const T o = (T)((double)a[i] - c[0] * (double)b[i]);
+    out[i] = o;
+    if (zs.dinv) zero_step(zs, i, o);
+  }
 }
 
 // out = y0 c1 + y1 c2, (y0, y1) the least-squares pair from the kdots partials
@@ -1970,7 +1987,8 @@ void AMG<T>::refresh(cudaStream_t s, int* d_status) {
 }
 
 template <class T>
-void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start, const T* xc) {
+void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start, const T* xc,
+                    bool first_done) {
   // degree steps ping-pong between x and L.t, ordered so that the last one
   // writes x; the first step of an odd count from a non-zero start, which
   // would overwrite its own input, writes L.u instead.  Only a single step
@@ -1985,10 +2003,11 @@ void AMG<T>::smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_
     constexpr int LN = decltype(ln)::value;
     const int g = grid_for((long long)L.n * LN, 256);
     if (zero_start) {
-      T* out = (steps % 2 == 1) ? x : t;
-      launch_pdl(cheb_step_kernel<T, true, LN>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
-                 (const T*)L.dinv.get(), b, (const T*)nullptr, out, L.r.get(), (const double*)L.lmax.get(), 0,
-                 (const int*)nullptr, (const T*)nullptr);
+      T* out = (steps % 2 == 1) ? x : t;  // zero_step_for() names the same buffer
+      if (!first_done)
+        launch_pdl(cheb_step_kernel<T, true, LN>, g, 256, 0, s, L.n, L.row_ptr, L.col, (const T*)L.val.get(),
+                   (const T*)L.dinv.get(), b, (const T*)nullptr, out, L.r.get(), (const double*)L.lmax.get(), 0,
+                   (const int*)nullptr, (const T*)nullptr);
       cur = out;
       step = 1;
     }
@@ -2123,8 +2142,31 @@ static const char* level_phase(int l, int kind) {
   return names[(size_t)std::min(l, 31) * 4 + kind].c_str();
 }
 
+// The first step of level m's pre-smoothing on right-hand side into x, for
+// the kernel that writes that right-hand side to take over, where level m
+// runs the per-step smoothing (not the coarsest, the cluster tail or the
+// fused cycle).
 template <class T>
-void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
+ZeroStep<T> AMG<T>::zero_step_for(int m, T* x) {
+  ZeroStep<T> z;
+  if (m >= (int)levels_.size() || (tail_start_ >= 0 && m >= tail_start_) || (coop_start_ >= 0 && m >= coop_start_))
+    return z;
+  static const bool enabled = [] {
+    const char* e = std::getenv("PMB_AMG_FUSE_ZERO_STEP");
+    return !(e && e[0] == '0');
+  }();
+  if (!enabled) return z;
+  AMGLevel<T>& L = levels_[m];
+  const int steps = std::max(1, L.degree > 0 ? L.degree : degree);
+  z.dinv = L.dinv.get();
+  z.tab = L.lmax.get();
+  z.d = L.r.get();
+  z.x = (steps % 2 == 1) ? x : L.t.get();
+  return z;
+}
+
+template <class T>
+void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s, bool zero_done) {
   if (tail_start_ >= 0 && l == tail_start_) {
     PhaseTimer pt("amg.tail", s);
     launch_tail(b, x, s);
@@ -2147,26 +2189,31 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
   T* xc = next_is_coarsest ? co_x_.get() : levels_[l + 1].x.get();
   {
     PhaseTimer pt(level_phase(l, 0), s);
-    smooth(L, b, x, s, true);
+    smooth(L, b, x, s, true, nullptr, zero_done);
   }
+  // the next level's first pre-smoothing step rides on the restriction: its
+  // first visit smooths bc into xc (a plain correction) or into kc1 (K-cycle)
+  const bool kc = l < k_levels && l + 1 < (int)levels_.size();
+  ZeroStep<T> zs = zero_step_for(l + 1, kc ? levels_[l + 1].kc1.get() : xc);
   {
     PhaseTimer pt(level_phase(l, 1), s);
     static const bool by_rows = [] {
       const char* e = std::getenv("PMB_RESTRICT_ROWS");
       return !(e && e[0] == '0');
     }();
+    if (!by_rows && L.ell_k == 0) zs = ZeroStep<T>();  // restrict_residual_kernel does not take it
     if (L.ell_k > 0) {
       launch_pdl(ell_residual_kernel<T>, grid_for(L.n, 256), 256, 0, s, ell_view(L), b, (const T*)x,
                  L.ell_rr.get());
       launch_pdl(aggregate_sum_kernel<T>, grid_for(nc, 256), 256, 0, s, nc, (const int*)L.cptr.get(),
-                 (const int*)L.cmem.get(), (const double*)L.ell_rr.get(), bc);
+                 (const int*)L.cmem.get(), (const double*)L.ell_rr.get(), bc, zs);
     } else {
       with_lanes(L.lanes, [&](auto ln) {
         constexpr int LN = decltype(ln)::value;
         if (by_rows)
           launch_pdl(restrict_rows_kernel<T, LN>, L.rblocks, 256, L.rsmem, s, (const int*)L.rblk.get(),
                      (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
-                     (const T*)x, bc);
+                     (const T*)x, bc, zs);
         else
           launch_pdl(restrict_residual_kernel<T, LN>, grid_for((long long)nc * LN, 256), 256, 0, s, nc,
                      (const int*)L.cptr.get(), (const int*)L.cmem.get(), L.row_ptr, L.col, (const T*)L.val.get(), b,
@@ -2174,7 +2221,7 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
       });
     }
   }
-  coarse_correction(l, bc, xc, s);
+  coarse_correction(l, bc, xc, s, zs.dinv != nullptr);
   PhaseTimer pt(level_phase(l, 2), s);
   if (L.n < kFoldProlongRows && degree >= 1) {
     smooth(L, b, x, s, false, xc);  // prolongation folded into the first smoothing step
@@ -2190,16 +2237,17 @@ void AMG<T>::cycle(int l, const T* b, T* x, cudaStream_t s) {
 //   c1 = B rc, v1 = A c1, r2 = rc - (v1.rc / v1.v1) v1,
 //   c2 = B r2, v2 = A c2, ec = y0 c1 + y1 c2 with y minimising |rc - y0 v1 - y1 v2|.
 template <class T>
-void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
+void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s, bool first_done) {
   const bool kc = l < k_levels && l + 1 < (int)levels_.size();
   if (!kc) {
-    cycle(l + 1, rc, ec, s);
+    cycle(l + 1, rc, ec, s, first_done);
     return;
   }
   AMGLevel<T>& C = levels_[l + 1];
   const int n = C.n, g = grid_for(n, 256);
   const int G = std::min(2 * kNumSM, g);
-  cycle(l + 1, rc, C.kc1.get(), s);
+  cycle(l + 1, rc, C.kc1.get(), s, first_done);
+  const ZeroStep<T> zs2 = zero_step_for(l + 1, C.kc2.get());  // rides on the kaxpy below
   {
     PhaseTimer pt(level_phase(l + 1, 3), s);
     with_lanes(C.lanes, [&](auto ln) {
@@ -2209,9 +2257,9 @@ void AMG<T>::coarse_correction(int l, const T* rc, T* ec, cudaStream_t s) {
     });
     launch_pdl(kdots_kernel<T, 2>, G, 256, 0, s, n, (const T*)C.kv1.get(), (const T*)nullptr, rc, C.kpart.get());
     launch_pdl(kaxpy_kernel<T>, G, 256, 0, s, n, rc, (const T*)C.kv1.get(), G, (const double*)C.kpart.get(),
-               C.kr2.get());
+               C.kr2.get(), zs2);
   }
-  cycle(l + 1, C.kr2.get(), C.kc2.get(), s);
+  cycle(l + 1, C.kr2.get(), C.kc2.get(), s, zs2.dinv != nullptr);
   PhaseTimer pt(level_phase(l + 1, 3), s);
   with_lanes(C.lanes, [&](auto ln) {
     constexpr int LN = decltype(ln)::value;

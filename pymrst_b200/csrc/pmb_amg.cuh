@@ -35,6 +35,17 @@ std::vector<AMGHostLevel> amg_build_hierarchy(int n, const int* row_ptr, const i
                                               const double* val, double theta, int passes,
                                               int coarse_size, int max_levels, int aggressive_below = 0);
 
+// The first Chebyshev step of a level from a zero start (no matrix:
+// d = c2 D^-1 b, x = d), fused into the kernel that writes that level's
+// right-hand side; dinv null: not fused.
+template <class T>
+struct ZeroStep {
+  const T* dinv = nullptr;
+  const double* tab = nullptr;  // the level's Chebyshev table
+  T* d = nullptr;
+  T* x = nullptr;
+};
+
 constexpr int kEllMaxK = 8;  // slots of an ELL level
 
 // An ELL level as its kernels see it (by value).  Column form: col holds
@@ -206,10 +217,14 @@ class AMG {
   int* coop_status_ = nullptr;
   void build_fused(cudaStream_t s);
   void launch_fused(const T* b, T* x, cudaStream_t s);
-  void cycle(int l, const T* b, T* x, cudaStream_t s);
-  void coarse_correction(int l, const T* rc, T* ec, cudaStream_t s);
+  // zero_done / first_done: the kernel that wrote b already took the first
+  // pre-smoothing step of level l (l + 1)
+  void cycle(int l, const T* b, T* x, cudaStream_t s, bool zero_done = false);
+  void coarse_correction(int l, const T* rc, T* ec, cudaStream_t s, bool first_done = false);
+  ZeroStep<T> zero_step_for(int m, T* x);
   // xc (non-zero start only): fold x += P xc into the first step
-  void smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start, const T* xc = nullptr);
+  void smooth(AMGLevel<T>& L, const T* b, T* x, cudaStream_t s, bool zero_start, const T* xc = nullptr,
+              bool first_done = false);
   void build_ell(AMGLevel<T>& L, const AMGHostLevel& h, cudaStream_t s);
   std::vector<AMGLevel<T>> levels_;
   // coarsest level: dense inverse in FP64
