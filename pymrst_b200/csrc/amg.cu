@@ -1061,6 +1061,7 @@ __device__ __forceinline__ double group_sum_rt(double v, int lanes) {
 constexpr int kTailThreads = 1024;
 constexpr int kTailMaxRows = 65536;
 constexpr int kFusedMaxRows = 65536;  // the largest level of the fused coarse cycle
+constexpr int kEllMinRows = 262144;   // the smallest level with an ELL copy
 
 template <class T>
 __device__ __forceinline__ T* ct_sec(unsigned char* base, int off) {
@@ -1635,9 +1636,11 @@ static EllView<T> ell_view(const AMGLevel<T>& L) {
 
 // The ELL copy of a level, where it pays: rows of nearly equal length (at
 // most 0.1% longer than the slot count, which is at most kEllMaxK, and the
-// padding at most 30% of the entries), on levels above the sizes the cluster
-// tail and the fused cycle take (those read the CSR arrays and must give the
-// per-step path's bits).  The diagonal form is taken where it fits, the
+// padding at most 30% of the entries), on levels of at least kEllMinRows
+// rows (one thread per row needs a few waves of threads to hide its
+// latency; PMB_AMG_ELL_MIN_ROWS changes the bound, never below the sizes the
+// cluster tail and the fused cycle take: those read the CSR arrays and must
+// give the per-step path's bits).  The diagonal form is taken where it fits, the
 // column form otherwise.  PMB_AMG_ELL=0 keeps every level in CSR,
 // PMB_AMG_ELL=1 allows only the column form.
 template <class T>
@@ -1646,13 +1649,16 @@ void AMG<T>::build_ell(AMGLevel<T>& L, const AMGHostLevel& h, cudaStream_t s) {
   L.ell_ovf = 0;
   L.ell_dia = false;
   const char* e = std::getenv("PMB_AMG_ELL");
-  if ((e && e[0] == '0') || L.n <= std::max(kTailMaxRows, kFusedMaxRows)) return;
+  const char* em = std::getenv("PMB_AMG_ELL_MIN_ROWS");
+  const long long min_rows = std::max<long long>(em ? std::atoll(em) : kEllMinRows,
+                                                 std::max(kTailMaxRows, kFusedMaxRows) + 1LL);
+  if ((e && e[0] == '0') || L.n < min_rows) return;
   const int n = L.n;
   const long long nnz = h.row_ptr[n];
   if (!(e && e[0] == '1')) {
     // diagonal form: the fewest column offsets, most frequent first, that
-    // hold all but 0.1% of the entries, with at most 0.1% of the rows
-    // reaching off them and at most 30% padding
+    // hold all but 1% of the entries, with at most 1% of the rows reaching
+    // off them (through the overflow list) and at most 30% padding
     std::unordered_map<int, long long> freq;
     for (int i = 0; i < n; ++i)
       for (int k = h.row_ptr[i]; k < h.row_ptr[i + 1]; ++k) ++freq[h.col[k] - i];
@@ -1664,7 +1670,7 @@ void AMG<T>::build_ell(AMGLevel<T>& L, const AMGHostLevel& h, cudaStream_t s) {
     long long covered = 0;
     for (int K = 1; K <= std::min<int>(kEllMaxK, (int)byf.size()); ++K) {
       covered += byf[K - 1].first;
-      if ((nnz - covered) * 1000 > nnz || (double)K * n > 1.3 * (double)nnz) continue;
+      if ((nnz - covered) * 100 > nnz || (double)K * n > 1.3 * (double)nnz) continue;
       std::vector<int> off(K);
       for (int k = 0; k < K; ++k) off[k] = byf[k].second;
       std::sort(off.begin(), off.end());
@@ -1687,7 +1693,7 @@ void AMG<T>::build_ell(AMGLevel<T>& L, const AMGHostLevel& h, cudaStream_t s) {
           optr.push_back((int)ocol.size());
         }
       }
-      if ((long long)(optr.size() - 1) * 1000 > n) break;  // too many rows off the diagonals
+      if ((long long)(optr.size() - 1) * 100 > n) break;  // too many rows off the diagonals
       L.ell_src.upload(src, s);
       L.ell_val.resize((size_t)K * n);
       L.ell_orow.upload(orow, s);

@@ -1,4 +1,5 @@
 """The slot-major ELL copy of the large AMG levels (one thread per row)
+(its diagonal form, and the column form that PMB_AMG_ELL=1 forces)
 against the CSR kernels (PMB_AMG_ELL=0): the CPR-FGMRES solve of the same
 Newton system, run in two processes, reaches the same solution to the
 tolerance, in FP64 and in mixed precision, with Krylov counts within 2%
@@ -52,20 +53,24 @@ print(json.dumps({"krylov": info[0], "relres": info[1], "cycle_bytes": cb[0], "l
 """
 
 
-def _run(tmp_path, ell, precision):
+def _run(tmp_path, mode, precision):
     env = dict(os.environ)
-    env["PMB_AMG_ELL"] = "1" if ell else "0"
-    out = tmp_path / f"state_{int(ell)}_{precision}.npy"
+    env.pop("PMB_AMG_ELL", None)
+    if mode != "diagonal":
+        env["PMB_AMG_ELL"] = "1" if mode == "column" else "0"
+    env["PMB_AMG_ELL_MIN_ROWS"] = "65537"  # a small model, so that level 0 takes the ELL copy
+    out = tmp_path / f"state_{mode}_{precision}.npy"
     r = subprocess.run([sys.executable, "-c", SNIPPET, str(ROOT), str(out), str(precision)], env=env,
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     return json.loads(r.stdout.strip().splitlines()[-1]), np.load(out)
 
 
+@pytest.mark.parametrize("mode", ["diagonal", "column"])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_ell_levels_match_the_csr_kernels(tmp_path, precision):
-    ell, xe = _run(tmp_path, True, precision)
-    csr, xc = _run(tmp_path, False, precision)
+def test_ell_levels_match_the_csr_kernels(tmp_path, precision, mode):
+    ell, xe = _run(tmp_path, mode, precision)
+    csr, xc = _run(tmp_path, "csr", precision)
     assert csr["levels"][0] > 65536  # level 0 is large enough to take the ELL copy
     assert ell["relres"] <= 1e-11 and csr["relres"] <= 1e-11
     assert abs(ell["krylov"] - csr["krylov"]) <= (0.02 if precision == 0 else 0.1) * csr["krylov"] + 1
