@@ -193,10 +193,10 @@ class AMG {
   // replayed from a CUDA graph.
   double time_visit(int l, int reps, cudaStream_t s);
   // The levels from tail_first_level() down (the first level below the
-  // K-cycle levels with at most PMB_AMG_TAIL_ROWS rows, and all coarser
-  // ones) run as one thread-block-cluster launch per visit
-  // (amg_tail_kernel), bitwise the per-step path; -1 when off (the default,
-  // or no cluster launch possible).
+  // K-cycle levels with at most PMB_AMG_TAIL_ROWS rows whose levels fit a
+  // cluster's shared memory, and all coarser ones) run as one
+  // thread-block-cluster launch per visit (amg_ctail_kernel), bitwise the
+  // per-step path; -1 when off (the default, or no layout fits).
   int tail_first_level() const { return tail_start_; }
   int tail_cluster_size() const { return tail_cluster_; }
 
