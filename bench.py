@@ -45,9 +45,10 @@ WORKLOAD = dict(name="channelised oil-water 60x220x85 (1,122,000 cells), 10-day 
 CPU_SAMPLE = dict(dims=(18, 66, 25), cell_size=(6.1 * 60 / 18, 3.05 * 220 / 66, 0.61 * 85 / 25))
 # DRAM bytes per swept cell of one line_pcr_ell_kernel launch, from ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the 60x220x60 model
-# (396,000 cells per colour).
-PCR_DRAM_BYTES_PER_CELL = {"fp64": (119810560 + 4159744) / 396000.0,
-                           "mixed": (78398208 + 1757952) / 396000.0}
+# (396,000 cells per colour).  The mixed-precision kernel has read and
+# written its line-ordered r and z in FP32 since that capture, so its entry
+# is left out (reported as null) until it is captured again.
+PCR_DRAM_BYTES_PER_CELL = {"fp64": (119810560 + 4159744) / 396000.0}
 
 
 def parse():
