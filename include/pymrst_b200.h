@@ -47,6 +47,27 @@ int pmb_launch_count(int64_t* h_out);
 int pmb_profile_report(char* h_buf, int32_t len, int32_t reset);
 
 /* ------------------------------------------------------------------------
+ * Grid geometry.
+ * pmb_compute_geometry3d replaces compute_geometry for 3-D grids
+ * (pymrst/gridprocessing/compute_geometry.py:211-325): every face is split
+ * into a fan of triangles around its pivot (the mean of its nodes, or row f
+ * of d_hinge where that row's x is finite; d_hinge may be NULL), giving its
+ * area (the sum of the triangles' areas), normal (the sum of their area
+ * vectors) and centroid (area-weighted, the pivot where the area is not
+ * positive); every cell into the tetrahedra joining the mean of its face
+ * centroids to its faces' triangles, oriented out of the cell, giving its
+ * volume and centroid.  Topology: node_pos (nf + 1) / nodes, face_pos
+ * (nc + 1) / cell_faces, neighbors (nf x 2, -1 outside), coords nn x 3;
+ * outputs face_areas (nf), face_normals and face_centroids (nf x 3),
+ * cell_volumes (nc), cell_centroids (nc x 3).  Synchronises the stream.
+ */
+int pmb_compute_geometry3d(int32_t nf, int32_t nc, const double* d_coords, const int32_t* d_node_pos,
+                           const int32_t* d_nodes, const double* d_hinge, const int32_t* d_face_pos,
+                           const int32_t* d_cell_faces, const int32_t* d_neighbors, double* d_face_areas,
+                           double* d_face_normals, double* d_face_centroids, double* d_cell_volumes,
+                           double* d_cell_centroids, void* stream);
+
+/* ------------------------------------------------------------------------
  * Transmissibilities.
  * pmb_compute_trans replaces compute_trans (pymrst/solvers/compute_trans.py:11-53):
  * one-sided T = (c . K n) / (c . c) per half-face, c = face centroid - cell

@@ -97,6 +97,7 @@ SIGNATURES = {
     "pmb_launch_count": (c_int, [P_i64]),
     "pmb_profile_report": (c_int, [C.c_char_p, c_int, c_int]),
     "pmb_compute_trans": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_vp, c_vp]),
+    "pmb_compute_geometry3d": (c_int, [c_int, c_int] + [c_vp] * 13),
     "pmb_face_trans": (c_int, [c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "pmb_dense_inverse": (c_int, [c_int, c_vp, c_vp, c_vp]),
     "pmb_ow_create": (c_int, [C.POINTER(OWDesc), c_vp, C.POINTER(c_vp)]),

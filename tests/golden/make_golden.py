@@ -7,7 +7,7 @@ Run once, where the reference's Python package is importable:
 NAME selects fixture groups: small (the toy-grid fixtures), cfg0 (incomp_tpfa
 at 64x64x8), cfg1 (the first oil-water steps at 100x100x10), cfg4 (the
 adjoint at 64x64x4), transport (the phase-3 transport cases), bo (the three-phase black-oil model on a synthetic
-deck: residuals and Jacobians, and Newton histories).  Without --only every
+deck: residuals and Jacobians, and Newton histories), geometry (compute_geometry on a perturbed 3-D grid).  Without --only every
 group is written.
 
 It writes small .npz files holding inputs and the reference's own outputs
@@ -579,6 +579,27 @@ def transport_fixture():
     save("transport_phase3.npz", **out)
 
 
+def geometry_fixture():
+    """compute_geometry on a 5x4x3 grid with seeded perturbed nodes
+    (non-planar faces), without and with hinge points on four faces: the
+    topology arrays and the reference's face and cell geometry."""
+    g = cart_grid([5, 4, 3], [50.0, 40.0, 6.0])
+    rng = np.random.default_rng(11)
+    g.nodes.coords = g.nodes.coords + rng.uniform(-0.15, 0.15, g.nodes.coords.shape) * np.array([10.0, 10.0, 2.0])
+    out = dict(coords=g.nodes.coords, node_pos=g.faces.nodePos, nodes=g.faces.nodes, face_pos=g.cells.facePos,
+               cell_faces=g.cells.faces, neighbors=g.faces.neighbors)
+    hf = np.array([0, 7, 31, 50])
+    hn = np.array([g.nodes.coords[g.faces.nodes[g.faces.nodePos[f]:g.faces.nodePos[f + 1]]].mean(axis=0)
+                   for f in hf]) + np.array([0.3, -0.2, 0.1])
+    for tag, hinge in (("plain", None), ("hinge", {"faces": hf, "nodes": hn})):
+        r = compute_geometry(g, hinge_nodes=hinge)
+        out.update({f"{tag}_face_areas": r.faces.areas, f"{tag}_face_normals": r.faces.normals,
+                    f"{tag}_face_centroids": r.faces.centroids, f"{tag}_cell_volumes": r.cells.volumes,
+                    f"{tag}_cell_centroids": r.cells.centroids})
+    out.update(hinge_faces=hf, hinge_nodes=hn)
+    save("geometry3d.npz", **out)
+
+
 if __name__ == "__main__":
     def want(name):
         return ONLY is None or name in ONLY
@@ -605,3 +626,5 @@ if __name__ == "__main__":
     if want("bo"):
         bo_assemble_fixture()
         bo_newton_fixture()
+    if want("geometry"):
+        geometry_fixture()
